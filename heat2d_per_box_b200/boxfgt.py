@@ -1,0 +1,155 @@
+"""Python mirror of the reference's boxfgt interface (bfgt/boxfgt.f:5-8) over
+the C ABI of libbfgt_b200.so, plus the device-resident plan.
+
+`boxfgt(...)` takes the reference's argument list in order, with numpy arrays
+in the reference layout, and calls the gfortran-ABI symbol boxfgt_ exactly as
+compiled Fortran would (every argument by reference).  Like the reference it
+accumulates into pot on leaf boxes and rewrites the colleague arrays of itree.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import BFGT_PREC_FP64, BFGT_PREC_SPLIT, BfgtError
+
+
+def _iref(v):
+    return C.byref(C.c_int(int(v)))
+
+
+def boxfgt(nd, ndim, delta, eps, ipoly, iperiod, norder, npbox, nboxes, nlevels, ltree, itree, iptr, centers, boxsize,
+           fvals, ifpgh, pot, grad, hess, ifnewtree, ntarg, targs, ifpghtarg, pote, grade, hesse, timeinfo):
+    """Drop-in for `call boxfgt(...)`: pot(nd,npbox,nboxes) += G_delta * fvals on leaves.
+
+    Raises BfgtError when the library records an error (the Fortran routine
+    itself has no error argument; the C ABI keeps its message in
+    bfgt_last_error()).
+    """
+    L = _lib.lib()
+    for name, a, dt in (("itree", itree, np.int32), ("iptr", iptr, np.int32), ("centers", centers, np.float64),
+                        ("boxsize", boxsize, np.float64), ("fvals", fvals, np.float64), ("pot", pot, np.float64),
+                        ("timeinfo", timeinfo, np.float64)):
+        if not (isinstance(a, np.ndarray) and a.dtype == dt and a.flags.c_contiguous):
+            raise TypeError(f"{name} must be a C-contiguous {np.dtype(dt).name} numpy array")
+    ip = C.c_int(int(iperiod))
+    nb, nl, lt = C.c_int(int(nboxes)), C.c_int(int(nlevels)), C.c_int(int(ltree))
+    dl, ep = C.c_double(float(delta)), C.c_double(float(eps))
+    L.boxfgt_(_iref(nd), _iref(ndim), C.byref(dl), C.byref(ep), _iref(ipoly), C.byref(ip), _iref(norder), _iref(npbox),
+              C.byref(nb), C.byref(nl), C.byref(lt), itree.reshape(-1), iptr, centers.reshape(-1), boxsize,
+              fvals.reshape(-1), _iref(ifpgh), pot.reshape(-1), None, None, _iref(ifnewtree), _iref(ntarg), None,
+              _iref(ifpghtarg), None, None, None, timeinfo)
+    err = _lib.last_error()
+    if err:
+        raise BfgtError(1, err)
+    return pot
+
+
+class Plan:
+    """Device-resident boxfgt for one tree / delta / eps / norder / nd.
+
+    execute(d_fvals, d_pot, stream) takes raw device pointers (ints) or torch
+    CUDA tensors; execute_host(fvals, pot) takes host numpy arrays.
+    """
+
+    def __init__(self, tree, delta, eps, nd=1, precision=BFGT_PREC_FP64):
+        self._L = _lib.lib()
+        self.tree = tree
+        self.nd = nd
+        self.itree = tree.itree.copy()
+        h = C.c_void_p()
+        _lib.check(self._L.bfgt_plan_create(C.byref(h), int(nd), float(delta), float(eps), int(tree.ipoly),
+                                            int(tree.iperiod), int(tree.norder), int(tree.nboxes), int(tree.nlevels),
+                                            int(tree.ltree), self.itree, np.ascontiguousarray(tree.iptr, np.int32),
+                                            np.ascontiguousarray(tree.centers, np.float64).reshape(-1),
+                                            np.ascontiguousarray(tree.boxsize, np.float64), int(precision)))
+        self._h = h
+
+    @staticmethod
+    def _ptr(x):
+        if x is None:
+            return None
+        if isinstance(x, int):
+            return x
+        if hasattr(x, "data_ptr"):
+            return x.data_ptr()
+        raise TypeError("expected a device pointer or a torch CUDA tensor")
+
+    def execute(self, d_fvals, d_pot, stream=None):
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_plan_execute(self._h, self._ptr(d_fvals), self._ptr(d_pot), s))
+
+    def execute_host(self, fvals, pot, stream=None):
+        fv = np.ascontiguousarray(fvals, np.float64)
+        if not (isinstance(pot, np.ndarray) and pot.dtype == np.float64 and pot.flags.c_contiguous):
+            raise TypeError("pot must be a C-contiguous float64 array")
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_plan_execute_host(self._h, fv.ctypes.data, pot.ctypes.data, s))
+        return pot
+
+    def graph_capture(self, d_fvals, d_pot, stream=None):
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_plan_graph_capture(self._h, self._ptr(d_fvals), self._ptr(d_pot), s))
+
+    def graph_launch(self, stream=None):
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_plan_graph_launch(self._h, s))
+
+    def stage_ms(self):
+        out = np.zeros(8)
+        _lib.check(self._L.bfgt_plan_stage_ms(self._h, out))
+        return out
+
+    def info(self):
+        out = np.zeros(16, np.int32)
+        _lib.check(self._L.bfgt_plan_info(self._h, out))
+        keys = ["npwlevel", "npw", "nlevstart", "nlevend", "regime", "nleafbox", "npwleaves", "nnear_targets",
+                "nnear_pairs", "mnlist1", "iperiod_int", "nchunks"]
+        return {k: int(out[i]) for i, k in enumerate(keys)}
+
+    def work(self):
+        out = np.zeros(4)
+        _lib.check(self._L.bfgt_plan_work(self._h, out))
+        return {"flops": out[0], "bytes": out[1], "tc_flops": out[2], "points": out[3]}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.bfgt_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def host_plan_dump(tree, delta, eps, nd=1, mnlist1_cap=64):
+    """Host half of a plan (no device needed): lists, band patterns, near-field tables, PW nodes."""
+    L = _lib.lib()
+    n, nb, nl = tree.norder, tree.nboxes, tree.nlevels
+    it = tree.itree.copy()
+    info = np.zeros(16, np.int32)
+    out = dict(ifpwexp=np.zeros(nb, np.int32), nlist1=np.zeros(nb, np.int32),
+               list1=np.zeros(mnlist1_cap * nb, np.int32), nlistpw=np.zeros(nb, np.int32),
+               listpw=np.zeros(8 * nb, np.int32), ind_loc=np.zeros(2 * (n + 1) * 13 * (nl + 1), np.int32),
+               tab_loc=np.zeros(n * n * 13 * (nl + 1)), ts=np.zeros(256), ws=np.zeros(256))
+    _lib.check(L.bfgt_host_plan_dump(int(nd), float(delta), float(eps), int(tree.ipoly), int(tree.iperiod), int(n),
+                                     int(nb), int(nl), int(tree.ltree), it, np.ascontiguousarray(tree.iptr, np.int32),
+                                     np.ascontiguousarray(tree.centers, np.float64).reshape(-1),
+                                     np.ascontiguousarray(tree.boxsize, np.float64), info.ctypes.data,
+                                     out["ifpwexp"].ctypes.data, out["nlist1"].ctypes.data, out["list1"].ctypes.data,
+                                     int(mnlist1_cap), out["nlistpw"].ctypes.data, out["listpw"].ctypes.data,
+                                     out["ind_loc"].ctypes.data, out["tab_loc"].ctypes.data, out["ts"].ctypes.data,
+                                     out["ws"].ctypes.data))
+    keys = ["npwlevel", "npw", "nlevstart", "nlevend", "regime", "nleafbox", "npwleaves", "nnear_targets",
+            "nnear_pairs", "mnlist1", "iperiod_int", "nchunks"]
+    d = {k: int(info[i]) for i, k in enumerate(keys)}
+    out["list1"] = out["list1"].reshape(nb, mnlist1_cap)
+    out["listpw"] = out["listpw"].reshape(nb, 8)
+    out["ts"] = out["ts"][: d["npw"]].copy()
+    out["ws"] = out["ws"][: d["npw"]].copy()
+    out["itree"] = it
+    return d, out

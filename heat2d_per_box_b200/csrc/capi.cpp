@@ -1,0 +1,392 @@
+// C ABI of libbfgt_b200.so (declared in include/bfgt.h).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/bfgt.h"
+#include "device_plan.hpp"
+#include "host_plan.hpp"
+
+struct bfgt_plan_s {
+  bfgt::HostPlan hp;
+  bfgt::DevicePlan dp;
+  double stage_ms[8] = {0};
+};
+
+struct bfgt_tree_s {
+  std::unique_ptr<bfgt::TreeData> t;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &m) {
+  g_err = m;
+  if (std::getenv("BFGT_ABORT_ON_ERROR")) {
+    std::fprintf(stderr, "bfgt: %s\n", m.c_str());
+    std::abort();
+  }
+  return code;
+}
+
+bfgt::TreeView make_view(int nboxes, int nlevels, int ltree, int *itree, const int *iptr, const double *centers,
+                         const double *boxsize) {
+  if (!itree || !iptr || !centers || !boxsize) throw std::runtime_error("null tree array");
+  if (iptr[0] != 1 || iptr[1] != 2 * (nlevels + 1) + 1) throw std::runtime_error("iptr(1:2) inconsistent with nlevels");
+  const long need = (long)iptr[6] - 1 + 9L * nboxes;
+  if (need > ltree) throw std::runtime_error("ltree too small for nboxes");
+  if (iptr[2] != iptr[1] + nboxes || iptr[3] != iptr[2] + nboxes || iptr[4] != iptr[3] + nboxes ||
+      iptr[5] != iptr[4] + 4 * nboxes || iptr[6] != iptr[5] + nboxes)
+    throw std::runtime_error("iptr(3:7) inconsistent with nboxes (expected the vol_tree_build layout)");
+  bfgt::TreeView t;
+  t.nboxes = nboxes;
+  t.nlevels = nlevels;
+  t.itree = itree;
+  t.iptr = iptr;
+  t.centers = centers;
+  t.boxsize = boxsize;
+  return t;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *bfgt_last_error(void) { return g_err.c_str(); }
+
+int bfgt_plan_create(bfgt_plan *plan, int nd, double delta, double eps, int ipoly, int iperiod, int norder,
+                     int nboxes, int nlevels, int ltree, int *itree, const int *iptr, const double *centers,
+                     const double *boxsize, int precision) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan pointer is NULL");
+  *plan = nullptr;
+  if (precision != BFGT_PREC_FP64 && precision != BFGT_PREC_SPLIT) return fail(BFGT_ERR_ARG, "unknown precision mode");
+  std::unique_ptr<bfgt_plan_s> p(new bfgt_plan_s());
+  try {
+    bfgt::TreeView t = make_view(nboxes, nlevels, ltree, itree, iptr, centers, boxsize);
+    bfgt::build_host_plan(p->hp, t, nd, delta, eps, ipoly, iperiod, norder, precision);
+  } catch (const std::exception &e) {
+    return fail(BFGT_ERR_TREE, e.what());
+  }
+  std::string msg;
+  int rc = bfgt::device_plan_create(p->dp, p->hp, msg);
+  if (rc != BFGT_OK) {
+    bfgt::device_plan_destroy(p->dp);
+    return fail(rc, msg);
+  }
+  *plan = p.release();
+  return BFGT_OK;
+}
+
+int bfgt_plan_execute(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (!d_fvals || !d_pot) return fail(BFGT_ERR_ARG, "fvals/pot device pointers are NULL");
+  std::string msg;
+  int rc = bfgt::device_plan_execute(plan->dp, d_fvals, d_pot, (cudaStream_t)stream, msg);
+  if (rc != BFGT_OK) return fail(rc, msg);
+  return BFGT_OK;
+}
+
+int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, void *stream) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (!fvals || !pot) return fail(BFGT_ERR_ARG, "fvals/pot are NULL");
+  bfgt::DevicePlan &dp = plan->dp;
+  const size_t elems = (size_t)dp.nd * dp.n * dp.n * dp.nboxes;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dp.stage_elems < elems) {
+    if (dp.d_stage_f) cudaFree(dp.d_stage_f);
+    if (dp.d_stage_p) cudaFree(dp.d_stage_p);
+    dp.d_stage_f = dp.d_stage_p = nullptr;
+    dp.stage_elems = 0;
+    if (cudaMalloc(&dp.d_stage_f, elems * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&dp.d_stage_p, elems * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(BFGT_ERR_OOM, "cannot allocate device staging buffers");
+    }
+    dp.stage_elems = elems;
+  }
+  if (cudaMemcpyAsync(dp.d_stage_f, fvals, elems * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(dp.d_stage_p, pot, elems * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
+  std::string msg;
+  int rc = bfgt::device_plan_execute(dp, dp.d_stage_f, dp.d_stage_p, s, msg);
+  if (rc != BFGT_OK) return fail(rc, msg);
+  if (cudaMemcpyAsync(pot, dp.d_stage_p, elems * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return fail(BFGT_ERR_CUDA, "device-to-host copy failed");
+  if (cudaStreamSynchronize(s) != cudaSuccess) return fail(BFGT_ERR_CUDA, std::string("transform failed: ") + cudaGetErrorString(cudaGetLastError()));
+  return BFGT_OK;
+}
+
+int bfgt_plan_graph_capture(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  bfgt::DevicePlan &dp = plan->dp;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaStream_t cs = s;
+  bool own = false;
+  if (!cs) {
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return fail(BFGT_ERR_CUDA, "stream create failed");
+    own = true;
+  }
+  if (dp.graph_exec) cudaGraphExecDestroy(dp.graph_exec);
+  if (dp.graph) cudaGraphDestroy(dp.graph);
+  dp.graph_exec = nullptr;
+  dp.graph = nullptr;
+  bool ev = dp.events;
+  dp.events = false;  // no event records inside the graph
+  std::string msg;
+  int rc = BFGT_OK;
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = BFGT_ERR_CUDA, msg = "begin capture failed";
+  if (rc == BFGT_OK) rc = bfgt::device_plan_execute(dp, d_fvals, d_pot, cs, msg);
+  cudaGraph_t g = nullptr;
+  if (cudaStreamEndCapture(cs, &g) != cudaSuccess && rc == BFGT_OK) rc = BFGT_ERR_CUDA, msg = "end capture failed";
+  dp.events = ev;
+  if (rc == BFGT_OK && cudaGraphInstantiate(&dp.graph_exec, g, 0) != cudaSuccess) rc = BFGT_ERR_CUDA, msg = "graph instantiate failed";
+  dp.graph = g;
+  if (own) cudaStreamDestroy(cs);
+  if (rc != BFGT_OK) {
+    cudaGetLastError();
+    return fail(rc, msg);
+  }
+  return BFGT_OK;
+}
+
+int bfgt_plan_graph_launch(bfgt_plan plan, void *stream) {
+  g_err.clear();
+  if (!plan || !plan->dp.graph_exec) return fail(BFGT_ERR_ARG, "no captured graph on this plan");
+  if (cudaGraphLaunch(plan->dp.graph_exec, (cudaStream_t)stream) != cudaSuccess) return fail(BFGT_ERR_CUDA, "graph launch failed");
+  return BFGT_OK;
+}
+
+int bfgt_plan_stage_ms(bfgt_plan plan, double *out) {
+  g_err.clear();
+  if (!plan || !out) return fail(BFGT_ERR_ARG, "NULL argument");
+  bfgt::DevicePlan &dp = plan->dp;
+  for (int i = 0; i < 8; i++) out[i] = 0;
+  if (!dp.events) return BFGT_OK;
+  if (cudaEventSynchronize(dp.ev[5]) != cudaSuccess) return fail(BFGT_ERR_CUDA, "event sync failed");
+  float ms;
+  for (int i = 0; i < 5; i++) {
+    if (cudaEventElapsedTime(&ms, dp.ev[i], dp.ev[i + 1]) == cudaSuccess) out[i] = ms;
+  }
+  if (cudaEventElapsedTime(&ms, dp.ev[0], dp.ev[5]) == cudaSuccess) out[5] = ms;
+  cudaGetLastError();
+  return BFGT_OK;
+}
+
+int bfgt_plan_info(bfgt_plan plan, int *out) {
+  g_err.clear();
+  if (!plan || !out) return fail(BFGT_ERR_ARG, "NULL argument");
+  const bfgt::HostPlan &h = plan->hp;
+  for (int i = 0; i < 16; i++) out[i] = 0;
+  out[0] = h.npwlevel;
+  out[1] = h.npw;
+  out[2] = h.nlevstart;
+  out[3] = h.nlevend;
+  out[4] = h.regime;
+  out[5] = h.nleafbox;
+  out[6] = (int)h.leaves.size();
+  out[7] = (int)h.nf_target.size();
+  out[8] = (int)h.nf_src.size();
+  out[9] = h.mnlist1;
+  out[10] = h.iperiod_int;
+  out[11] = (int)h.chunks.size();
+  return BFGT_OK;
+}
+
+int bfgt_plan_work(bfgt_plan plan, double *out) {
+  g_err.clear();
+  if (!plan || !out) return fail(BFGT_ERR_ARG, "NULL argument");
+  out[0] = plan->hp.flops;
+  out[1] = plan->hp.bytes;
+  out[2] = plan->hp.tc_flops;
+  out[3] = plan->hp.points;
+  return BFGT_OK;
+}
+
+int bfgt_plan_destroy(bfgt_plan plan) {
+  g_err.clear();
+  if (!plan) return BFGT_OK;
+  bfgt::device_plan_destroy(plan->dp);
+  delete plan;
+  return BFGT_OK;
+}
+
+int bfgt_boxfgt(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
+                int ltree, int *itree, const int *iptr, const double *centers, const double *boxsize,
+                const double *fvals, double *pot, double *timeinfo, int precision) {
+  double t0 = now_s();
+  bfgt_plan plan = nullptr;
+  int rc = bfgt_plan_create(&plan, nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree, iptr,
+                            centers, boxsize, precision);
+  if (rc != BFGT_OK) return rc;
+  double t1 = now_s();
+  rc = bfgt_plan_execute_host(plan, fvals, pot, nullptr);
+  if (rc == BFGT_OK && timeinfo) {
+    double st[8];
+    bfgt_plan_stage_ms(plan, st);
+    for (int i = 0; i < 20; i++) timeinfo[i] = 0;
+    timeinfo[0] = t1 - t0;           // step 0: precomputation
+    timeinfo[1] = st[0] * 1e-3;      // steps 1+2: leaf -> cutoff expansions
+    timeinfo[2] = st[1] * 1e-3;      // fixed-order partial-sum reduction
+    timeinfo[3] = st[2] * 1e-3;      // step 3: cutoff translations
+    timeinfo[4] = 0;                 // step 4 is fused into step 5
+    timeinfo[5] = st[3] * 1e-3;      // steps 4+5: cutoff expansions -> leaf values
+    timeinfo[6] = st[4] * 1e-3;      // step 6: near field
+  }
+  std::string keep = g_err;
+  bfgt_plan_destroy(plan);
+  g_err = keep;
+  return rc;
+}
+
+void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *eps, const int *ipoly, int *iperiod,
+             const int *norder, const int *npbox, int *nboxes, int *nlevels, int *ltree, int *itree, int *iptr,
+             double *centers, double *boxsize, const double *fvals, const int *ifpgh, double *pot, double *grad,
+             double *hess, const int *ifnewtree, const int *ntarg, const double *targs, const int *ifpghtarg,
+             double *pote, double *grade, double *hesse, double *timeinfo) {
+  (void)grad;
+  (void)hess;
+  (void)targs;
+  (void)pote;
+  (void)grade;
+  (void)hesse;
+  g_err.clear();
+  if (!nd || !ndim || !delta || !eps || !ipoly || !iperiod || !norder || !npbox || !nboxes || !nlevels || !ltree ||
+      !ifpgh || !ifnewtree || !ntarg || !ifpghtarg) {
+    fail(BFGT_ERR_ARG, "boxfgt_: NULL scalar argument");
+    return;
+  }
+  if (*ndim != 2) {
+    fail(BFGT_ERR_ARG, "boxfgt_: only ndim=2 is supported");
+    return;
+  }
+  if (*ifpgh != 1 || *ifpghtarg > 0 || *ifnewtree != 0) {
+    fail(BFGT_ERR_ARG, "boxfgt_: only ifpgh=1, ifpghtarg=0, ifnewtree=0 are supported");
+    return;
+  }
+  if (*npbox != (*norder) * (*norder)) {
+    fail(BFGT_ERR_ARG, "boxfgt_: npbox must equal norder**2");
+    return;
+  }
+  double ti[20];
+  bfgt_boxfgt(*nd, *delta, *eps, *ipoly, *iperiod, *norder, *nboxes, *nlevels, *ltree, itree, iptr, centers, boxsize,
+              fvals, pot, timeinfo ? timeinfo : ti, BFGT_PREC_FP64);
+}
+
+int bfgt_host_plan_dump(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes,
+                        int nlevels, int ltree, int *itree, const int *iptr, const double *centers,
+                        const double *boxsize, int *info, int *ifpwexp, int *nlist1, int *list1, int mnlist1_cap,
+                        int *nlistpw, int *listpw, int *ind_loc, double *tab_loc, double *ts, double *ws) {
+  g_err.clear();
+  bfgt::HostPlan hp;
+  try {
+    bfgt::TreeView t = make_view(nboxes, nlevels, ltree, itree, iptr, centers, boxsize);
+    bfgt::build_host_plan(hp, t, nd, delta, eps, ipoly, iperiod, norder, BFGT_PREC_FP64);
+  } catch (const std::exception &e) {
+    return fail(BFGT_ERR_TREE, e.what());
+  }
+  if (info) {
+    for (int i = 0; i < 16; i++) info[i] = 0;
+    info[0] = hp.npwlevel;
+    info[1] = hp.npw;
+    info[2] = hp.nlevstart;
+    info[3] = hp.nlevend;
+    info[4] = hp.regime;
+    info[5] = hp.nleafbox;
+    info[6] = (int)hp.leaves.size();
+    info[7] = (int)hp.nf_target.size();
+    info[8] = (int)hp.nf_src.size();
+    info[9] = hp.mnlist1;
+    info[10] = hp.iperiod_int;
+    info[11] = (int)hp.chunks.size();
+  }
+  if (ifpwexp) std::memcpy(ifpwexp, hp.ifpwexp.data(), sizeof(int) * nboxes);
+  if (nlist1) std::memcpy(nlist1, hp.nlist1.data(), sizeof(int) * nboxes);
+  if (list1) {
+    if (mnlist1_cap < hp.mnlist1) return fail(BFGT_ERR_ARG, "mnlist1_cap smaller than mnlist1");
+    for (int b = 0; b < nboxes; b++)
+      for (int j = 0; j < hp.nlist1[b]; j++) list1[(size_t)mnlist1_cap * b + j] = hp.list1[(size_t)hp.mnlist1 * b + j];
+  }
+  if (nlistpw) {
+    if (hp.nlistpw.empty()) std::memset(nlistpw, 0, sizeof(int) * nboxes);
+    else std::memcpy(nlistpw, hp.nlistpw.data(), sizeof(int) * nboxes);
+  }
+  if (listpw && !hp.listpw.empty()) std::memcpy(listpw, hp.listpw.data(), sizeof(int) * 8 * (size_t)nboxes);
+  if (ind_loc) std::memcpy(ind_loc, hp.ind_loc.data(), sizeof(int) * hp.ind_loc.size());
+  if (tab_loc) std::memcpy(tab_loc, hp.tab_loc.data(), sizeof(double) * hp.tab_loc.size());
+  if (ts && !hp.ts.empty()) std::memcpy(ts, hp.ts.data(), sizeof(double) * hp.ts.size());
+  if (ws && !hp.ws.empty()) std::memcpy(ws, hp.ws.data(), sizeof(double) * hp.ws.size());
+  return BFGT_OK;
+}
+
+int bfgt_tree_build_gauss(bfgt_tree *tree, int ipoly, int iperiod, double eps, double boxlen, int norder, double eta,
+                          int ng, const double *gauss, int minlev, int maxlev) {
+  g_err.clear();
+  if (!tree) return fail(BFGT_ERR_ARG, "tree pointer is NULL");
+  *tree = nullptr;
+  try {
+    auto *h = new bfgt_tree_s();
+    h->t.reset(bfgt::tree_build(ipoly, iperiod, eps, boxlen, norder, eta, ng, gauss, minlev, maxlev, false));
+    *tree = h;
+  } catch (const std::exception &e) {
+    return fail(BFGT_ERR_ARG, e.what());
+  }
+  return BFGT_OK;
+}
+
+int bfgt_tree_build_uniform(bfgt_tree *tree, int ipoly, int iperiod, double boxlen, int norder, int nlev, int ng,
+                            const double *gauss) {
+  g_err.clear();
+  if (!tree) return fail(BFGT_ERR_ARG, "tree pointer is NULL");
+  *tree = nullptr;
+  try {
+    auto *h = new bfgt_tree_s();
+    h->t.reset(bfgt::tree_build(ipoly, iperiod, 1.0, boxlen, norder, 0.0, ng, gauss, nlev, nlev, true));
+    *tree = h;
+  } catch (const std::exception &e) {
+    return fail(BFGT_ERR_ARG, e.what());
+  }
+  return BFGT_OK;
+}
+
+int bfgt_tree_sizes(bfgt_tree tree, int *nboxes, int *nlevels, int *ltree) {
+  g_err.clear();
+  if (!tree) return fail(BFGT_ERR_ARG, "tree is NULL");
+  if (nboxes) *nboxes = tree->t->nboxes;
+  if (nlevels) *nlevels = tree->t->nlevels;
+  if (ltree) *ltree = (int)tree->t->itree.size();
+  return BFGT_OK;
+}
+
+int bfgt_tree_export(bfgt_tree tree, int *itree, int *iptr, double *centers, double *boxsize, double *fvals) {
+  g_err.clear();
+  if (!tree) return fail(BFGT_ERR_ARG, "tree is NULL");
+  const bfgt::TreeData &t = *tree->t;
+  if (itree) std::memcpy(itree, t.itree.data(), sizeof(int) * t.itree.size());
+  if (iptr) std::memcpy(iptr, t.iptr, sizeof(int) * 8);
+  if (centers) std::memcpy(centers, t.centers.data(), sizeof(double) * t.centers.size());
+  if (boxsize) std::memcpy(boxsize, t.boxsize.data(), sizeof(double) * t.boxsize.size());
+  if (fvals) std::memcpy(fvals, t.fvals.data(), sizeof(double) * t.fvals.size());
+  return BFGT_OK;
+}
+
+int bfgt_tree_free(bfgt_tree tree) {
+  delete tree;
+  return BFGT_OK;
+}
+
+}  // extern "C"

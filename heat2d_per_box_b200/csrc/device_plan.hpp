@@ -1,0 +1,57 @@
+// Device half of a box-FGT plan: the uploaded tables and work lists, and the
+// launch sequence of one transform.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "host_plan.hpp"
+
+namespace bfgt {
+
+struct DevicePlan {
+  int device = 0;
+  int nd = 1, n = 0, npw = 0, hh = 0, nexp = 0, nlevels = 0, nboxes = 0, precision = 0;
+  int ncut = 0, nchunks = 0, nleaves = 0, nnf = 0, nnf_entries = 0;
+  bool direct_only = false;
+  // plane-wave part
+  double2 *T = nullptr;         // tab_poly2pw, per level (n, npw)
+  double2 *E = nullptr;         // tab_pw2pot, per level (npw, n)
+  double2 *PH = nullptr;        // phase tables
+  long long *ph_off = nullptr;  // per level offsets into PH
+  int4 *leaves = nullptr;       // {box, ox, oy, level}
+  int4 *chunks = nullptr;       // {begin, end, icut, level}
+  int *cut_chunk_begin = nullptr, *cut_pw_begin = nullptr, *cut_pw_src = nullptr, *cut_pw_ind = nullptr;
+  double2 *W = nullptr;         // cutoff shifts (nexp, 9)
+  double *pw_weight = nullptr;  // (hh)
+  double2 *Mpart = nullptr;     // (nchunks, nd, nexp)
+  double2 *M = nullptr;         // (ncut, nd, nexp)
+  double2 *L = nullptr;         // (ncut, nd, nexp)
+  // split-precision scratch (FP16 operand slices of the level tables)
+  void *Tsplit = nullptr, *Esplit = nullptr;
+  double *Tscale = nullptr, *Escale = nullptr;
+  // near field
+  int *nf_target = nullptr, *nf_level = nullptr, *nf_begin = nullptr, *nf_src = nullptr;
+  int2 *nf_ixy = nullptr;
+  double *tab_loc = nullptr;
+  int *ind_loc = nullptr;
+  // staging for host-buffer execution
+  double *h_stage_f = nullptr, *h_stage_p = nullptr;  // pinned
+  double *d_stage_f = nullptr, *d_stage_p = nullptr;
+  size_t stage_elems = 0;
+  // timing
+  cudaEvent_t ev[8] = {};
+  bool events = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  size_t smem_form = 0, smem_eval = 0, smem_near = 0;
+};
+
+// Allocates and uploads; returns a BFGT_* status and fills msg on failure.
+int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);
+void device_plan_destroy(DevicePlan &dp);
+// Queues the transform on stream; returns BFGT_* status.
+int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cudaStream_t stream,
+                        std::string &msg);
+
+}  // namespace bfgt

@@ -1,0 +1,602 @@
+// Device kernels of the 2D box FGT and the plan's launch sequence.
+//
+// The reference's steps (bfgt/boxfgt.f) map onto the kernels as follows:
+//   step 1 (leaf values -> multipole PW, boxfgt.f:728-744, g2d_tens_prod_to_pw
+//   bfgt_pwrouts.f:98-147) and step 2 (merge to parents, boxfgt.f:764-783,
+//   gnd_shiftpw bfgt_pwrouts.f:1798-1844) are fused in k_form: the merge shifts
+//   are diagonal, so the product of the shifts from a leaf up to its cutoff
+//   ancestor is one phase exp(-i ts.(c_leaf - c_anc)/sqrt(delta0)), taken from
+//   a precomputed FP64 phase table, and each leaf's expansion is added
+//   straight into its ancestor's expansion.  Partial sums per chunk of leaves
+//   are reduced in a fixed order (k_reduce), so the result is deterministic.
+//   step 3 (mp -> loc at the cutoff level, boxfgt.f:805-822) is k_translate.
+//   step 4 (split, boxfgt.f:845-863, gnd_shiftpw_loc bfgt_pwrouts.f:1905-1941)
+//   and step 5 (loc PW -> values, boxfgt.f:884-900, g2d_pw2pot
+//   bfgt_pwrouts.f:549-602) are fused in k_eval by the conjugate phases.
+//   step 6 (near field, boxfgt.f:915-1071, g2d_tens_prod_to_potloc
+//   bfgt_local.f:315-375) is k_near over a host-built list of
+//   (target, source, table x, table y) entries that already contains the
+//   periodic level-1 images of boxfgt.f:938-1053.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/bfgt.h"
+#include "device_plan.hpp"
+#include "split_kernels.cuh"
+
+namespace bfgt {
+
+namespace {
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ void cfma(double2 &acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+}
+
+constexpr int kWarps = 4;
+
+struct FormArgs {
+  const double *fvals;
+  const int4 *leaves;
+  const int4 *chunks;
+  const double2 *T;
+  const double2 *PH;
+  const long long *ph_off;
+  double2 *Mpart;
+  int nd, n, npw, hh, nexp;
+};
+
+// One CTA per chunk (leaves with the same cutoff ancestor and level).  Warp w
+// takes leaves w, w+4, ... of the chunk; for each leaf and density it forms
+//   ff(m1,k2) = ey(k2) sum_m2 F(m1,m2) T(m2,k2)
+//   M(k1,k2) += ex(k1) sum_m1 T(m1,k1) ff(m1,k2)
+// with ex, ey the conjugate phases from the leaf to the ancestor centre.  The
+// (k1,k2) outputs are cut into TM x TN tiles dealt round-robin to the lanes.
+template <int TM, int TN>
+__global__ void __launch_bounds__(kWarps * 32) k_form_fp64(FormArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 ch = a.chunks[blockIdx.x];
+  const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *sT = reinterpret_cast<double2 *>(smem_raw);  // [m][k], n x npw
+  const size_t per_warp = (size_t)npw * hh + (size_t)n * hh + npw + hh + (npb + 1) / 2;
+  double2 *wb = sT + (size_t)n * npw + per_warp * warp;
+  double2 *sM = wb;                      // [k2][k1]
+  double2 *sff = sM + (size_t)npw * hh;  // [m1][k2]
+  double2 *sex = sff + (size_t)n * hh;
+  double2 *sey = sex + npw;
+  double *sF = reinterpret_cast<double *>(sey + hh);  // [m2][m1]
+
+  const double2 *Tg = a.T + (size_t)n * npw * ch.w;
+  for (int i = threadIdx.x; i < n * npw; i += blockDim.x) {
+    int m = i % n, k = i / n;
+    sT[m * npw + k] = Tg[i];
+  }
+  __syncthreads();
+  const int ntm = (npw + TM - 1) / TM, ntn = (hh + TN - 1) / TN, ntiles = ntm * ntn;
+  for (int ind = 0; ind < nd; ind++) {
+    for (int e = lane; e < npw * hh; e += 32) sM[e] = make_double2(0, 0);
+    __syncwarp();
+    for (int li = ch.x + warp; li < ch.y; li += kWarps) {
+      const int4 lf = a.leaves[li];
+      const double *fv = a.fvals + (size_t)lf.x * nd * npb;
+      for (int j = lane; j < npb; j += 32) sF[j] = fv[ind + (size_t)nd * j];
+      const double2 *phx = a.PH + a.ph_off[lf.w] + (size_t)lf.y * npw;
+      const double2 *phy = a.PH + a.ph_off[lf.w] + (size_t)lf.z * npw;
+      for (int k = lane; k < npw; k += 32) {
+        double2 p = phx[k];
+        sex[k] = make_double2(p.x, -p.y);
+      }
+      for (int k = lane; k < hh; k += 32) {
+        double2 p = phy[k];
+        sey[k] = make_double2(p.x, -p.y);
+      }
+      __syncwarp();
+      for (int o = lane; o < n * hh; o += 32) {
+        const int m1 = o / hh, k2 = o - m1 * hh;
+        double2 acc = make_double2(0, 0);
+        for (int m2 = 0; m2 < n; m2++) {
+          const double f = sF[m1 + n * m2];
+          const double2 t = sT[m2 * npw + k2];
+          acc.x = fma(f, t.x, acc.x);
+          acc.y = fma(f, t.y, acc.y);
+        }
+        sff[m1 * hh + k2] = cmul(acc, sey[k2]);
+      }
+      __syncwarp();
+      for (int tile = lane; tile < ntiles; tile += 32) {
+        const int k1b = (tile % ntm) * TM, k2b = (tile / ntm) * TN;
+        double2 P[TM][TN];
+#pragma unroll
+        for (int i = 0; i < TM; i++)
+#pragma unroll
+          for (int j = 0; j < TN; j++) P[i][j] = make_double2(0, 0);
+        for (int m1 = 0; m1 < n; m1++) {
+          double2 av[TM], bv[TN];
+#pragma unroll
+          for (int i = 0; i < TM; i++) av[i] = (k1b + i < npw) ? sT[m1 * npw + k1b + i] : make_double2(0, 0);
+#pragma unroll
+          for (int j = 0; j < TN; j++) bv[j] = (k2b + j < hh) ? sff[m1 * hh + k2b + j] : make_double2(0, 0);
+#pragma unroll
+          for (int i = 0; i < TM; i++)
+#pragma unroll
+            for (int j = 0; j < TN; j++) cfma(P[i][j], av[i], bv[j]);
+        }
+#pragma unroll
+        for (int i = 0; i < TM; i++) {
+          const int k1 = k1b + i;
+          if (k1 >= npw) continue;
+          const double2 ex = sex[k1];
+#pragma unroll
+          for (int j = 0; j < TN; j++) {
+            const int k2 = k2b + j;
+            if (k2 >= hh) continue;
+            double2 &m = sM[k2 * npw + k1];
+            const double2 v = cmul(ex, P[i][j]);
+            m.x += v.x;
+            m.y += v.y;
+          }
+        }
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+    // fixed-order reduction of the warps' partial expansions
+    double2 *out = a.Mpart + ((size_t)blockIdx.x * nd + ind) * a.nexp;
+    const double2 *w0 = sT + (size_t)n * npw;
+    for (int e = threadIdx.x; e < a.nexp; e += blockDim.x) {
+      double2 s = make_double2(0, 0);
+      for (int w = 0; w < kWarps; w++) {
+        const double2 v = w0[per_warp * w + e];
+        s.x += v.x;
+        s.y += v.y;
+      }
+      out[e] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// M(icut, ind, :) = sum over the cutoff box's chunks, in chunk order
+__global__ void k_reduce(const double2 *__restrict__ Mpart, const int *__restrict__ cut_chunk_begin,
+                         double2 *__restrict__ M, int nd, int nexp) {
+  const int ic = blockIdx.x, ind = blockIdx.y;
+  const int c0 = cut_chunk_begin[ic], c1 = cut_chunk_begin[ic + 1];
+  for (int e = blockIdx.z * blockDim.x + threadIdx.x; e < nexp; e += gridDim.z * blockDim.x) {
+    double2 s = make_double2(0, 0);
+    for (int c = c0; c < c1; c++) {
+      const double2 v = Mpart[((size_t)c * nd + ind) * nexp + e];
+      s.x += v.x;
+      s.y += v.y;
+    }
+    M[((size_t)ic * nd + ind) * nexp + e] = s;
+  }
+}
+
+// L(icut) = M(icut) + sum_{listpw} M(src) * W(shift)   (boxfgt.f:805-822)
+__global__ void k_translate(const double2 *__restrict__ M, const int *__restrict__ pw_begin,
+                            const int *__restrict__ pw_src, const int *__restrict__ pw_ind,
+                            const double2 *__restrict__ W, double2 *__restrict__ L, int nd, int nexp) {
+  const int ic = blockIdx.x, ind = blockIdx.y;
+  const int j0 = pw_begin[ic], j1 = pw_begin[ic + 1];
+  for (int e = blockIdx.z * blockDim.x + threadIdx.x; e < nexp; e += gridDim.z * blockDim.x) {
+    double2 s = M[((size_t)ic * nd + ind) * nexp + e];
+    for (int j = j0; j < j1; j++) {
+      const double2 m = M[((size_t)pw_src[j] * nd + ind) * nexp + e];
+      const double2 w = W[(size_t)pw_ind[j] * nexp + e];
+      s.x += m.x * w.x - m.y * w.y;
+      s.y += m.x * w.y + m.y * w.x;
+    }
+    L[((size_t)ic * nd + ind) * nexp + e] = s;
+  }
+}
+
+struct EvalArgs {
+  double *pot;
+  const int4 *leaves;
+  const int4 *chunks;
+  const double2 *E;
+  const double2 *PH;
+  const long long *ph_off;
+  const double2 *L;
+  const double *pw_weight;
+  int nd, n, npw, hh, nexp;
+};
+
+// One CTA per chunk.  For each leaf and density:
+//   L'(m1,m2) = L(m1,m2) ex(m1) ey(m2) w(m2)        (split phases, FP64)
+//   G(k1,m2)  = sum_m1 E(m1,k1) L'(m1,m2)
+//   pot(k1,k2) += 2 Re sum_m2 E(m2,k2) G(k1,m2)
+template <int GM, int GN>
+__global__ void __launch_bounds__(kWarps * 32) k_eval_fp64(EvalArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 ch = a.chunks[blockIdx.x];
+  const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *sE = reinterpret_cast<double2 *>(smem_raw);  // [m][k] (npw x n, k fastest)
+  double2 *sL = sE + (size_t)npw * n;                    // [m2][m1]
+  const size_t per_warp = (size_t)npw * hh + (size_t)n * hh + npw + hh;
+  double2 *wb = sL + (size_t)npw * hh + per_warp * warp;
+  double2 *sLp = wb;                     // [m1][m2]
+  double2 *sG = sLp + (size_t)npw * hh;  // [m2][k1]
+  double2 *sex = sG + (size_t)n * hh;
+  double2 *sey = sex + npw;
+  const double2 *Eg = a.E + (size_t)n * npw * ch.w;  // Fortran (npw, n)
+  for (int i = threadIdx.x; i < n * npw; i += blockDim.x) {
+    const int m = i % npw, k = i / npw;
+    sE[m * n + k] = Eg[i];
+  }
+  const int ntm = (n + GM - 1) / GM, ntn = (hh + GN - 1) / GN, ntiles = ntm * ntn;
+  for (int ind = 0; ind < nd; ind++) {
+    const double2 *Lg = a.L + ((size_t)ch.z * nd + ind) * a.nexp;
+    for (int e = threadIdx.x; e < a.nexp; e += blockDim.x) sL[e] = Lg[e];
+    __syncthreads();
+    for (int li = ch.x + warp; li < ch.y; li += kWarps) {
+      const int4 lf = a.leaves[li];
+      const double2 *phx = a.PH + a.ph_off[lf.w] + (size_t)lf.y * npw;
+      const double2 *phy = a.PH + a.ph_off[lf.w] + (size_t)lf.z * npw;
+      for (int k = lane; k < npw; k += 32) sex[k] = phx[k];
+      for (int k = lane; k < hh; k += 32) {
+        double2 p = phy[k];
+        const double w = a.pw_weight[k];
+        sey[k] = make_double2(p.x * w, p.y * w);
+      }
+      __syncwarp();
+      for (int e = lane; e < npw * hh; e += 32) {
+        const int m2 = e / npw, m1 = e - m2 * npw;
+        sLp[m1 * hh + m2] = cmul(cmul(sL[e], sex[m1]), sey[m2]);
+      }
+      __syncwarp();
+      for (int tile = lane; tile < ntiles; tile += 32) {
+        const int k1b = (tile % ntm) * GM, m2b = (tile / ntm) * GN;
+        double2 G[GM][GN];
+#pragma unroll
+        for (int i = 0; i < GM; i++)
+#pragma unroll
+          for (int j = 0; j < GN; j++) G[i][j] = make_double2(0, 0);
+        for (int m1 = 0; m1 < npw; m1++) {
+          double2 av[GM], bv[GN];
+#pragma unroll
+          for (int i = 0; i < GM; i++) av[i] = (k1b + i < n) ? sE[m1 * n + k1b + i] : make_double2(0, 0);
+#pragma unroll
+          for (int j = 0; j < GN; j++) bv[j] = (m2b + j < hh) ? sLp[m1 * hh + m2b + j] : make_double2(0, 0);
+#pragma unroll
+          for (int i = 0; i < GM; i++)
+#pragma unroll
+            for (int j = 0; j < GN; j++) cfma(G[i][j], av[i], bv[j]);
+        }
+#pragma unroll
+        for (int i = 0; i < GM; i++) {
+          if (k1b + i >= n) continue;
+#pragma unroll
+          for (int j = 0; j < GN; j++)
+            if (m2b + j < hh) sG[(m2b + j) * n + k1b + i] = G[i][j];
+        }
+      }
+      __syncwarp();
+      double *pb = a.pot + (size_t)lf.x * nd * npb;
+      for (int o = lane; o < npb; o += 32) {
+        const int k1 = o % n, k2 = o / n;
+        double acc = 0;
+        for (int m2 = 0; m2 < hh; m2++) {
+          const double2 e = sE[m2 * n + k2];
+          const double2 g = sG[m2 * n + k1];
+          acc = fma(e.x, g.x, acc);
+          acc = fma(-e.y, g.y, acc);
+        }
+        pb[ind + (size_t)nd * o] += 2 * acc;
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+}
+
+// tile shape with the fewest wasted lane-slots for an a x b output
+struct TileChoice {
+  int tm, tn;
+};
+inline TileChoice best_tile(int a, int b, const TileChoice *cands, int nc) {
+  TileChoice best = cands[0];
+  double beff = -1;
+  for (int i = 0; i < nc; i++) {
+    const int tm = cands[i].tm, tn = cands[i].tn;
+    const int tiles = ((a + tm - 1) / tm) * ((b + tn - 1) / tn);
+    const int passes = (tiles + 31) / 32;
+    const double eff = (double)a * b / (32.0 * passes * tm * tn);
+    if (eff > beff + 1e-9 || (std::abs(eff - beff) <= 1e-9 && tm * tn > best.tm * best.tn)) {
+      beff = eff;
+      best = cands[i];
+    }
+  }
+  return best;
+}
+
+const TileChoice kFormTiles[] = {{4, 4}, {5, 4}, {4, 5}, {5, 5}, {6, 6}, {8, 4}};
+const TileChoice kEvalTiles[] = {{1, 5}, {2, 5}, {2, 4}, {4, 4}, {2, 8}, {4, 5}};
+
+void launch_form_fp64(const TileChoice &t, int grid, size_t smem, cudaStream_t s, const FormArgs &a) {
+#define FORM_CASE(M_, N_)                                                                    \
+  if (t.tm == M_ && t.tn == N_) {                                                            \
+    k_form_fp64<M_, N_><<<grid, kWarps * 32, smem, s>>>(a);                                  \
+    return;                                                                                  \
+  }
+  FORM_CASE(4, 4) FORM_CASE(5, 4) FORM_CASE(4, 5) FORM_CASE(5, 5) FORM_CASE(6, 6) FORM_CASE(8, 4)
+#undef FORM_CASE
+}
+
+void launch_eval_fp64(const TileChoice &t, int grid, size_t smem, cudaStream_t s, const EvalArgs &a) {
+#define EVAL_CASE(M_, N_)                                                                    \
+  if (t.tm == M_ && t.tn == N_) {                                                            \
+    k_eval_fp64<M_, N_><<<grid, kWarps * 32, smem, s>>>(a);                                  \
+    return;                                                                                  \
+  }
+  EVAL_CASE(1, 5) EVAL_CASE(2, 5) EVAL_CASE(2, 4) EVAL_CASE(4, 4) EVAL_CASE(2, 8) EVAL_CASE(4, 5)
+#undef EVAL_CASE
+}
+
+void set_smem_attrs(int bytes) {
+  cudaFuncSetAttribute(k_form_fp64<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_form_fp64<5, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_form_fp64<4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_form_fp64<5, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_form_fp64<6, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_form_fp64<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_eval_fp64<1, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_eval_fp64<2, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_eval_fp64<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_eval_fp64<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_eval_fp64<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_eval_fp64<4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+struct NearArgs {
+  const double *fvals;
+  double *pot;
+  const int *target, *level, *begin, *src;
+  const int2 *ixy;
+  const double *tab_loc;
+  const int *ind_loc;
+  int ntarget, nd, n;
+};
+
+// One warp per near-field target leaf; pot(k1,k2) += sum over its list1
+// entries of Ty^T (Tx^T F) on the banded 1D tables of the target's level.
+__global__ void __launch_bounds__(kWarps * 32) k_near_fp64(NearArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * kWarps + warp;
+  if (t >= a.ntarget) return;
+  const int n = a.n, npb = n * n, nd = a.nd;
+  double *wb = reinterpret_cast<double *>(smem_raw) + (size_t)warp * 3 * npb;
+  double *sF = wb, *sff = wb + npb, *sP = wb + 2 * npb;
+  const int tb = a.target[t], lev = a.level[t];
+  const size_t tsz = (size_t)npb * 13, isz = (size_t)2 * (n + 1) * 13;
+  const double *tl = a.tab_loc + tsz * lev;
+  const int *il = a.ind_loc + isz * lev;
+  for (int ind = 0; ind < nd; ind++) {
+    for (int o = lane; o < npb; o += 32) sP[o] = 0;
+    for (int e = a.begin[t]; e < a.begin[t + 1]; e++) {
+      const int sb = a.src[e];
+      const int ix = a.ixy[e].x, iy = a.ixy[e].y;
+      const int *bx = il + (size_t)2 * (n + 1) * (ix + 6);
+      const int *by = il + (size_t)2 * (n + 1) * (iy + 6);
+      const int kx0 = bx[2 * n], kx1 = bx[2 * n + 1], ky0 = by[2 * n], ky1 = by[2 * n + 1];
+      if (kx1 - kx0 + 1 == 0 || ky1 - ky0 + 1 == 0) continue;
+      const double *tx = tl + (size_t)npb * (ix + 6);
+      const double *ty = tl + (size_t)npb * (iy + 6);
+      const double *fv = a.fvals + (size_t)sb * nd * npb;
+      __syncwarp();
+      for (int o = lane; o < npb; o += 32) sF[o] = fv[ind + (size_t)nd * o];
+      __syncwarp();
+      // ff(k1, j2) for k1 in [kx0, kx1] (1-based)
+      const int nkx = kx1 - kx0 + 1;
+      for (int o = lane; o < nkx * n; o += 32) {
+        const int k1 = kx0 + o % nkx, j2 = o / nkx;
+        const int lo = bx[2 * (k1 - 1)], hi = bx[2 * (k1 - 1) + 1];
+        double cd = 0;
+        for (int j1 = lo; j1 <= hi; j1++) cd = fma(tx[(j1 - 1) + (size_t)n * (k1 - 1)], sF[(j1 - 1) + (size_t)n * j2], cd);
+        sff[(k1 - 1) + (size_t)n * j2] = cd;
+      }
+      __syncwarp();
+      const int nky = ky1 - ky0 + 1;
+      for (int o = lane; o < nkx * nky; o += 32) {
+        const int k1 = kx0 + o % nkx, k2 = ky0 + o / nkx;
+        const int lo = by[2 * (k2 - 1)], hi = by[2 * (k2 - 1) + 1];
+        double cd = 0;
+        for (int j2 = lo; j2 <= hi; j2++) cd = fma(ty[(j2 - 1) + (size_t)n * (k2 - 1)], sff[(k1 - 1) + (size_t)n * (j2 - 1)], cd);
+        sP[(k1 - 1) + (size_t)n * (k2 - 1)] += cd;
+      }
+    }
+    __syncwarp();
+    double *pb = a.pot + (size_t)tb * nd * npb;
+    for (int o = lane; o < npb; o += 32) pb[ind + (size_t)nd * o] += sP[o];
+    __syncwarp();
+  }
+}
+
+template <typename T>
+int upload(T *&dptr, const std::vector<T> &v, std::string &msg) {
+  dptr = nullptr;
+  if (v.empty()) return BFGT_OK;
+  if (cudaMalloc(&dptr, sizeof(T) * v.size()) != cudaSuccess) {
+    msg = "cudaMalloc failed (" + std::to_string(sizeof(T) * v.size()) + " bytes)";
+    return BFGT_ERR_OOM;
+  }
+  if (cudaMemcpy(dptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    msg = "cudaMemcpy to device failed";
+    return BFGT_ERR_CUDA;
+  }
+  return BFGT_OK;
+}
+
+int alloc_bytes(void **p, size_t bytes, std::string &msg) {
+  *p = nullptr;
+  if (bytes == 0) return BFGT_OK;
+  if (cudaMalloc(p, bytes) != cudaSuccess) {
+    msg = "cudaMalloc failed (" + std::to_string(bytes) + " bytes)";
+    return BFGT_ERR_OOM;
+  }
+  return BFGT_OK;
+}
+
+}  // namespace
+
+int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    msg = "no CUDA device visible";
+    return BFGT_ERR_NODEVICE;
+  }
+  cudaGetDevice(&dp.device);
+  dp.nd = hp.nd;
+  dp.n = hp.norder;
+  dp.npw = hp.npw;
+  dp.hh = hp.hh;
+  dp.nexp = hp.nexp;
+  dp.nlevels = hp.nlevels;
+  dp.nboxes = hp.nboxes;
+  dp.precision = hp.precision;
+  dp.direct_only = hp.direct_only;
+  int rc = BFGT_OK;
+  auto chk = [&](int r) {
+    if (rc == BFGT_OK && r != BFGT_OK) rc = r;
+  };
+  const int n = dp.n;
+  if (!hp.direct_only) {
+    dp.ncut = (int)hp.cut_box.size();
+    dp.nchunks = (int)hp.chunks.size();
+    dp.nleaves = (int)hp.leaves.size();
+    std::vector<double2> T(hp.tab_poly2pw.size()), E(hp.tab_pw2pot.size()), PH(hp.phase.size()), W(hp.wshift.size());
+    for (size_t i = 0; i < T.size(); i++) T[i] = make_double2(hp.tab_poly2pw[i].re, hp.tab_poly2pw[i].im);
+    for (size_t i = 0; i < E.size(); i++) E[i] = make_double2(hp.tab_pw2pot[i].re, hp.tab_pw2pot[i].im);
+    for (size_t i = 0; i < PH.size(); i++) PH[i] = make_double2(hp.phase[i].re, hp.phase[i].im);
+    for (size_t i = 0; i < W.size(); i++) W[i] = make_double2(hp.wshift[i].re, hp.wshift[i].im);
+    chk(upload(dp.T, T, msg));
+    chk(upload(dp.E, E, msg));
+    chk(upload(dp.PH, PH, msg));
+    chk(upload(dp.W, W, msg));
+    std::vector<long long> po(hp.phase_off.begin(), hp.phase_off.end());
+    chk(upload(dp.ph_off, po, msg));
+    std::vector<int4> lv(hp.leaves.size()), cv(hp.chunks.size());
+    for (size_t i = 0; i < lv.size(); i++) lv[i] = make_int4(hp.leaves[i].box, hp.leaves[i].ox, hp.leaves[i].oy, hp.leaves[i].level);
+    for (size_t i = 0; i < cv.size(); i++) cv[i] = make_int4(hp.chunks[i].begin, hp.chunks[i].end, hp.chunks[i].icut, hp.chunks[i].level);
+    chk(upload(dp.leaves, lv, msg));
+    chk(upload(dp.chunks, cv, msg));
+    chk(upload(dp.cut_chunk_begin, hp.cut_chunk_begin, msg));
+    chk(upload(dp.cut_pw_begin, hp.cut_pw_begin, msg));
+    chk(upload(dp.cut_pw_src, hp.cut_pw_src, msg));
+    chk(upload(dp.cut_pw_ind, hp.cut_pw_ind, msg));
+    chk(upload(dp.pw_weight, hp.pw_weight, msg));
+    const size_t ex = (size_t)dp.nd * dp.nexp * sizeof(double2);
+    chk(alloc_bytes((void **)&dp.Mpart, ex * dp.nchunks, msg));
+    chk(alloc_bytes((void **)&dp.M, ex * dp.ncut, msg));
+    chk(alloc_bytes((void **)&dp.L, ex * dp.ncut, msg));
+    const int npb = n * n;
+    dp.smem_form = sizeof(double2) * ((size_t)n * dp.npw +
+                                      (size_t)kWarps * ((size_t)dp.npw * dp.hh + (size_t)n * dp.hh + dp.npw + dp.hh + (npb + 1) / 2));
+    dp.smem_eval = sizeof(double2) * ((size_t)n * dp.npw + (size_t)dp.npw * dp.hh +
+                                      (size_t)kWarps * ((size_t)dp.npw * dp.hh + (size_t)n * dp.hh + dp.npw + dp.hh));
+    if (rc == BFGT_OK && dp.precision == BFGT_PREC_SPLIT) rc = split_plan_create(dp, hp, msg);
+  }
+  dp.nnf = (int)hp.nf_target.size();
+  dp.nnf_entries = (int)hp.nf_src.size();
+  if (dp.nnf > 0) {
+    std::vector<int2> ixy(hp.nf_src.size());
+    for (size_t i = 0; i < ixy.size(); i++) ixy[i] = make_int2(hp.nf_ix[i], hp.nf_iy[i]);
+    chk(upload(dp.nf_target, hp.nf_target, msg));
+    chk(upload(dp.nf_level, hp.nf_level, msg));
+    chk(upload(dp.nf_begin, hp.nf_begin, msg));
+    chk(upload(dp.nf_src, hp.nf_src, msg));
+    chk(upload(dp.nf_ixy, ixy, msg));
+    chk(upload(dp.tab_loc, hp.tab_loc, msg));
+    chk(upload(dp.ind_loc, hp.ind_loc, msg));
+    dp.smem_near = sizeof(double) * (size_t)kWarps * 3 * n * n;
+  }
+  const size_t smax = 227 * 1024;
+  if (rc == BFGT_OK && (dp.smem_form > smax || dp.smem_eval > smax || dp.smem_near > smax)) {
+    msg = "npw/norder need more than 227 KB of shared memory per block";
+    rc = BFGT_ERR_CAPACITY;
+  }
+  if (rc == BFGT_OK) {
+    set_smem_attrs((int)smax);
+    cudaFuncSetAttribute(k_near_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+    for (int i = 0; i < 8; i++) cudaEventCreate(&dp.ev[i]);
+    dp.events = true;
+    if (cudaGetLastError() != cudaSuccess) {
+      msg = "CUDA error while creating the plan";
+      rc = BFGT_ERR_CUDA;
+    }
+  }
+  return rc;
+}
+
+void device_plan_destroy(DevicePlan &dp) {
+  if (dp.graph_exec) cudaGraphExecDestroy(dp.graph_exec);
+  if (dp.graph) cudaGraphDestroy(dp.graph);
+  void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.cut_chunk_begin, dp.cut_pw_begin,
+                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.Mpart, dp.M, dp.L, dp.Tsplit, dp.Esplit,
+                  dp.Tscale, dp.Escale, dp.nf_target, dp.nf_level, dp.nf_begin, dp.nf_src, dp.nf_ixy,
+                  dp.tab_loc, dp.ind_loc, dp.d_stage_f, dp.d_stage_p};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (dp.h_stage_f) cudaFreeHost(dp.h_stage_f);
+  if (dp.h_stage_p) cudaFreeHost(dp.h_stage_p);
+  if (dp.events)
+    for (int i = 0; i < 8; i++) cudaEventDestroy(dp.ev[i]);
+  dp = DevicePlan();
+}
+
+int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cudaStream_t s, std::string &msg) {
+  const int nthreads = kWarps * 32;
+  if (dp.events) cudaEventRecord(dp.ev[0], s);
+  if (!dp.direct_only && dp.nchunks > 0) {
+    if (dp.precision == BFGT_PREC_SPLIT) {
+      split_form(dp, d_fvals, s);
+    } else {
+      FormArgs fa{d_fvals, dp.leaves, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
+      launch_form_fp64(best_tile(dp.npw, dp.hh, kFormTiles, 6), dp.nchunks, dp.smem_form, s, fa);
+    }
+    if (dp.events) cudaEventRecord(dp.ev[1], s);
+    const int zb = (dp.nexp + 255) / 256;
+    k_reduce<<<dim3(dp.ncut, dp.nd, zb), 256, 0, s>>>(dp.Mpart, dp.cut_chunk_begin, dp.M, dp.nd, dp.nexp);
+    if (dp.events) cudaEventRecord(dp.ev[2], s);
+    k_translate<<<dim3(dp.ncut, dp.nd, zb), 256, 0, s>>>(dp.M, dp.cut_pw_begin, dp.cut_pw_src, dp.cut_pw_ind,
+                                                         dp.W, dp.L, dp.nd, dp.nexp);
+    if (dp.events) cudaEventRecord(dp.ev[3], s);
+    if (dp.precision == BFGT_PREC_SPLIT) {
+      split_eval(dp, d_pot, s);
+    } else {
+      EvalArgs ea{d_pot, dp.leaves, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
+      launch_eval_fp64(best_tile(dp.n, dp.hh, kEvalTiles, 6), dp.nchunks, dp.smem_eval, s, ea);
+    }
+    if (dp.events) cudaEventRecord(dp.ev[4], s);
+  } else if (dp.events) {
+    for (int i = 1; i <= 4; i++) cudaEventRecord(dp.ev[i], s);
+  }
+  if (dp.nnf > 0) {
+    NearArgs na{d_fvals, d_pot, dp.nf_target, dp.nf_level, dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc,
+                dp.ind_loc, dp.nnf, dp.nd, dp.n};
+    k_near_fp64<<<(dp.nnf + kWarps - 1) / kWarps, nthreads, dp.smem_near, s>>>(na);
+  }
+  if (dp.events) cudaEventRecord(dp.ev[5], s);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    msg = std::string("kernel launch failed: ") + cudaGetErrorString(e);
+    return BFGT_ERR_CUDA;
+  }
+  return BFGT_OK;
+}
+
+}  // namespace bfgt

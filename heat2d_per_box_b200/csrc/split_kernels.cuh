@@ -1,0 +1,18 @@
+// Split-precision (tensor-core) variants of the plane-wave kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "device_plan.hpp"
+
+namespace bfgt {
+
+// Uploads the FP16 operand slices of the level tables; BFGT_* status.
+int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);
+// leaf values -> partial cutoff expansions (same output as k_form_fp64)
+void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s);
+// cutoff expansions -> leaf values, accumulated into pot (same as k_eval_fp64)
+void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s);
+
+}  // namespace bfgt

@@ -1,0 +1,151 @@
+/*
+ * bfgt.h -- C ABI of the B200 box fast Gauss transform (libbfgt_b200.so).
+ *
+ * The drop-in entry point is boxfgt_, the symbol gfortran emits for
+ *   call boxfgt(nd,ndim,delta,eps,ipoly,iperiod,norder,npbox,nboxes,nlevels,
+ *               ltree,itree,iptr,centers,boxsize,fvals,ifpgh,pot,grad,hess,
+ *               ifnewtree,ntarg,targs,ifpghtarg,pote,grade,hesse,timeinfo)
+ * (bfgt/boxfgt.f:5-8).  Every argument is passed by reference, integers are
+ * 32-bit, reals are double, arrays are Fortran column-major, and there are no
+ * hidden character-length arguments.  All arrays are host memory owned by the
+ * caller, exactly as for the Fortran routine.
+ *
+ * The plan API (bfgt_plan_*) is the device-resident form of the same
+ * transform: the tree-dependent precomputation (boxfgt.f step 0) is done once
+ * and the transform runs on device pointers, on a caller-supplied stream.
+ *
+ * Errors: the reference routine has no error argument.  boxfgt_ keeps the void
+ * signature and records failures in bfgt_last_error(); when the environment
+ * variable BFGT_ABORT_ON_ERROR is set it prints the message and aborts instead
+ * of returning with pot untouched.  The bfgt_* functions return one of the
+ * BFGT_* status codes below.
+ */
+#ifndef BFGT_H
+#define BFGT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define BFGT_OK 0
+#define BFGT_ERR_ARG 1          /* unsupported or inconsistent argument       */
+#define BFGT_ERR_TREE 2         /* tree arrays are not a valid 2:1 quad tree  */
+#define BFGT_ERR_CAPACITY 3     /* npw, norder or nd beyond the built kernels */
+#define BFGT_ERR_OOM 4          /* device allocation failed                  */
+#define BFGT_ERR_CUDA 5         /* a CUDA runtime call failed                */
+#define BFGT_ERR_NODEVICE 6     /* no CUDA device visible                     */
+#define BFGT_ERR_TIMEOUT 7      /* a bounded device-side wait gave up         */
+
+/* precision modes of a plan */
+#define BFGT_PREC_FP64 0        /* every contraction in FP64                   */
+#define BFGT_PREC_SPLIT 1       /* tensor-core split-FP16 slices, FP32 accum.,
+                                   FP64 phases and FP64 cross-leaf accumulation */
+
+/* Replaces bfgt/boxfgt.f:5-286 (boxfgt).  Supported: ndim=2, ifpgh=1,
+   ifnewtree=0, ifpghtarg=0 (the configuration every solver in the reference
+   uses, hpots/hpots2dadap.f:79-106).  pot is accumulated into, on leaf boxes
+   only; the colleague arrays itree(iptr(6)), itree(iptr(7)) are recomputed as
+   the reference does (boxfgt.f:516-528); timeinfo(1:20) is zeroed and filled
+   with per-stage seconds. */
+void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *eps, const int *ipoly,
+             int *iperiod, const int *norder, const int *npbox, int *nboxes, int *nlevels, int *ltree,
+             int *itree, int *iptr, double *centers, double *boxsize, const double *fvals, const int *ifpgh,
+             double *pot, double *grad, double *hess, const int *ifnewtree, const int *ntarg,
+             const double *targs, const int *ifpghtarg, double *pote, double *grade, double *hesse,
+             double *timeinfo);
+
+/* Last error message of this thread ("" when the last call succeeded). */
+const char *bfgt_last_error(void);
+
+/* Same as boxfgt_ with values instead of references and a precision mode.
+   Replaces bfgt/boxfgt.f:5-286 for callers that are not Fortran. Returns a
+   BFGT_* status. */
+int bfgt_boxfgt(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
+                int ltree, int *itree, const int *iptr, const double *centers, const double *boxsize,
+                const double *fvals, double *pot, double *timeinfo, int precision);
+
+/* ---- plan API (device-resident boxfgt) ---------------------------------- */
+typedef struct bfgt_plan_s *bfgt_plan;
+
+/* Builds the step-0 precomputation of bfgt/boxfgt.f:472-703 (cutoff level,
+   plane-wave nodes, 1D tables, interaction lists) for one tree, delta, eps,
+   norder, ipoly and nd, and uploads it to the current CUDA device.  itree's
+   colleague arrays are recomputed in place as boxfgt does. */
+int bfgt_plan_create(bfgt_plan *plan, int nd, double delta, double eps, int ipoly, int iperiod, int norder,
+                     int nboxes, int nlevels, int ltree, int *itree, const int *iptr, const double *centers,
+                     const double *boxsize, int precision);
+
+/* Steps 1-6 of bfgt/boxfgt.f:720-1071 on device arrays laid out as
+   fvals(nd,norder**2,nboxes) and pot(nd,norder**2,nboxes); pot is accumulated
+   into on leaf boxes.  stream is a cudaStream_t (NULL = default stream).
+   Asynchronous: returns after the launches are queued. */
+int bfgt_plan_execute(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream);
+
+/* Same transform on host arrays: uploads the leaf values, runs, and adds the
+   result into the host pot (the reference-facing form of a planned call). */
+int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, void *stream);
+
+/* Capture bfgt_plan_execute for these device buffers into a CUDA graph and
+   replay it with bfgt_plan_graph_launch. */
+int bfgt_plan_graph_capture(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream);
+int bfgt_plan_graph_launch(bfgt_plan plan, void *stream);
+
+/* Per-stage device milliseconds of the last bfgt_plan_execute on this plan
+   (CUDA events; the stage order matches timeinfo(2:7)). out must hold 8. */
+int bfgt_plan_stage_ms(bfgt_plan plan, double *out);
+
+/* Plan scalars: out[0]=npwlevel (boxfgt.f:137-150), out[1]=npw, out[2]=nlevstart,
+   out[3]=nlevend, out[4]=regime (0 periodic Fourier, 1 PW + near field,
+   2 near field only), out[5]=nleafbox, out[6]=number of PW leaves,
+   out[7]=number of near-field target leaves, out[8]=number of near-field
+   interactions, out[9]=mnlist1, out[10]=internal iperiod, out[11]=nchunks.
+   out must hold 16 ints. */
+int bfgt_plan_info(bfgt_plan plan, int *out);
+
+/* Algorithmic FP64 work of one execute: out[0]=FLOP, out[1]=compulsory HBM
+   bytes (leaf fvals read + pot read/write), out[2]=tensor-core FLOP issued
+   (split mode; counts every slice product), out[3]=leaf points x nd. */
+int bfgt_plan_work(bfgt_plan plan, double *out);
+
+int bfgt_plan_destroy(bfgt_plan plan);
+
+/* ---- host-side plan introspection (no device needed) ------------------- */
+/* Builds only the host half of a plan (tables and lists) and copies out the
+   interaction lists and near-field band patterns so that they can be compared
+   bit for bit with another implementation of bfgt/boxfgt.f step 0.  Any output
+   pointer may be NULL.  list1 is written as list1(mnlist1_cap, nboxes), listpw
+   as listpw(8, nboxes), ind_loc as ind_loc(2, norder+1, -6:6, 0:nlevels) and
+   tab_loc as tab_loc(norder, norder, -6:6, 0:nlevels). info as bfgt_plan_info. */
+int bfgt_host_plan_dump(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes,
+                        int nlevels, int ltree, int *itree, const int *iptr, const double *centers,
+                        const double *boxsize, int *info, int *ifpwexp, int *nlist1, int *list1,
+                        int mnlist1_cap, int *nlistpw, int *listpw, int *ind_loc, double *tab_loc, double *ts,
+                        double *ws);
+
+/* ---- caller-side tree generator ---------------------------------------- */
+/* Adaptive level-restricted quad tree on [-L/2,L/2]^2 resolving
+   f(x) = sum_g a_g exp(-|x-c_g|^2 / w_g^2) (gauss: ng rows of {cx,cy,w,a}),
+   with the tail criterion of common/tree_vol_coeffs_nd.f:689-780 (iptype=2,
+   given eta) and 2:1 balance, as vol_tree_build (tree_vol_coeffs_nd.f:440)
+   produces; maxlev caps the depth (0 = no cap), minlev forces uniform
+   refinement down to that level.  Returns a handle; sizes via
+   bfgt_tree_sizes, arrays via bfgt_tree_export (itree(ltree), iptr(8),
+   centers(2,nboxes), boxsize(0:nlevels), fvals(nd=1,norder**2,nboxes)). */
+typedef struct bfgt_tree_s *bfgt_tree;
+int bfgt_tree_build_gauss(bfgt_tree *tree, int ipoly, int iperiod, double eps, double boxlen, int norder,
+                          double eta, int ng, const double *gauss, int minlev, int maxlev);
+/* Uniform tree of depth nlev (4**nlev leaves), f evaluated as above. */
+int bfgt_tree_build_uniform(bfgt_tree *tree, int ipoly, int iperiod, double boxlen, int norder, int nlev,
+                            int ng, const double *gauss);
+int bfgt_tree_sizes(bfgt_tree tree, int *nboxes, int *nlevels, int *ltree);
+int bfgt_tree_export(bfgt_tree tree, int *itree, int *iptr, double *centers, double *boxsize, double *fvals);
+int bfgt_tree_free(bfgt_tree tree);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

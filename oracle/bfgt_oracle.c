@@ -1,0 +1,1612 @@
+/*
+ * CPU oracle for the 2D periodic/free-space box fast Gauss transform.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is a line-by-line C restatement of the
+ * reference Fortran (Jsu1029/heat2d_per_box) for ndim=2, ifpgh=1, ifnewtree=0,
+ * ifpghtarg=0.  It is linked only by the tests, by __graft_entry__.smoke() as
+ * the checker, and by bench.py's CPU-baseline leg.  The product library never
+ * links or calls it.
+ *
+ * Followed files (paths inside the reference project):
+ *   bfgt/boxfgt.f        boxfgt 5-286, bfgtmain 291-1591, gnd_mpalloc 1598-1702
+ *   bfgt/bfgt_pwrouts.f  g2d_tens_prod_to_pw 98-147, g2d_pw2pot 549-602,
+ *                        g2d_mk_pw_translation_matrices 1415-1471,
+ *                        g2d_mk_merge_split_pw_matrices 1645-1703,
+ *                        gnd_shiftpw 1798-1844, gnd_find_pwshift_ind 1848-1892,
+ *                        gnd_shiftpw_loc 1905-1941, gnd_find_msshift_ind 1946-1976,
+ *                        gnd_copy_pwexp 1987-2015, gnd_pwzero 2021-2046
+ *   bfgt/bfgt_local.f    g2d_tens_prod_to_potloc 315-375, gnd_find_loctab_ind 1729-1765
+ *   bfgt/bfgt_volrouts.f mk_leg2pw_tables 58-143, mk_cheb2pw_tables 151-275,
+ *                        mk_pw2pgh_tables 339-401, mk_loctab_all 407-660,
+ *                        mk_loctab 920-1060, mk_legetab_recur 1095-1187,
+ *                        mk_chebtab_recur 1191-1294, compute_sparse_pattern 1300-1378
+ *   common/fgtterms.f    fgtpwterms 72-141, get_pwnodes 151-179, get_periodic_pwnodes 189-209
+ *   common/legeexps.f    legeexps 141-215, legepol 522-555, legepols 597-630,
+ *                        legerts 2399-2530, legetayl 2536-2590
+ *   common/chebexps.f    chebexps 12-180, chebpols 594-625
+ *   common/besseljs3d.f  besseljs3d 5-169 (real argument)
+ *   common/lapack_f77.f  dgemm_f77 'T','N' branch
+ *   common/tree_routs_nd.f computecoll 106-250, compute_mnlist1 493-600,
+ *                        gnd_compute_modified_list1 864-1050,
+ *                        gnd_find_pwexp_boxes 1266-1367, gnd_compute_listpw 1564-1615
+ *
+ * Arrays use the reference's Fortran (column-major, 1-based) layout through
+ * the index macros below, so the restatement can be read against the source.
+ * Compile without -ffast-math and with -ffp-contract=off.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct { double re, im; } zc;
+
+static inline zc zmk(double re, double im) { zc r; r.re = re; r.im = im; return r; }
+static inline zc zadd(zc a, zc b) { return zmk(a.re + b.re, a.im + b.im); }
+static inline zc zmul(zc a, zc b) { return zmk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+static inline zc zconj(zc a) { return zmk(a.re, -a.im); }
+static inline zc zexpi(double x) { return zmk(cos(x), sin(x)); } /* exp(i*x) */
+static inline zc zscal(zc a, double s) { return zmk(a.re * s, a.im * s); }
+
+static double wtime(void) {
+#ifdef _OPENMP
+  return omp_get_wtime();
+#else
+  return 0.0;
+#endif
+}
+
+/* ------------------------------------------------------------------------- */
+/* Legendre / Chebyshev helpers (common/legeexps.f, common/chebexps.f)       */
+/* ------------------------------------------------------------------------- */
+
+static void legepol(double x, int n, double *pol, double *der) {
+  double pkm1, pk = 1, pkp1 = x;
+  if (n < 2) {
+    if (n == 0) { *pol = 1; *der = 0; return; }
+    *pol = x; *der = 1; return;
+  }
+  for (int k = 1; k <= n - 1; k++) {
+    pkm1 = pk;
+    pk = pkp1;
+    pkp1 = ((2 * k + 1) * x * pk - k * pkm1) / (k + 1);
+  }
+  *pol = pkp1;
+  *der = n * (x * pkp1 - pk) / (x * x - 1);
+}
+
+static void legetayl(double pol, double der, double x, double h, int n, int k,
+                     double *sum, double *sumder) {
+  double done = 1;
+  double q0 = pol, q1 = der * h;
+  double q2 = (2 * x * der - n * (n + done) * pol) / (1 - x * x);
+  q2 = q2 * (h * h) / 2;
+  *sum = q0 + q1 + q2;
+  *sumder = q1 / h + q2 * 2 / h;
+  if (k <= 2) return;
+  double qi = q1, qip1 = q2, qip2, d;
+  for (int i = 1; i <= k - 2; i++) {
+    d = 2 * x * ((i + 1) * (i + 1)) / h * qip1 - (n * (n + done) - i * (i + 1)) * qi;
+    d = d / (i + 1) / (i + 2) * (h * h) / (1 - x * x);
+    qip2 = d;
+    *sum = *sum + qip2;
+    *sumder = *sumder + d * (i + 2) / h;
+    qi = qip1;
+    qip1 = qip2;
+  }
+}
+
+/* Gauss-Legendre nodes (ascending) and weights, legeexps.f:2399-2530 */
+static void legerts(int itype, int n, double *ts, double *whts) {
+  int k = 30;
+  double d = 1, d2 = d + 1.0e-24;
+  if (d2 != d) k = 54;
+  int i = n / 2;
+  int ifodd = n - 2 * i;
+  double done = 1, pi = atan(done) * 4, h = pi / (2 * n);
+  /* ts has room for n+1 entries: the reference reads ts(kk+1) once past the
+     initial guesses on its final sweep and discards it. */
+  int ii = 0;
+  for (i = 1; i <= n; i++) {
+    if (i < n / 2 + 1) continue;
+    ii++;
+    double t = (2 * i - 1) * h;
+    ts[ii - 1] = -cos(t);
+  }
+  double pol = 1, der = 0, x0 = 0;
+  legepol(x0, n, &pol, &der);
+  double x1 = ts[0];
+  int n2 = (n + 1) / 2;
+  double pol3 = pol, der3 = der;
+  for (int kk = 1; kk <= n2; kk++) {
+    if (ifodd == 1 && kk == 1) {
+      ts[kk - 1] = x0;
+      whts[kk - 1] = der;
+      x0 = x1;
+      x1 = ts[kk];
+      pol3 = pol;
+      der3 = der;
+      continue;
+    }
+    int ifstop = 0;
+    for (i = 1; i <= 10; i++) {
+      double hh = x1 - x0;
+      legetayl(pol3, der3, x0, hh, n, k, &pol, &der);
+      x1 = x1 - pol / der;
+      if (fabs(pol) < 1.0e-12) ifstop++;
+      if (ifstop == 3) break;
+    }
+    ts[kk - 1] = x1;
+    if (itype > 0) whts[kk - 1] = der;
+    x0 = x1;
+    x1 = ts[kk];
+    pol3 = pol;
+    der3 = der;
+  }
+  for (i = (n + 1) / 2; i >= 1; i--) ts[i + n / 2 - 1] = ts[i - 1];
+  for (i = 1; i <= n / 2; i++) ts[i - 1] = -ts[n - i];
+  if (itype <= 0) return;
+  for (i = (n + 1) / 2; i >= 1; i--) whts[i + n / 2 - 1] = whts[i - 1];
+  for (i = 1; i <= n / 2; i++) whts[i - 1] = whts[n - i];
+  for (i = 1; i <= n; i++) whts[i - 1] = 2 / (1 - ts[i - 1] * ts[i - 1]) / (whts[i - 1] * whts[i - 1]);
+}
+
+static void legepols(double x, int n, double *pols) {
+  double pkm1, pk = 1, pkp1 = x;
+  if (n < 2) {
+    pols[0] = 1;
+    if (n == 0) return;
+    pols[1] = x;
+    return;
+  }
+  pols[0] = 1;
+  pols[1] = x;
+  for (int k = 1; k <= n - 1; k++) {
+    pkm1 = pk;
+    pk = pkp1;
+    pkp1 = ((2 * k + 1) * x * pk - k * pkm1) / (k + 1);
+    pols[k + 1] = pkp1;
+  }
+}
+
+static void chebpols(double x, int n, double *pols) {
+  double pkm1, pk = 1, pkp1 = x;
+  if (n < 2) {
+    pols[0] = 1;
+    if (n == 0) return;
+    pols[1] = x;
+    return;
+  }
+  pols[0] = 1;
+  pols[1] = x;
+  for (int k = 1; k <= n - 1; k++) {
+    pkm1 = pk;
+    pk = pkp1;
+    pkp1 = 2 * x * pk - pkm1;
+    pols[k + 1] = pkp1;
+  }
+}
+
+#define M2(a, ld, i, j) (a)[((i) - 1) + (size_t)((j) - 1) * (ld)]
+
+/* legeexps.f:141-215.  u: values->coefficients, v: coefficients->values. */
+static void legeexps(int itype, int n, double *x, double *u, double *v, double *whts) {
+  int itype_rts = 0;
+  if (itype > 0) itype_rts = 1;
+  double *tsbuf = (double *)malloc(sizeof(double) * (n + 2));
+  double *wbuf = (double *)malloc(sizeof(double) * (n + 2));
+  legerts(itype_rts, n, tsbuf, wbuf);
+  for (int i = 0; i < n; i++) { x[i] = tsbuf[i]; if (whts && itype > 0) whts[i] = wbuf[i]; }
+  if (itype != 2) { free(tsbuf); free(wbuf); return; }
+  for (int i = 1; i <= n; i++) legepols(x[i - 1], n - 1, &M2(u, n, 1, i));
+  for (int i = 1; i <= n; i++)
+    for (int j = 1; j <= n; j++) M2(v, n, i, j) = M2(u, n, j, i);
+  for (int i = 1; i <= n; i++) {
+    double d = 1;
+    d = d * (2 * i - 1) / 2;
+    for (int j = 1; j <= n; j++) M2(u, n, i, j) = M2(v, n, j, i) * wbuf[j - 1] * d;
+  }
+  free(tsbuf);
+  free(wbuf);
+}
+
+/* chebexps.f:12-180.  Chebyshev nodes of the first kind, ascending. */
+static void chebexps(int itype, int n, double *x, double *u, double *v, double *whts) {
+  double done = 1;
+  double pi = atan(done) * 4;
+  double h = pi / (2 * n);
+  for (int i = 1; i <= n; i++) {
+    double t = (2 * i - 1) * h;
+    x[n - i] = cos(t);
+  }
+  if (itype == 0) return;
+  double *w = whts;
+  double *wtmp = NULL;
+  if (!w) { wtmp = (double *)malloc(sizeof(double) * n); w = wtmp; }
+  if (itype > 1) {
+    for (int i = 1; i <= n; i++) {
+      M2(u, n, 1, i) = 1;
+      M2(u, n, 2, i) = x[i - 1];
+    }
+  }
+  for (int i = 1; i <= n; i++) {
+    double tjm2 = 1, tjm1 = x[i - 1], tj;
+    w[i - 1] = 2;
+    int ic = -1;
+    for (int j = 2; j <= n - 1; j++) {
+      tj = 2 * x[i - 1] * tjm1 - tjm2;
+      if (itype == 2) M2(u, n, j + 1, i) = tj;
+      tjm2 = tjm1;
+      tjm1 = tj;
+      ic = -ic;
+      if (ic < 0) continue;
+      double rint = -2 * (done / (j + 1) - done / (j - 1));
+      w[i - 1] = w[i - 1] - rint * tj;
+    }
+    w[i - 1] = w[i - 1] / n;
+  }
+  if (wtmp) free(wtmp);
+  if (itype != 2) return;
+  for (int i = 1; i <= n; i++) {
+    double d = 0;
+    for (int j = 1; j <= n; j++) d = d + M2(u, n, i, j) * M2(u, n, i, j);
+    d = done / sqrt(d);
+    for (int j = 1; j <= n; j++) M2(u, n, i, j) = M2(u, n, i, j) * d;
+  }
+  double ddd = 2;
+  ddd = sqrt(ddd);
+  double dd = n;
+  dd = done / sqrt(dd / 2);
+  for (int i = 1; i <= n; i++) {
+    for (int j = 1; j <= n; j++) M2(u, n, j, i) = M2(u, n, j, i) * dd;
+    M2(u, n, 1, i) = M2(u, n, 1, i) / ddd;
+  }
+  dd = n;
+  dd = dd / 2;
+  for (int i = 1; i <= n; i++)
+    for (int j = 1; j <= n; j++) M2(v, n, j, i) = M2(u, n, i, j) * dd;
+  for (int i = 1; i <= n; i++)
+    for (int j = 1; j <= n; j++) {
+      double d = M2(v, n, j, i);
+      M2(v, n, j, i) = M2(u, n, j, i) * n / 2;
+      M2(u, n, j, i) = d / n * 2;
+    }
+  for (int i = 1; i <= n; i++) M2(v, n, 1, i) = M2(v, n, 1, i) * 2;
+  for (int i = 1; i <= n; i++)
+    for (int j = 1; j <= i - 1; j++) {
+      double d = M2(u, n, j, i);
+      M2(u, n, j, i) = M2(u, n, i, j);
+      M2(u, n, i, j) = d;
+      d = M2(v, n, j, i);
+      M2(v, n, j, i) = M2(v, n, i, j);
+      M2(v, n, i, j) = d;
+    }
+}
+
+/* Spherical Bessel j_0..j_nterms at a real argument (besseljs3d.f:5-169;
+   the reference evaluates it at a complex argument with zero imaginary part,
+   for which every complex operation reduces to the real one used here). */
+static void besseljs3d_real(int nterms, double z, double scale, double *fjs) {
+  const double upbound2 = 1.0e+40, upbound2inv = 1.0e-40, tiny = 1.0e-200, done = 1.0;
+  if (fabs(z) < tiny) {
+    fjs[0] = done;
+    for (int i = 1; i <= nterms; i++) fjs[i] = 0;
+    return;
+  }
+  double zinv = done / z;
+  double fjm1 = 0, fj0 = done, fj1;
+  int lwfjs = nterms + 100000;
+  int ntop = lwfjs;
+  for (int i = nterms; i <= lwfjs; i++) {
+    double dcoef = 2 * i + done;
+    fj1 = dcoef * zinv * fj0 - fjm1;
+    double dd = fj1 * fj1;
+    if (dd > upbound2) { ntop = i + 1; break; }
+    fjm1 = fj0;
+    fj0 = fj1;
+  }
+  int *iscale = (int *)calloc((size_t)ntop + 1, sizeof(int));
+  double *fjtmp = (double *)malloc(sizeof(double) * ((size_t)ntop + 1));
+  fjtmp[ntop] = 0;
+  fjtmp[ntop - 1] = done;
+  for (int i = ntop - 1; i >= 1; i--) {
+    double dcoef = 2 * i + done;
+    fjtmp[i - 1] = dcoef * zinv * fjtmp[i] - fjtmp[i + 1];
+    double dd = fjtmp[i - 1] * fjtmp[i - 1];
+    if (dd > upbound2) {
+      fjtmp[i] = fjtmp[i] * upbound2inv;
+      fjtmp[i - 1] = fjtmp[i - 1] * upbound2inv;
+      iscale[i] = 1;
+    }
+  }
+  double scalinv = done / scale, sctot = 1.0;
+  for (int i = 1; i <= ntop; i++) {
+    sctot = sctot * scalinv;
+    if (iscale[i - 1] == 1) sctot = sctot * upbound2inv;
+    fjtmp[i] = fjtmp[i] * sctot;
+  }
+  fj0 = sin(z) * zinv;
+  fj1 = fj0 * zinv - cos(z) * zinv;
+  double d0 = fabs(fj0), d1 = fabs(fj1), zscale;
+  if (d1 > d0) zscale = fj1 / (fjtmp[1] * scale);
+  else zscale = fj0 / fjtmp[0];
+  for (int i = 0; i <= nterms; i++) fjs[i] = fjtmp[i] * zscale;
+  free(iscale);
+  free(fjtmp);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Plane-wave term counts and nodes (common/fgtterms.f)                       */
+/* ------------------------------------------------------------------------- */
+
+static void fgtpwterms(double bsize, double delta, double eps, int iperiod, double *pmax, int *npw) {
+  double pi = 4.0 * atan(1.0);
+  if (iperiod == 0) {
+    double rmax = bsize / sqrt(delta);
+    double d = sqrt(log(1.0 / eps));
+    *pmax = 2.0 * d;
+    double h = 2 * pi / (rmax + d);
+    int n = (int)(*pmax / h) + 1;
+    *npw = 2 * n;
+  } else {
+    *npw = 2 * ((int)(bsize * sqrt(log(1.0 / eps) / delta) / pi) + 1) + 1;
+  }
+}
+
+/* midpoint rule (itype=0) or trapezoid (itype=1); ts/ws indexed 0..npw-1 <-> j=-npw/2..npw/2-1 */
+static void get_pwnodes(int itype, double pmax, int npw, double *ws, double *ts) {
+  double pi = 4.0 * atan(1.0);
+  int npw2 = npw / 2;
+  double h = pmax / npw2;
+  double w = h / (2.0 * sqrt(pi));
+  for (int j = -npw2; j <= npw2 - 1; j++) {
+    int idx = j + npw2;
+    if (itype == 1) ts[idx] = j * h;
+    else ts[idx] = (j + 0.5) * h;
+    ws[idx] = w * exp(-ts[idx] * ts[idx] / 4);
+  }
+}
+
+static void get_periodic_pwnodes(double bsize0, double delta, double eps, int npw, double *ws, double *ts) {
+  (void)eps;
+  double pi = 4.0 * atan(1.0);
+  int npw2 = npw / 2;
+  double h = 2 * pi / bsize0;
+  double w = sqrt(pi * delta) / bsize0;
+  double hw = h * sqrt(delta) / 2;
+  for (int j = -npw2; j <= (npw - 1) / 2; j++) {
+    int idx = j + npw2;
+    ts[idx] = j * h;
+    ws[idx] = w * exp(-(hw * j) * (hw * j));
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* 1D tables (bfgt/bfgt_volrouts.f)                                          */
+/* ------------------------------------------------------------------------- */
+
+#define ZT(t, n, m, j) (t)[((m) - 1) + (size_t)((j) - 1) * (n)]
+
+static void mk_leg2pw_tables(int n, int npw, const double *ws, const double *ts, double delta,
+                             double boxdim, zc *tab) {
+  zc *tabtemp = (zc *)calloc((size_t)n * npw, sizeof(zc));
+  double *xq = malloc(sizeof(double) * n), *wq = malloc(sizeof(double) * n);
+  double *u = malloc(sizeof(double) * n * n), *v = malloc(sizeof(double) * n * n);
+  double *fjs = malloc(sizeof(double) * (n + 1));
+  double scale = 1.0;
+  zc eye = zmk(0, 1);
+  double fac = boxdim / (2 * sqrt(delta));
+  for (int j = npw / 2 + 1; j <= npw; j++) {
+    double dd = ws[j - 1] * boxdim;
+    if (fabs(ts[j - 1]) < 1e-12) {
+      ZT(tabtemp, n, 1, j) = zmk(dd, 0);
+      for (int m = 2; m <= n; m++) ZT(tabtemp, n, m, j) = zmk(0, 0);
+    } else {
+      double z = ts[j - 1] * fac;
+      besseljs3d_real(n, z, scale, fjs);
+      zc eyem = zmk(1, 0);
+      for (int m = 1; m <= n; m++) {
+        /* dd*fjs(m-1)/eyem with eyem = i^(m-1): exact division by a unit */
+        double val = dd * fjs[m - 1];
+        zc t;
+        switch ((m - 1) & 3) {
+          case 0: t = zmk(val, 0); break;
+          case 1: t = zmk(0, -val); break;
+          case 2: t = zmk(-val, 0); break;
+          default: t = zmk(0, val); break;
+        }
+        ZT(tabtemp, n, m, j) = t;
+        ZT(tabtemp, n, m, npw - j + 1) = zconj(t);
+        eyem = zmul(eyem, eye);
+      }
+    }
+  }
+  legeexps(2, n, xq, u, v, wq);
+  for (int i = 1; i <= npw; i++)
+    for (int j = 1; j <= n; j++) {
+      zc cd = zmk(0, 0);
+      for (int k = 1; k <= n; k++) cd = zadd(cd, zscal(ZT(tabtemp, n, k, i), M2(u, n, k, j)));
+      ZT(tab, n, j, i) = cd;
+    }
+  free(tabtemp); free(xq); free(wq); free(u); free(v); free(fjs);
+}
+
+static void mk_cheb2pw_tables(int n, int npw, const double *ws, const double *ts, double delta,
+                              double boxdim, zc *tab) {
+  zc *tabtemp = (zc *)calloc((size_t)n * npw, sizeof(zc));
+  double *fjs = malloc(sizeof(double) * (n + 1));
+  double *xq = malloc(sizeof(double) * n), *wq = malloc(sizeof(double) * n);
+  double *u = malloc(sizeof(double) * n * n), *v = malloc(sizeof(double) * n * n);
+  double *chebv = malloc(sizeof(double) * n * n), *whts = malloc(sizeof(double) * n);
+  double *xnodes = malloc(sizeof(double) * n);
+  zc *legv = malloc(sizeof(zc) * n);
+  legeexps(2, n, xnodes, u, v, whts);
+  for (int i = 1; i <= n; i++) chebpols(xnodes[i - 1], n - 1, &M2(chebv, n, 1, i));
+  for (int j = 1; j <= n; j++)
+    for (int i = 1; i <= n; i++) {
+      double dd = 0;
+      for (int k = 1; k <= n; k++) dd = dd + M2(u, n, j, k) * M2(chebv, n, i, k);
+      M2(v, n, j, i) = dd;
+    }
+  double scale = 1.0;
+  double fac = boxdim / (2 * sqrt(delta));
+  for (int j = npw / 2 + 1; j <= npw; j++) {
+    double dd = ws[j - 1] * boxdim;
+    if (fabs(ts[j - 1]) < 1e-12) {
+      for (int m = 0; m <= n - 1; m += 2) ZT(tabtemp, n, m + 1, j) = zmk(dd / (1.0 - m * m), 0);
+      for (int m = 1; m <= n - 1; m += 2) ZT(tabtemp, n, m + 1, j) = zmk(0, 0);
+    } else {
+      double z = ts[j - 1] * fac;
+      besseljs3d_real(n, z, scale, fjs);
+      for (int m = 1; m <= n; m++) {
+        double val = dd * fjs[m - 1];
+        switch ((m - 1) & 3) {
+          case 0: legv[m - 1] = zmk(val, 0); break;
+          case 1: legv[m - 1] = zmk(0, -val); break;
+          case 2: legv[m - 1] = zmk(-val, 0); break;
+          default: legv[m - 1] = zmk(0, val); break;
+        }
+      }
+      for (int i = 1; i <= n; i++) {
+        zc cd = zmk(0, 0);
+        for (int k = 1; k <= n; k++) cd = zadd(cd, zscal(legv[k - 1], M2(v, n, k, i)));
+        ZT(tabtemp, n, i, j) = cd;
+      }
+    }
+    if (j != npw - j + 1)
+      for (int i = 1; i <= n; i++) ZT(tabtemp, n, i, npw - j + 1) = zconj(ZT(tabtemp, n, i, j));
+  }
+  chebexps(2, n, xq, u, v, wq);
+  for (int i = 1; i <= npw; i++)
+    for (int j = 1; j <= n; j++) {
+      zc cd = zmk(0, 0);
+      for (int k = 1; k <= n; k++) cd = zadd(cd, zscal(ZT(tabtemp, n, k, i), M2(u, n, k, j)));
+      ZT(tab, n, j, i) = cd;
+    }
+  free(tabtemp); free(fjs); free(xq); free(wq); free(u); free(v); free(chebv); free(whts);
+  free(xnodes); free(legv);
+}
+
+/* tab_pw2pot(npw,n): exp(i ts(j) xs(k) D/(2 sqrt(delta))), bfgt_volrouts.f:339-401 */
+static void mk_pw2pot_table(int n, int npw, const double *ts, const double *xs, double delta,
+                            double boxdim, zc *tab) {
+  double dsq = boxdim / 2 / sqrt(delta);
+  int npw2 = npw / 2;
+  for (int i = 1; i <= n; i++) {
+    double x = xs[i - 1] * dsq;
+    for (int j1 = npw2 + 1; j1 <= npw; j1++) {
+      ZT(tab, npw, j1, i) = zexpi(ts[j1 - 1] * x);
+      ZT(tab, npw, npw - j1 + 1, i) = zconj(ZT(tab, npw, j1, i));
+    }
+  }
+}
+
+static void mk_legetab_recur(int m, double targ, double lambda, double boxdim, double *fint,
+                             double *fx, double *fxx) {
+  const double sqrtpih = 0.886226925452757940959713778283913;
+  double fp[100], fpp[100];
+  double lambda2 = lambda * lambda;
+  double a = (-1 - targ) / lambda, b = (1 - targ) / lambda;
+  double erfa = erf(a), erfb = erf(b);
+  double expa = exp(-a * a), expb = exp(-b * b);
+  double d1 = lambda * (expb - expa), d2 = lambda * (expb + expa);
+  fint[0] = sqrtpih * (erfb - erfa);
+  fint[1] = -d1 / 2 + targ * fint[0];
+  fint[2] = -d2 - targ * d1 + (lambda2 - 2.0 / 3 + 2 * (targ * targ)) * fint[0];
+  fint[2] = 0.75 * fint[2];
+  fint[3] = -d1 + 2 * targ * (4.0 * fint[2] / 3 - fint[0] / 3) - (0.4 - 4 * lambda2) * fint[1];
+  fint[3] = 5.0 * fint[3] / 8;
+  for (int k = 5; k <= m; k++) {
+    int n = k - 3;
+    fint[k - 1] = targ * (fint[k - 2] - fint[k - 4]) +
+                  (2 * n + 1) * (lambda2 / 2 + 1.0 / ((2 * n + 3) * (2 * n - 1))) * fint[k - 3] +
+                  (n - 1.0) * fint[k - 5] / (2 * n - 1);
+    fint[k - 1] = (2 * n + 3.0) * fint[k - 1] / (n + 2);
+  }
+  fp[0] = 0;
+  fp[1] = fint[0] * lambda;
+  for (int k = 3; k <= m; k++) fp[k - 1] = fp[k - 3] + (2 * k - 3) * fint[k - 2] * lambda;
+  fpp[0] = 0;
+  fpp[1] = 0;
+  for (int k = 3; k <= m; k++) fpp[k - 1] = fpp[k - 3] + (2 * k - 3) * fp[k - 2];
+  int isign = 1;
+  for (int k = 1; k <= m; k++) {
+    double px1 = (k - 1) * k / 2.0;
+    fxx[k - 1] = fpp[k - 1] - px1 * (expb + isign * expa) - 2 * (b * expb - isign * a * expa) / lambda;
+    isign = -isign;
+  }
+  double ww = boxdim * lambda / 2;
+  for (int k = 1; k <= m; k++) {
+    fint[k - 1] = fint[k - 1] * ww;
+    fxx[k - 1] = fxx[k - 1] * 2 / boxdim;
+  }
+  for (int k = 2; k <= m; k += 2) fx[k - 1] = fp[k - 1] - d2 / lambda;
+  for (int k = 1; k <= m; k += 2) fx[k - 1] = fp[k - 1] - d1 / lambda;
+}
+
+static void mk_chebtab_recur(int m, double targ, double lambda, double boxdim, double *fint,
+                             double *fx, double *fxx) {
+  const double sqrtpih = 0.886226925452757940959713778283913;
+  double fp[100], fpp[100];
+  double lambda2 = lambda * lambda;
+  double a = (-1 - targ) / lambda, b = (1 - targ) / lambda;
+  double erfa = erf(a), erfb = erf(b);
+  double expa = exp(-a * a), expb = exp(-b * b);
+  double d1 = lambda * (expb - expa), d2 = lambda * (expb + expa);
+  fint[0] = sqrtpih * (erfb - erfa);
+  fint[1] = -d1 / 2 + targ * fint[0];
+  fint[2] = -d2 - targ * d1 + (lambda2 - 1 + 2 * (targ * targ)) * fint[0];
+  fint[3] = -d1 + 2 * targ * fint[2] - (1 - 4 * lambda2) * fint[1];
+  int isign = 1;
+  for (int k = 5; k <= m; k++) {
+    double dc = 0;
+    if (isign == 1) dc = d2;
+    if (isign == -1) dc = d1;
+    int n = k - 1;
+    double dd = (n - 1.0) / (n - 3);
+    fint[k - 1] = 2 * targ * fint[k - 2] + 2 * ((n - 1) * lambda2 + 1.0 / (n - 3)) * fint[k - 3] +
+                  dd * (fint[k - 5] - 2 * targ * fint[k - 4]) - (1 - dd) * dc;
+    isign = -isign;
+  }
+  fp[0] = 0;
+  fp[1] = fint[0] * lambda;
+  fp[2] = 4 * fint[1] * lambda;
+  for (int k = 4; k <= m; k++) fp[k - 1] = (fp[k - 3] / (k - 3) + 2 * fint[k - 2] * lambda) * (k - 1);
+  fpp[0] = 0;
+  fpp[1] = 0;
+  fpp[2] = 4 * fint[0] * lambda;
+  for (int k = 4; k <= m; k++) fpp[k - 1] = (fpp[k - 3] / (k - 3) + 2 * fp[k - 2]) * (k - 1);
+  isign = 1;
+  for (int k = 1; k <= m; k++) {
+    double tp1 = (double)((k - 1) * (k - 1));
+    fxx[k - 1] = fpp[k - 1] - tp1 * (expb + isign * expa) - 2 * (b * expb - isign * a * expa) / lambda;
+    isign = -isign;
+  }
+  double ww = boxdim * lambda / 2;
+  double sc = 2 / boxdim;
+  for (int k = 1; k <= m; k++) {
+    fint[k - 1] = fint[k - 1] * ww;
+    fxx[k - 1] = fxx[k - 1] * sc;
+  }
+  for (int k = 2; k <= m; k += 2) fx[k - 1] = fp[k - 1] - d2 / lambda;
+  for (int k = 1; k <= m; k += 2) fx[k - 1] = fp[k - 1] - d1 / lambda;
+}
+
+static void mk_loctab(int ipoly, int n, double delta, int nt, const double *tnodes, double tboxdim,
+                      double tboxcen, double scale, double *tab, double *tabx, double *tabxx, int nquad,
+                      const double *xnodes, const double *wts, const double *polyv) {
+  double fint[100], fx[100], fxx[100];
+  double *targs = malloc(sizeof(double) * n);
+  for (int i = 1; i <= nt; i++) targs[i - 1] = tnodes[i - 1] / scale + tboxcen;
+  double bs = tboxdim * scale;
+  double sigma = 4 * delta / (bs * bs);
+  double lambda = sqrt(sigma);
+  double reps = 1e-16;
+  double dmax = sqrt(log(1 / reps) * sigma);
+  if (lambda <= 0.125) {
+    for (int j = 1; j <= nt; j++) {
+      double targ = targs[j - 1];
+      double dis = 0;
+      if (targ < -1) dis = -1 - targ;
+      if (targ > 1) dis = targ - 1;
+      if (dis > dmax) {
+        for (int m = 1; m <= n; m++) {
+          M2(tab, n, m, j) = 0; M2(tabx, n, m, j) = 0; M2(tabxx, n, m, j) = 0;
+        }
+      } else {
+        if (ipoly == 0) mk_legetab_recur(n, targ, lambda, bs, fint, fx, fxx);
+        if (ipoly == 1) mk_chebtab_recur(n, targ, lambda, bs, fint, fx, fxx);
+        for (int m = 1; m <= n; m++) {
+          M2(tab, n, m, j) = fint[m - 1]; M2(tabx, n, m, j) = fx[m - 1]; M2(tabxx, n, m, j) = fxx[m - 1];
+        }
+      }
+    }
+  } else {
+    double *wexp = malloc(sizeof(double) * nquad * nt);
+    for (int j = 1; j <= nt; j++) {
+      double targ = targs[j - 1];
+      for (int i = 1; i <= nquad; i++) {
+        double dx = targ - xnodes[i - 1];
+        if (fabs(dx) < dmax) M2(wexp, nquad, i, j) = exp(-dx * dx / sigma) * wts[i - 1];
+        else M2(wexp, nquad, i, j) = 0;
+      }
+    }
+    double bsh = bs / 2;
+    for (int j = 1; j <= nt; j++) {
+      double targ = targs[j - 1];
+      double dis = 0;
+      if (targ < -1) dis = -1 - targ;
+      if (targ > 1) dis = targ - 1;
+      if (dis > dmax) {
+        for (int m = 1; m <= n; m++) {
+          M2(tab, n, m, j) = 0; M2(tabx, n, m, j) = 0; M2(tabxx, n, m, j) = 0;
+        }
+      } else {
+        for (int m = 1; m <= n; m++) {
+          double rsum = 0, rsumx = 0, rsumxx = 0;
+          for (int i = 1; i <= nquad; i++) {
+            double dx = targ - xnodes[i - 1];
+            double dd = -2 * dx / sigma * 2 / bs;
+            double pw = M2(polyv, nquad, i, m) * M2(wexp, nquad, i, j);
+            rsum = rsum + pw;
+            rsumx = rsumx + pw * dd;
+            rsumxx = rsumxx + pw * (dd * dd - 2 / delta);
+          }
+          M2(tab, n, m, j) = rsum * bsh;
+          M2(tabx, n, m, j) = rsumx * bsh;
+          M2(tabxx, n, m, j) = rsumxx * bsh;
+        }
+      }
+    }
+    free(wexp);
+  }
+  free(targs);
+}
+
+/* indc(2, n+1) stored as indc[2*(i-1)+0/1] */
+static void compute_sparse_pattern(double eps, int m, int n, const double *a, int *indc, int *ifzero) {
+  *ifzero = 0;
+  for (int i = 1; i <= n + 1; i++) { indc[2 * (i - 1)] = 0; indc[2 * (i - 1) + 1] = -1; }
+  double dmax = 0;
+  for (int i = 1; i <= n; i++)
+    for (int j = 1; j <= m; j++) {
+      double c = fabs(M2(a, m, j, i));
+      if (dmax < c) dmax = c;
+    }
+  if (dmax <= 2e-16) { *ifzero = 1; return; }
+  for (int i = 1; i <= n; i++)
+    for (int j = 1; j <= m; j++) {
+      double c = fabs(M2(a, m, j, i));
+      if (c > eps * dmax / n) { indc[2 * (i - 1)] = j; break; }
+    }
+  for (int i = 1; i <= n; i++)
+    for (int j = m; j >= 1; j--) {
+      double c = fabs(M2(a, m, j, i));
+      if (c > eps * dmax / n) { indc[2 * (i - 1) + 1] = j; break; }
+    }
+  for (int i = 1; i <= n; i++)
+    if (indc[2 * (i - 1)] > 0) { indc[2 * n] = i; break; }
+  for (int i = n; i >= 1; i--)
+    if (indc[2 * (i - 1) + 1] > 0) { indc[2 * n + 1] = i; break; }
+}
+
+/* Table layout: tab_loc(n,n,-nloctab:nloctab), ind_loc(2,n+1,-nloctab:nloctab) */
+#define TLOC(t, n, nl, m, j, k) (t)[((m) - 1) + (size_t)(n) * (((j) - 1) + (size_t)(n) * ((k) + (nl)))]
+#define ILOC(t, n, nl, c, j, k) (t)[((c) - 1) + 2 * (((j) - 1) + (size_t)((n) + 1) * ((k) + (nl)))]
+
+static void merge_pattern(int n, const int *ind, const int *indx, const int *indxx, int *ind_loc, int nloctab,
+                          int k) {
+  for (int j = 1; j <= n + 1; j++) {
+    int i2 = ind[2 * (j - 1) + 1];
+    if (i2 < indx[2 * (j - 1) + 1]) i2 = indx[2 * (j - 1) + 1];
+    if (i2 < indxx[2 * (j - 1) + 1]) i2 = indxx[2 * (j - 1) + 1];
+    ILOC(ind_loc, n, nloctab, 2, j, k) = i2;
+    int i1 = ind[2 * (j - 1)];
+    if (indx[2 * (j - 1)] == 0) {
+    } else if (i1 > indx[2 * (j - 1)]) {
+      i1 = indx[2 * (j - 1)];
+    }
+    if (indxx[2 * (j - 1)] == 0) {
+    } else if (i1 > indxx[2 * (j - 1)]) {
+      i1 = indxx[2 * (j - 1)];
+    }
+    if (i2 > 0 && i1 == 0) i1 = 1;
+    ILOC(ind_loc, n, nloctab, 1, j, k) = i1;
+  }
+}
+
+static void mk_loctab_all(double eps, int ipoly, int n, double delta, double boxdim, int mrefinelev,
+                          int nloctab, double *tab_loc, double *tabx_loc, double *tabxx_loc, int *ind_loc) {
+  double *tab = malloc(sizeof(double) * n * n), *tabx = malloc(sizeof(double) * n * n),
+         *tabxx = malloc(sizeof(double) * n * n);
+  double *tnodes = malloc(sizeof(double) * n), *ws = malloc(sizeof(double) * n);
+  double *umat = malloc(sizeof(double) * n * n), *vmat = malloc(sizeof(double) * n * n);
+  if (ipoly == 0) legeexps(2, n, tnodes, umat, vmat, ws);
+  if (ipoly == 1) chebexps(2, n, tnodes, umat, vmat, ws);
+  int nquad = 50;
+  double *xnodes = malloc(sizeof(double) * nquad), *wts = malloc(sizeof(double) * nquad);
+  double *ptmp = malloc(sizeof(double) * n), *polyv = malloc(sizeof(double) * nquad * n);
+  legeexps(1, nquad, xnodes, NULL, NULL, wts);
+  for (int i = 1; i <= nquad; i++) {
+    if (ipoly == 0) legepols(xnodes[i - 1], n - 1, ptmp);
+    else chebpols(xnodes[i - 1], n - 1, ptmp);
+    for (int j = 1; j <= n; j++) M2(polyv, nquad, i, j) = ptmp[j - 1];
+  }
+  int *ind = malloc(sizeof(int) * 2 * (n + 1)), *indx = malloc(sizeof(int) * 2 * (n + 1)),
+      *indxx = malloc(sizeof(int) * 2 * (n + 1));
+  int m0 = mrefinelev + 1;
+  for (int i0 = m0; i0 >= -1; i0--) {
+    for (int j0 = 1; j0 <= (1 << m0); j0++) {
+      int k = 0;
+      if (i0 > 0) k = -(1 << (m0 - i0)) - (1 << (m0 - i0 + 1)) * (j0 - 1);
+      else if (i0 == 0) k = -(1 << (m0 - i0 + 1)) * (j0 - 1);
+      else k = -(1 << m0) - (1 << (m0 + 1)) * (j0 - 1);
+      if (k < -nloctab) break;
+      double scale = pow(2.0, i0);
+      double cen = k / pow(2.0, m0);
+      mk_loctab(ipoly, n, delta, n, tnodes, boxdim, cen, scale, tab, tabx, tabxx, nquad, xnodes, wts, polyv);
+      /* dgemm_f77('t','n'): tab_loc(i,j,k) = sum_l umat(l,i) tab(l,j) */
+      for (int j = 1; j <= n; j++)
+        for (int i = 1; i <= n; i++) {
+          double t0 = 0, t1 = 0, t2 = 0;
+          for (int l = 1; l <= n; l++) {
+            t0 = t0 + M2(umat, n, l, i) * M2(tab, n, l, j);
+            t1 = t1 + M2(umat, n, l, i) * M2(tabx, n, l, j);
+            t2 = t2 + M2(umat, n, l, i) * M2(tabxx, n, l, j);
+          }
+          TLOC(tab_loc, n, nloctab, i, j, k) = 1.0 * t0;
+          TLOC(tabx_loc, n, nloctab, i, j, k) = 1.0 * t1;
+          TLOC(tabxx_loc, n, nloctab, i, j, k) = 1.0 * t2;
+        }
+      /* symmetry for targets on the right side (in place when k == 0) */
+      for (int j = 1; j <= n; j++)
+        for (int m = 1; m <= n; m++) {
+          TLOC(tab_loc, n, nloctab, m, j, -k) = TLOC(tab_loc, n, nloctab, n - m + 1, n - j + 1, k);
+          TLOC(tabx_loc, n, nloctab, m, j, -k) = -TLOC(tabx_loc, n, nloctab, n - m + 1, n - j + 1, k);
+          TLOC(tabxx_loc, n, nloctab, m, j, -k) = TLOC(tabxx_loc, n, nloctab, n - m + 1, n - j + 1, k);
+        }
+      int ifzero;
+      compute_sparse_pattern(eps, n, n, &TLOC(tab_loc, n, nloctab, 1, 1, -k), ind, &ifzero);
+      compute_sparse_pattern(eps, n, n, &TLOC(tabx_loc, n, nloctab, 1, 1, -k), indx, &ifzero);
+      compute_sparse_pattern(eps, n, n, &TLOC(tabxx_loc, n, nloctab, 1, 1, -k), indxx, &ifzero);
+      merge_pattern(n, ind, indx, indxx, ind_loc, nloctab, -k);
+      compute_sparse_pattern(eps, n, n, &TLOC(tab_loc, n, nloctab, 1, 1, k), ind, &ifzero);
+      compute_sparse_pattern(eps, n, n, &TLOC(tabx_loc, n, nloctab, 1, 1, k), indx, &ifzero);
+      compute_sparse_pattern(eps, n, n, &TLOC(tabxx_loc, n, nloctab, 1, 1, k), indxx, &ifzero);
+      merge_pattern(n, ind, indx, indxx, ind_loc, nloctab, k);
+    }
+  }
+  free(tab); free(tabx); free(tabxx); free(tnodes); free(ws); free(umat); free(vmat);
+  free(xnodes); free(wts); free(ptmp); free(polyv); free(ind); free(indx); free(indxx);
+}
+
+/* ------------------------------------------------------------------------- */
+/* PW shift tables (bfgt/bfgt_pwrouts.f)                                     */
+/* ------------------------------------------------------------------------- */
+
+/* wshift(npw*h, 4, nmax) */
+static void g2d_mk_merge_split_pw_matrices(double xmin, int npw, const double *ts, int nmax, zc *wshift) {
+  int hh = (npw + 1) / 2;
+  size_t nexp = (size_t)npw * hh;
+  zc *ww = malloc(sizeof(zc) * (size_t)npw * (nmax > 0 ? nmax : 1));
+  for (int j1 = 1; j1 <= npw; j1++) {
+    zc ztmp = zexpi(ts[j1 - 1] * xmin);
+    for (int k1 = 1; k1 <= nmax; k1++) {
+      ww[(j1 - 1) + (size_t)npw * (k1 - 1)] = ztmp;
+      ztmp = zmul(ztmp, ztmp);
+    }
+  }
+  for (int k1 = 1; k1 <= nmax; k1++) {
+    size_t j = 0;
+    for (int j1 = 1; j1 <= hh; j1++)
+      for (int j2 = 1; j2 <= npw; j2++) {
+        j++;
+        zc a = ww[(j2 - 1) + (size_t)npw * (k1 - 1)], b = ww[(j1 - 1) + (size_t)npw * (k1 - 1)];
+        zc *w = wshift + (size_t)4 * nexp * (k1 - 1);
+        w[(j - 1) + 0 * nexp] = zmul(a, b);
+        w[(j - 1) + 1 * nexp] = zmul(zconj(a), b);
+        w[(j - 1) + 2 * nexp] = zmul(a, zconj(b));
+        w[(j - 1) + 3 * nexp] = zmul(zconj(a), zconj(b));
+      }
+  }
+  free(ww);
+}
+
+/* wshift(npw*h, (2*nmax+1)^2) */
+static void g2d_mk_pw_translation_matrices(double xmin, int npw, const double *ts, int nmax, zc *wshift) {
+  int hh = (npw + 1) / 2;
+  size_t nexp = (size_t)npw * hh;
+  int nw = 2 * nmax + 1;
+  zc *ww = malloc(sizeof(zc) * (size_t)npw * nw);
+#define WW(j, k) ww[((j) - 1) + (size_t)npw * ((k) + nmax)]
+  for (int j1 = 1; j1 <= npw; j1++) {
+    zc ztmp = zexpi(ts[j1 - 1] * xmin);
+    WW(j1, 0) = zmk(1, 0);
+    for (int k1 = 1; k1 <= nmax; k1++) {
+      WW(j1, k1) = ztmp;
+      ztmp = zmul(ztmp, ztmp);
+      WW(j1, -k1) = zconj(WW(j1, k1));
+    }
+  }
+  int k = 0;
+  for (int k1 = -nmax; k1 <= nmax; k1++)
+    for (int k2 = -nmax; k2 <= nmax; k2++) {
+      k++;
+      size_t j = 0;
+      for (int j1 = 1; j1 <= hh; j1++)
+        for (int j2 = 1; j2 <= npw; j2++) {
+          j++;
+          wshift[(j - 1) + nexp * (k - 1)] = zmul(WW(j2, k2), WW(j1, k1));
+        }
+    }
+#undef WW
+  free(ww);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Tree lists (common/tree_routs_nd.f)                                       */
+/* ------------------------------------------------------------------------- */
+
+#define LADDR(itree, c, lev) (itree)[(c) - 1 + 2 * (lev)]
+#define IT(itree, iptr, k, ibox) (itree)[(iptr)[(k) - 1] + (ibox) - 2]
+#define ICHILD(itree, iptr, j, ibox) (itree)[(iptr)[4] + 4 * ((ibox) - 1) + (j) - 2]
+#define ICOLL(itree, iptr, j, ibox) (itree)[(iptr)[6] + 9 * ((ibox) - 1) + (j) - 2]
+#define CEN(c, k, ibox) (c)[((k) - 1) + 2 * ((ibox) - 1)]
+
+/* computecoll: writes itree(iptr(6)) ncoll and itree(iptr(7)) coll for boxes 1..nboxes */
+static void computecoll(int nlevels, int nboxes, int *itree, const int *iptr, const double *boxsize,
+                        const double *centers, int iperiod) {
+  double bs0 = boxsize[0];
+  for (int i = 1; i <= nboxes; i++) {
+    IT(itree, iptr, 6, i) = 0;
+    for (int j = 1; j <= 9; j++) ICOLL(itree, iptr, j, i) = -1;
+  }
+  IT(itree, iptr, 6, 1) = 1;
+  ICOLL(itree, iptr, 1, 1) = 1;
+  for (int ilev = 1; ilev <= nlevels; ilev++) {
+    int ifirst = LADDR(itree, 1, ilev), ilast = LADDR(itree, 2, ilev);
+#pragma omp parallel for schedule(static)
+    for (int ibox = ifirst; ibox <= ilast; ibox++) {
+      int dad = IT(itree, iptr, 3, ibox);
+      for (int i = 1; i <= IT(itree, iptr, 6, dad); i++) {
+        int jbox = ICOLL(itree, iptr, i, dad);
+        for (int j = 1; j <= 4; j++) {
+          int kbox = ICHILD(itree, iptr, j, jbox);
+          if (kbox > 0) {
+            int ifnbor = 1;
+            for (int k = 1; k <= 2; k++) {
+              double dis = fabs(CEN(centers, k, kbox) - CEN(centers, k, ibox));
+              if (iperiod == 1) {
+                double dp1 = bs0 - dis;
+                if (dp1 < dis) dis = dp1;
+              }
+              if (dis > 1.05 * boxsize[ilev]) { ifnbor = 0; break; }
+            }
+            if (ifnbor == 1) {
+              IT(itree, iptr, 6, ibox) += 1;
+              ICOLL(itree, iptr, IT(itree, iptr, 6, ibox), ibox) = kbox;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+static void gnd_find_pwexp_boxes(int npwlevel, int nboxes, int nlevels, const int *itree, const int *iptr,
+                                 int *ifpwexp) {
+  for (int i = 1; i <= nboxes; i++) ifpwexp[i - 1] = 0;
+  if (npwlevel <= 0) ifpwexp[0] = 1;
+  int ncutoff = npwlevel;
+  if (npwlevel <= 0) ncutoff = 0;
+  if (npwlevel <= nlevels) {
+    for (int ilev = ncutoff; ilev <= ncutoff; ilev++)
+      for (int ibox = LADDR(itree, 1, ilev); ibox <= LADDR(itree, 2, ilev); ibox++) {
+        int nchild = IT(itree, iptr, 4, ibox);
+        if (nchild == 0) {
+          int ncoll = IT(itree, iptr, 6, ibox);
+          for (int j = 1; j <= ncoll; j++) {
+            int jbox = ICOLL(itree, iptr, j, ibox);
+            if (IT(itree, iptr, 4, jbox) > 0) { ifpwexp[ibox - 1] = 1; break; }
+          }
+        } else {
+          ifpwexp[ibox - 1] = 1;
+        }
+      }
+    for (int ilev = ncutoff + 1; ilev <= nlevels; ilev++)
+      for (int ibox = LADDR(itree, 1, ilev); ibox <= LADDR(itree, 2, ilev); ibox++) ifpwexp[ibox - 1] = 1;
+  }
+}
+
+static int compute_mnlist1(int nboxes, int nlevels, const int *itree, const int *iptr, const double *centers,
+                           const double *boxsize, int isep, int iper) {
+  double bs0 = boxsize[0];
+  int *nlist1 = calloc((size_t)nboxes, sizeof(int));
+  nlist1[0] = 1;
+  for (int ilev = 1; ilev <= nlevels; ilev++) {
+    int first = LADDR(itree, 1, ilev), last = LADDR(itree, 2, ilev);
+#pragma omp parallel for schedule(static)
+    for (int ibox = first; ibox <= last; ibox++) {
+      int dad = IT(itree, iptr, 3, ibox);
+      if (IT(itree, iptr, 4, ibox) != 0) continue;
+      for (int i = 1; i <= IT(itree, iptr, 6, ibox); i++) {
+        int jbox = ICOLL(itree, iptr, i, ibox);
+        if (IT(itree, iptr, 4, jbox) == 0) nlist1[ibox - 1]++;
+        if (IT(itree, iptr, 4, jbox) > 0) {
+          double distest = 1.05 * (boxsize[ilev] + boxsize[ilev + 1]) / 2.0 * isep;
+          for (int j = 1; j <= 4; j++) {
+            int kbox = ICHILD(itree, iptr, j, jbox);
+            if (kbox > 0) {
+              int ifnbor = 1;
+              for (int k = 1; k <= 2; k++) {
+                double dis = fabs(CEN(centers, k, kbox) - CEN(centers, k, ibox));
+                if (iper == 1) { double dp1 = bs0 - dis; if (dp1 < dis) dis = dp1; }
+                if (dis > distest) { ifnbor = 0; break; }
+              }
+              if (ifnbor == 1) nlist1[ibox - 1]++;
+            }
+          }
+        }
+      }
+      for (int i = 1; i <= IT(itree, iptr, 6, dad); i++) {
+        int jbox = ICOLL(itree, iptr, i, dad);
+        if (IT(itree, iptr, 4, jbox) == 0) {
+          double distest = 1.05 * (boxsize[ilev] + boxsize[ilev - 1]) / 2.0 * isep;
+          int iflist1 = 1;
+          for (int k = 1; k <= 2; k++) {
+            double dis = fabs(CEN(centers, k, jbox) - CEN(centers, k, ibox));
+            if (iper == 1) { double dp1 = bs0 - dis; if (dp1 < dis) dis = dp1; }
+            if (dis >= distest) { iflist1 = 0; break; }
+          }
+          if (iflist1 == 1) nlist1[ibox - 1]++;
+        }
+      }
+    }
+  }
+  int mnlist1 = 0;
+  for (int i = 0; i < nboxes; i++)
+    if (nlist1[i] > mnlist1) mnlist1 = nlist1[i];
+  free(nlist1);
+  return mnlist1;
+}
+
+static void gnd_compute_modified_list1(int npwlevel, const int *ifpwexp, int nboxes, int nlevels,
+                                       const int *itree, const int *iptr, const double *centers,
+                                       const double *boxsize, int iperiod, int mnlist1, int *nlist1,
+                                       int *list1) {
+  double bs0 = boxsize[0];
+  for (int i = 0; i < nboxes; i++) nlist1[i] = 0;
+  if (IT(itree, iptr, 4, 1) == 0) {
+    nlist1[0] = 1;
+    list1[0] = 1;
+  } else {
+    nlist1[0] = 0;
+  }
+  int nlevend = nlevels;
+  if (npwlevel < nlevels) nlevend = npwlevel;
+  for (int ilev = 1; ilev <= nlevend; ilev++) {
+    int ifirst = LADDR(itree, 1, ilev), ilast = LADDR(itree, 2, ilev);
+#pragma omp parallel for schedule(static)
+    for (int ibox = ifirst; ibox <= ilast; ibox++) {
+      int dad = IT(itree, iptr, 3, ibox);
+      if (IT(itree, iptr, 4, ibox) != 0) continue;
+      int *l1 = list1 + (size_t)mnlist1 * (ibox - 1);
+      for (int i = 1; i <= IT(itree, iptr, 6, ibox); i++) {
+        int jbox = ICOLL(itree, iptr, i, ibox);
+        if (IT(itree, iptr, 4, jbox) == 0) {
+          if (ifpwexp[ibox - 1] != 1 || jbox != ibox) {
+            nlist1[ibox - 1]++;
+            l1[nlist1[ibox - 1] - 1] = jbox;
+          }
+        } else {
+          if (ilev < npwlevel) {
+            double distest = 1.05 * (boxsize[ilev] + boxsize[ilev + 1]) / 2.0;
+            for (int j = 1; j <= 4; j++) {
+              int kbox = ICHILD(itree, iptr, j, jbox);
+              if (IT(itree, iptr, 4, kbox) == 0) {
+                int iflist1 = 1;
+                for (int k = 1; k <= 2; k++) {
+                  double dis = fabs(CEN(centers, k, kbox) - CEN(centers, k, ibox));
+                  if (iperiod == 1) { double dp1 = bs0 - dis; if (dp1 < dis) dis = dp1; }
+                  if (dis >= distest) { iflist1 = 0; break; }
+                }
+                if (iflist1 == 1) {
+                  nlist1[ibox - 1]++;
+                  l1[nlist1[ibox - 1] - 1] = kbox;
+                }
+              }
+            }
+          }
+        }
+      }
+      for (int i = 1; i <= IT(itree, iptr, 6, dad); i++) {
+        int jbox = ICOLL(itree, iptr, i, dad);
+        if (IT(itree, iptr, 4, jbox) == 0) {
+          double distest = 1.05 * (boxsize[ilev] + boxsize[ilev - 1]) / 2.0;
+          int iflist1 = 1;
+          for (int k = 1; k <= 2; k++) {
+            double dis = fabs(CEN(centers, k, jbox) - CEN(centers, k, ibox));
+            if (iperiod == 1) { double dp1 = bs0 - dis; if (dp1 < dis) dis = dp1; }
+            if (dis >= distest) { iflist1 = 0; break; }
+          }
+          if (iflist1 == 1) {
+            nlist1[ibox - 1]++;
+            l1[nlist1[ibox - 1] - 1] = jbox;
+          }
+        }
+      }
+    }
+  }
+}
+
+static void gnd_compute_listpw(int npwlevel, int nboxes, int nlevels, const int *itree, const int *iptr,
+                               int mnlistpw, int *nlistpw, int *listpw) {
+  for (int i = 0; i < nboxes; i++) nlistpw[i] = 0;
+  if (npwlevel > nlevels) return;
+  int ncutoff = npwlevel > 0 ? npwlevel : 0;
+  for (int ibox = LADDR(itree, 1, ncutoff); ibox <= LADDR(itree, 2, ncutoff); ibox++) {
+    int ncoll = IT(itree, iptr, 6, ibox);
+    for (int i = 1; i <= ncoll; i++) {
+      int jbox = ICOLL(itree, iptr, i, ibox);
+      if (jbox != ibox && (IT(itree, iptr, 4, jbox) > 0 || IT(itree, iptr, 4, ibox) > 0)) {
+        nlistpw[ibox - 1]++;
+        listpw[(size_t)mnlistpw * (ibox - 1) + nlistpw[ibox - 1] - 1] = jbox;
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Per-box kernels (bfgt/bfgt_pwrouts.f, bfgt/bfgt_local.f)                  */
+/* ------------------------------------------------------------------------- */
+
+/* pwexp(npw,h,nd) from fvals(nd,n,n) with tab_poly2pw(n,npw) */
+static void g2d_tens_prod_to_pw(int nd, int n, const double *fvals, int npw, const zc *tab, zc *pwexp, zc *ff) {
+  int hh = (npw + 1) / 2;
+  for (int ind = 1; ind <= nd; ind++) {
+    for (int m1 = 1; m1 <= n; m1++)
+      for (int k2 = 1; k2 <= hh; k2++) {
+        zc cd = zmk(0, 0);
+        for (int m2 = 1; m2 <= n; m2++) {
+          double f = fvals[(ind - 1) + (size_t)nd * ((m1 - 1) + (size_t)n * (m2 - 1))];
+          cd = zadd(cd, zscal(ZT(tab, n, m2, k2), f));
+        }
+        ff[(m1 - 1) + (size_t)n * (k2 - 1)] = cd;
+      }
+    for (int k2 = 1; k2 <= hh; k2++)
+      for (int k1 = 1; k1 <= npw; k1++) {
+        zc cd = zmk(0, 0);
+        for (int m1 = 1; m1 <= n; m1++) cd = zadd(cd, zmul(ZT(tab, n, m1, k1), ff[(m1 - 1) + (size_t)n * (k2 - 1)]));
+        pwexp[(k1 - 1) + (size_t)npw * ((k2 - 1) + (size_t)hh * (ind - 1))] = cd;
+      }
+  }
+}
+
+/* pot(nd,n,n) += 2 Re(...) with tab_pw2pot(npw,n) */
+static void g2d_pw2pot(int nd, int n, int npw, const zc *pwexp, const zc *tab, double *pot, zc *ff) {
+  int hh = (npw + 1) / 2;
+  int npw2 = npw / 2;
+  for (int ind = 1; ind <= nd; ind++) {
+    for (int m2 = 1; m2 <= hh; m2++)
+      for (int k1 = 1; k1 <= n; k1++) {
+        zc cd = zmk(0, 0);
+        for (int m1 = 1; m1 <= npw; m1++)
+          cd = zadd(cd, zmul(ZT(tab, npw, m1, k1), pwexp[(m1 - 1) + (size_t)npw * ((m2 - 1) + (size_t)hh * (ind - 1))]));
+        ff[(k1 - 1) + (size_t)n * (m2 - 1)] = cd;
+      }
+    for (int k2 = 1; k2 <= n; k2++)
+      for (int k1 = 1; k1 <= n; k1++) {
+        zc cd = zmk(0, 0);
+        for (int m2 = 1; m2 <= npw2; m2++) cd = zadd(cd, zmul(ZT(tab, npw, m2, k2), ff[(k1 - 1) + (size_t)n * (m2 - 1)]));
+        int m2 = hh;
+        if (m2 > npw2) {
+          zc t = zmul(ZT(tab, npw, m2, k2), ff[(k1 - 1) + (size_t)n * (m2 - 1)]);
+          cd = zadd(cd, zmk(t.re / 2, t.im / 2));
+        }
+        size_t o = (ind - 1) + (size_t)nd * ((k1 - 1) + (size_t)n * (k2 - 1));
+        pot[o] = pot[o] + cd.re * 2;
+      }
+  }
+}
+
+static void gnd_shiftpw(int nd, size_t nexp, const zc *p1, zc *p2, const zc *w) {
+  for (int ind = 0; ind < nd; ind++)
+    for (size_t j = 0; j < nexp; j++) p2[j + nexp * ind] = zadd(p2[j + nexp * ind], zmul(p1[j + nexp * ind], w[j]));
+}
+
+static void gnd_shiftpw_loc(int nd, size_t nexp, const zc *p1, zc *p2, const zc *w) {
+  for (int ind = 0; ind < nd; ind++)
+    for (size_t j = 0; j < nexp; j++) p2[j + nexp * ind] = zmul(p1[j + nexp * ind], w[j]);
+}
+
+static int gnd_find_msshift_ind(const double *tcen, const double *scen) {
+  int k = 1, inc = 1;
+  for (int i = 0; i < 2; i++) {
+    double dx = tcen[i] - scen[i];
+    if (dx < 0) k = k + inc;
+    inc = inc * 2;
+  }
+  return k;
+}
+
+static int gnd_find_pwshift_ind(int iperiod, const double *tc, const double *sc, double bs0, double xmin, int nmax) {
+  int jxyz[2];
+  for (int i = 0; i < 2; i++) {
+    int jx = (int)lround((tc[i] - sc[i]) / xmin);
+    if (iperiod == 1) {
+      int jxp1 = (int)lround((tc[i] - sc[i] - bs0) / xmin);
+      int jxm1 = (int)lround((tc[i] - sc[i] + bs0) / xmin);
+      if (abs(jx) > abs(jxp1)) jx = jxp1;
+      if (abs(jx) > abs(jxm1)) jx = jxm1;
+    }
+    jxyz[i] = jx + nmax;
+  }
+  int n = 2 * nmax + 1, ind = 1, inc = 1;
+  for (int i = 0; i < 2; i++) { ind = ind + jxyz[i] * inc; inc = inc * n; }
+  return ind;
+}
+
+static void gnd_find_loctab_ind(int iperiod, const double *tc, const double *sc, double sboxsize, double bs0,
+                                int mrefinelev, int *ixyz) {
+  double bs = sboxsize / (double)(1 << (2 + mrefinelev));
+  for (int i = 0; i < 2; i++) {
+    double dx = (tc[i] - sc[i]) / bs;
+    if (iperiod == 1) {
+      double dxp1 = dx - bs0 / bs, dxm1 = dx + bs0 / bs;
+      if (fabs(dx) > fabs(dxp1)) dx = dxp1;
+      if (fabs(dx) > fabs(dxm1)) dx = dxm1;
+    }
+    ixyz[i] = (int)dx; /* Fortran integer assignment truncates toward zero */
+  }
+}
+
+static void g2d_tens_prod_to_potloc(int nd, int n, const double *fvals, double *pot, int ntab, const double *tab_loc,
+                                    const int *ind_loc, const int *ixy, double *ff) {
+  int ix = ixy[0], iy = ixy[1];
+  int nx = ILOC(ind_loc, n, ntab, 2, n + 1, ix) - ILOC(ind_loc, n, ntab, 1, n + 1, ix) + 1;
+  int ny = ILOC(ind_loc, n, ntab, 2, n + 1, iy) - ILOC(ind_loc, n, ntab, 1, n + 1, iy) + 1;
+  if (nx == 0 || ny == 0) return;
+  for (int ind = 1; ind <= nd; ind++) {
+    for (int j2 = 1; j2 <= n; j2++)
+      for (int k1 = ILOC(ind_loc, n, ntab, 1, n + 1, ix); k1 <= ILOC(ind_loc, n, ntab, 2, n + 1, ix); k1++) {
+        double cd = 0;
+        for (int j1 = ILOC(ind_loc, n, ntab, 1, k1, ix); j1 <= ILOC(ind_loc, n, ntab, 2, k1, ix); j1++)
+          cd = cd + TLOC(tab_loc, n, ntab, j1, k1, ix) * fvals[(ind - 1) + (size_t)nd * ((j1 - 1) + (size_t)n * (j2 - 1))];
+        ff[(k1 - 1) + (size_t)n * (j2 - 1)] = cd;
+      }
+    for (int k2 = ILOC(ind_loc, n, ntab, 1, n + 1, iy); k2 <= ILOC(ind_loc, n, ntab, 2, n + 1, iy); k2++)
+      for (int k1 = ILOC(ind_loc, n, ntab, 1, n + 1, ix); k1 <= ILOC(ind_loc, n, ntab, 2, n + 1, ix); k1++) {
+        double cd = 0;
+        for (int j2 = ILOC(ind_loc, n, ntab, 1, k2, iy); j2 <= ILOC(ind_loc, n, ntab, 2, k2, iy); j2++)
+          cd = cd + TLOC(tab_loc, n, ntab, j2, k2, iy) * ff[(k1 - 1) + (size_t)n * (j2 - 1)];
+        size_t o = (ind - 1) + (size_t)nd * ((k1 - 1) + (size_t)n * (k2 - 1));
+        pot[o] = pot[o] + cd;
+      }
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Driver (bfgt/boxfgt.f)                                                    */
+/* ------------------------------------------------------------------------- */
+
+/* Optional introspection of the internal plan, for tests that compare the
+   product's host-side plan with this restatement. */
+typedef struct {
+  int npwlevel;     /* boxfgt-level cutoff (after the periodic <=1 -> 0 rule) */
+  int npwlevel_int; /* bfgtmain-internal cutoff */
+  int npw;
+  int nlevstart;
+  int nlevend;
+  int iperiod_int;
+  int regime;       /* 0 = A (periodic Fourier), 1 = B (PW + near field), 2 = C (direct only) */
+  int mnlist1;
+  int nleafbox;
+  /* optional outputs (may be NULL) sized by the caller */
+  int *ifpwexp;     /* nboxes */
+  int *nlist1;      /* nboxes */
+  int *list1;       /* mnlist1_cap * nboxes */
+  int mnlist1_cap;
+  int *nlistpw;     /* nboxes */
+  int *listpw;      /* 8 * nboxes */
+  int *ind_loc;     /* 2*(n+1)*13*(nlevels+1) */
+  double *tab_loc;  /* n*n*13*(nlevels+1) */
+  double *ts;       /* npw */
+  double *ws;       /* npw */
+} oracle_info;
+
+static void boxfgt_core(int nd, double delta, double eps, int ipoly, int *iperiod_p, int norder, int npbox,
+                        int nboxes, int nlevels, int *itree, const int *iptr, const double *centers,
+                        const double *boxsize, const double *fvals, double *pot, double *timeinfo,
+                        oracle_info *info) {
+  int iperiod = *iperiod_p;
+  double pi = 4.0 * atan(1.0);
+  (void)pi;
+  double t1, t2;
+
+  /* ---- boxfgt: cutoff level and npw (boxfgt.f:130-167) ---- */
+  double dcutoff = sqrt(delta * log(1.0 / eps));
+  int npwlevel = nlevels + 1;
+  for (int i = nlevels; i >= 0; i--)
+    if (boxsize[i] >= dcutoff) { npwlevel = i; break; }
+  if (boxsize[nlevels] > dcutoff) npwlevel = nlevels + 1;
+  if (boxsize[0] <= dcutoff) npwlevel = 0;
+  if (npwlevel <= 1 && iperiod == 1) npwlevel = 0;
+  int npw = 0;
+  double pmax = 0;
+  if (npwlevel <= nlevels) {
+    if (npwlevel <= 0) fgtpwterms(boxsize[0], delta, eps, iperiod, &pmax, &npw);
+    else fgtpwterms(2 * boxsize[npwlevel], delta, eps, 0, &pmax, &npw);
+  }
+  if (info) info->npwlevel = npwlevel;
+
+  /* ---- bfgtmain (boxfgt.f:472-) ---- */
+  double bs0 = boxsize[0];
+  double ws[256], ts[256];
+  memset(ws, 0, sizeof(ws));
+  memset(ts, 0, sizeof(ts));
+  int iperiod0 = iperiod;
+  double delta0 = delta;
+  t1 = wtime();
+  if (npwlevel <= 1 && iperiod == 1) {
+    get_periodic_pwnodes(bs0, delta, eps, npw, ws, ts);
+    iperiod = 0;
+    npwlevel = 0;
+    delta0 = 1.0;
+    computecoll(nlevels, LADDR(itree, 2, nlevels), itree, iptr, boxsize, centers, iperiod);
+  } else {
+    computecoll(nlevels, LADDR(itree, 2, nlevels), itree, iptr, boxsize, centers, iperiod);
+    get_pwnodes(0, pmax, npw, ws, ts);
+  }
+  double *xq = malloc(sizeof(double) * norder), *umat = malloc(sizeof(double) * norder * norder);
+  double *vmat = malloc(sizeof(double) * norder * norder), *wts = malloc(sizeof(double) * norder);
+  if (ipoly == 0) legeexps(2, norder, xq, umat, vmat, wts);
+  if (ipoly == 1) chebexps(2, norder, xq, umat, vmat, wts);
+
+  int nlevend = nlevels;
+  if (npwlevel < nlevels) nlevend = npwlevel;
+  if (npwlevel == 0 && iperiod0 == 1) nlevend = -1;
+
+  int nleafbox = 0;
+  for (int ilevel = 1; ilevel <= nlevels; ilevel++)
+    for (int ibox = LADDR(itree, 1, ilevel); ibox <= LADDR(itree, 2, ilevel); ibox++)
+      if (IT(itree, iptr, 4, ibox) == 0) nleafbox++;
+  for (int i = 0; i < 20; i++) timeinfo[i] = 0;
+
+  int *ifpwexp = malloc(sizeof(int) * nboxes);
+  gnd_find_pwexp_boxes(npwlevel, nboxes, nlevels, itree, iptr, ifpwexp);
+  int mnlist1 = compute_mnlist1(nboxes, nlevels, itree, iptr, centers, boxsize, 1, iperiod);
+  if (mnlist1 < 1) mnlist1 = 1;
+  int *list1 = malloc(sizeof(int) * (size_t)mnlist1 * nboxes), *nlist1 = malloc(sizeof(int) * nboxes);
+  gnd_compute_modified_list1(npwlevel, ifpwexp, nboxes, nlevels, itree, iptr, centers, boxsize, iperiod, mnlist1,
+                             nlist1, list1);
+  int mrefinelev = 0;
+  int nloctab = (1 << (mrefinelev + 1)) * (mrefinelev + 3);
+  size_t ntabl = (size_t)norder * norder * (2 * nloctab + 1);
+  size_t nindl = (size_t)2 * (norder + 1) * (2 * nloctab + 1);
+  /* the +-5 slots are never written by mk_loctab_all (mrefinelev = 0); zero them */
+  double *tab_loc = calloc(ntabl * (nlevels + 1), sizeof(double));
+  double *tabx_loc = calloc(ntabl * (nlevels + 1), sizeof(double));
+  double *tabxx_loc = calloc(ntabl * (nlevels + 1), sizeof(double));
+  int *ind_loc = calloc(nindl * (nlevels + 1), sizeof(int));
+#pragma omp parallel for schedule(dynamic)
+  for (int ilev = 0; ilev <= nlevels; ilev++) {
+    mk_loctab_all(eps, ipoly, norder, delta, boxsize[ilev], mrefinelev, nloctab, tab_loc + ntabl * ilev,
+                  tabx_loc + ntabl * ilev, tabxx_loc + ntabl * ilev, ind_loc + nindl * ilev);
+    /* mk_loctab_all never builds the offsets +-5, but the periodic level-1
+       image loop (boxfgt.f:1040-1052) can ask for them when a level-2 target
+       borders a level-1 source; the reference then reads uninitialised
+       memory.  That image lies beyond the cutoff distance, so its exact
+       contribution is below eps: give those slots the pattern of a zero table
+       (compute_sparse_pattern's ifzero output) so they contribute nothing. */
+    for (int kk = -5; kk <= 5; kk += 10)
+      for (int j = 1; j <= norder + 1; j++) {
+        ILOC(ind_loc + nindl * ilev, norder, nloctab, 1, j, kk) = 0;
+        ILOC(ind_loc + nindl * ilev, norder, nloctab, 2, j, kk) = -1;
+      }
+  }
+
+  int regime = 1;
+  if (npwlevel == 0 && iperiod0 == 1) regime = 0;
+  int direct_only = (npwlevel >= nlevels && npwlevel > 0);
+  if (direct_only) regime = 2;
+
+  int nlevstart = npwlevel > 0 ? npwlevel : 0;
+  int hh = (npw + 1) / 2;
+  size_t nexp = (size_t)hh * npw;
+  int64_t *iaddr = NULL;
+  zc *rmlexp = NULL;
+  int *nlistpw = NULL, *listpw = NULL;
+  zc *tab_poly2pw = NULL, *tab_pw2pot = NULL, *wpwmsshift = NULL, *wpwshift = NULL;
+  int nmaxms = 0;
+  if (!direct_only) {
+    /* gnd_mpalloc (boxfgt.f:1598-1702), in complex units */
+    iaddr = malloc(sizeof(int64_t) * 2 * nboxes);
+    int64_t nn = (int64_t)nexp * nd;
+    int64_t istart = 0;
+    for (int i = nlevstart; i <= nlevels; i++) {
+      for (int ibox = LADDR(itree, 1, i); ibox <= LADDR(itree, 2, i); ibox++)
+        iaddr[2 * (ibox - 1)] = istart + (int64_t)(ibox - LADDR(itree, 1, i)) * nn;
+      istart += (int64_t)(LADDR(itree, 2, i) - LADDR(itree, 1, i) + 1) * nn;
+    }
+    for (int ibox = LADDR(itree, 1, nlevstart); ibox <= LADDR(itree, 2, nlevstart); ibox++)
+      iaddr[2 * (ibox - 1) + 1] = istart + (int64_t)(ibox - LADDR(itree, 1, nlevstart)) * nn;
+    istart += (int64_t)(LADDR(itree, 2, nlevstart) - LADDR(itree, 1, nlevstart) + 1) * nn;
+    for (int i = nlevstart + 1; i <= nlevels; i++)
+      for (int ibox = LADDR(itree, 1, i); ibox <= LADDR(itree, 2, i); ibox++)
+        iaddr[2 * (ibox - 1) + 1] = iaddr[2 * (ibox - 1)];
+    rmlexp = malloc(sizeof(zc) * (size_t)(istart > 0 ? istart : 1));
+
+    tab_poly2pw = malloc(sizeof(zc) * (size_t)norder * npw * (nlevels + 1));
+    tab_pw2pot = malloc(sizeof(zc) * (size_t)norder * npw * (nlevels + 1));
+#pragma omp parallel for schedule(dynamic)
+    for (int ilev = nlevstart; ilev <= nlevels; ilev++) {
+      if (ipoly == 0) mk_leg2pw_tables(norder, npw, ws, ts, delta0, boxsize[ilev], tab_poly2pw + (size_t)norder * npw * ilev);
+      else mk_cheb2pw_tables(norder, npw, ws, ts, delta0, boxsize[ilev], tab_poly2pw + (size_t)norder * npw * ilev);
+      mk_pw2pot_table(norder, npw, ts, xq, delta0, boxsize[ilev], tab_pw2pot + (size_t)norder * npw * ilev);
+    }
+    nmaxms = nlevels - (npwlevel > 0 ? npwlevel : 0);
+    wpwmsshift = malloc(sizeof(zc) * nexp * 4 * (nmaxms > 0 ? nmaxms : 1));
+    double xmin2 = boxsize[nlevels] / sqrt(delta0) / 2;
+    g2d_mk_merge_split_pw_matrices(xmin2, npw, ts, nmaxms, wpwmsshift);
+    wpwshift = malloc(sizeof(zc) * nexp * 9);
+    double xmin = boxsize[nlevstart] / sqrt(delta0);
+    g2d_mk_pw_translation_matrices(xmin, npw, ts, 1, wpwshift);
+    nlistpw = malloc(sizeof(int) * nboxes);
+    listpw = calloc(8 * (size_t)nboxes, sizeof(int));
+    gnd_compute_listpw(npwlevel, nboxes, nlevels, itree, iptr, 8, nlistpw, listpw);
+  }
+  t2 = wtime();
+  timeinfo[0] += t2 - t1;
+
+  if (info) {
+    info->npwlevel_int = npwlevel;
+    info->npw = npw;
+    info->nlevstart = nlevstart;
+    info->nlevend = nlevend;
+    info->iperiod_int = iperiod;
+    info->regime = regime;
+    info->mnlist1 = mnlist1;
+    info->nleafbox = nleafbox;
+    if (info->ifpwexp) memcpy(info->ifpwexp, ifpwexp, sizeof(int) * nboxes);
+    if (info->nlist1) memcpy(info->nlist1, nlist1, sizeof(int) * nboxes);
+    if (info->list1 && info->mnlist1_cap >= mnlist1)
+      for (int i = 0; i < nboxes; i++)
+        for (int j = 0; j < nlist1[i]; j++) info->list1[(size_t)info->mnlist1_cap * i + j] = list1[(size_t)mnlist1 * i + j];
+    if (info->nlistpw) {
+      if (nlistpw) memcpy(info->nlistpw, nlistpw, sizeof(int) * nboxes);
+      else memset(info->nlistpw, 0, sizeof(int) * nboxes);
+    }
+    if (info->listpw && listpw) memcpy(info->listpw, listpw, sizeof(int) * 8 * (size_t)nboxes);
+    if (info->ind_loc) memcpy(info->ind_loc, ind_loc, sizeof(int) * nindl * (nlevels + 1));
+    if (info->tab_loc) memcpy(info->tab_loc, tab_loc, sizeof(double) * ntabl * (nlevels + 1));
+    if (info->ts) memcpy(info->ts, ts, sizeof(double) * npw);
+    if (info->ws) memcpy(info->ws, ws, sizeof(double) * npw);
+  }
+
+  size_t ffsz = (size_t)norder * (hh > norder ? hh : norder) + (size_t)norder * norder;
+  if (!direct_only) {
+    /* STEP 1: leaf values -> mp PW (boxfgt.f:728-744) */
+    t1 = wtime();
+    for (int ilev = nlevels; ilev >= nlevstart; ilev--) {
+      int b0 = LADDR(itree, 1, ilev), b1 = LADDR(itree, 2, ilev);
+#pragma omp parallel
+      {
+        zc *ff = malloc(sizeof(zc) * ffsz);
+#pragma omp for schedule(dynamic)
+        for (int ibox = b0; ibox <= b1; ibox++) {
+          if (ifpwexp[ibox - 1] == 1 && IT(itree, iptr, 4, ibox) == 0)
+            g2d_tens_prod_to_pw(nd, norder, fvals + (size_t)nd * npbox * (ibox - 1), npw,
+                                tab_poly2pw + (size_t)norder * npw * ilev, rmlexp + iaddr[2 * (ibox - 1)], ff);
+        }
+        free(ff);
+      }
+    }
+    t2 = wtime();
+    timeinfo[1] += t2 - t1;
+
+    /* STEP 2: merge mp (boxfgt.f:764-783) */
+    t1 = wtime();
+    for (int ilev = nlevels - 1; ilev >= nlevstart; ilev--) {
+      int klev = nlevels - ilev;
+      int b0 = LADDR(itree, 1, ilev), b1 = LADDR(itree, 2, ilev);
+#pragma omp parallel for schedule(dynamic)
+      for (int ibox = b0; ibox <= b1; ibox++) {
+        int nchild = IT(itree, iptr, 4, ibox);
+        if (nchild > 0) memset(rmlexp + iaddr[2 * (ibox - 1)], 0, sizeof(zc) * nexp * nd);
+        for (int i = 1; i <= nchild; i++) {
+          int jbox = ICHILD(itree, iptr, i, ibox);
+          int k = gnd_find_msshift_ind(&CEN(centers, 1, ibox), &CEN(centers, 1, jbox));
+          gnd_shiftpw(nd, nexp, rmlexp + iaddr[2 * (jbox - 1)], rmlexp + iaddr[2 * (ibox - 1)],
+                      wpwmsshift + nexp * ((size_t)(k - 1) + 4 * (size_t)(klev - 1)));
+        }
+      }
+    }
+    t2 = wtime();
+    timeinfo[2] += t2 - t1;
+
+    /* STEP 3: mp -> loc at the cutoff level (boxfgt.f:805-822) */
+    t1 = wtime();
+    double xmin = boxsize[nlevstart];
+    {
+      int b0 = LADDR(itree, 1, nlevstart), b1 = LADDR(itree, 2, nlevstart);
+#pragma omp parallel for schedule(dynamic)
+      for (int ibox = b0; ibox <= b1; ibox++) {
+        memcpy(rmlexp + iaddr[2 * (ibox - 1) + 1], rmlexp + iaddr[2 * (ibox - 1)], sizeof(zc) * nexp * nd);
+        for (int j = 1; j <= nlistpw[ibox - 1]; j++) {
+          int jbox = listpw[(size_t)8 * (ibox - 1) + j - 1];
+          int ind = gnd_find_pwshift_ind(iperiod, &CEN(centers, 1, ibox), &CEN(centers, 1, jbox), bs0, xmin, 1);
+          gnd_shiftpw(nd, nexp, rmlexp + iaddr[2 * (jbox - 1)], rmlexp + iaddr[2 * (ibox - 1) + 1],
+                      wpwshift + nexp * (size_t)(ind - 1));
+        }
+      }
+    }
+    t2 = wtime();
+    timeinfo[3] += t2 - t1;
+
+    /* STEP 4: split loc (boxfgt.f:845-863) */
+    t1 = wtime();
+    for (int ilev = nlevstart; ilev <= nlevels - 1; ilev++) {
+      int klev = nlevels - ilev;
+      int b0 = LADDR(itree, 1, ilev), b1 = LADDR(itree, 2, ilev);
+#pragma omp parallel for schedule(dynamic)
+      for (int ibox = b0; ibox <= b1; ibox++) {
+        int nchild = IT(itree, iptr, 4, ibox);
+        for (int i = 1; i <= nchild; i++) {
+          int jbox = ICHILD(itree, iptr, i, ibox);
+          int k = gnd_find_msshift_ind(&CEN(centers, 1, jbox), &CEN(centers, 1, ibox));
+          gnd_shiftpw_loc(nd, nexp, rmlexp + iaddr[2 * (ibox - 1) + 1], rmlexp + iaddr[2 * (jbox - 1) + 1],
+                          wpwmsshift + nexp * ((size_t)(k - 1) + 4 * (size_t)(klev - 1)));
+        }
+      }
+    }
+    t2 = wtime();
+    timeinfo[4] += t2 - t1;
+
+    /* STEP 5: evaluate loc PW at leaves (boxfgt.f:884-900) */
+    t1 = wtime();
+    for (int ilev = nlevstart; ilev <= nlevels; ilev++) {
+      int b0 = LADDR(itree, 1, ilev), b1 = LADDR(itree, 2, ilev);
+#pragma omp parallel
+      {
+        zc *ff = malloc(sizeof(zc) * ffsz);
+#pragma omp for schedule(dynamic)
+        for (int ibox = b0; ibox <= b1; ibox++) {
+          if (ifpwexp[ibox - 1] == 1 && IT(itree, iptr, 4, ibox) == 0)
+            g2d_pw2pot(nd, norder, npw, rmlexp + iaddr[2 * (ibox - 1) + 1], tab_pw2pot + (size_t)norder * npw * ilev,
+                       pot + (size_t)nd * npbox * (ibox - 1), ff);
+        }
+        free(ff);
+      }
+    }
+    t2 = wtime();
+    timeinfo[5] += t2 - t1;
+  }
+
+  /* STEP 6: direct near field (boxfgt.f:915-1071) */
+  t1 = wtime();
+  if (!(npwlevel == 0 && iperiod == 0)) {
+    for (int ilev = 0; ilev <= nlevend; ilev++) {
+      int b0 = LADDR(itree, 1, ilev), b1 = LADDR(itree, 2, ilev);
+      const double *tl = tab_loc + ntabl * ilev;
+      const int *il = ind_loc + nindl * ilev;
+#pragma omp parallel
+      {
+        double *ff = malloc(sizeof(double) * norder * norder);
+#pragma omp for schedule(dynamic)
+        for (int ibox = b0; ibox <= b1; ibox++) {
+          int nl1 = nlist1[ibox - 1];
+          for (int j = 1; j <= nl1; j++) {
+            int jbox = list1[(size_t)mnlist1 * (ibox - 1) + j - 1];
+            int jlev = IT(itree, iptr, 2, jbox);
+            double bs = boxsize[jlev];
+            int ixyz[2];
+            const double *fj = fvals + (size_t)nd * npbox * (jbox - 1);
+            double *pi_ = pot + (size_t)nd * npbox * (ibox - 1);
+            if (iperiod == 1 && jlev == 1) {
+              gnd_find_loctab_ind(0, &CEN(centers, 1, ibox), &CEN(centers, 1, jbox), bs, bs0, mrefinelev, ixyz);
+              g2d_tens_prod_to_potloc(nd, norder, fj, pi_, nloctab, tl, il, ixyz, ff);
+              int nimage = 0, iimage[2];
+              double dxyz[2], ctmp[2][3];
+              double bsh = bs * 0.25;
+              for (int i = 0; i < 2; i++) {
+                iimage[i] = 0;
+                dxyz[i] = CEN(centers, i + 1, jbox) - CEN(centers, i + 1, ibox);
+                if (fabs(dxyz[i]) > bsh) iimage[i] = 1;
+                if (iimage[i] == 1) nimage++;
+              }
+              if (nimage > 0) {
+                for (int i = 0; i < 2; i++) {
+                  if (dxyz[i] < -bsh) ctmp[i][0] = CEN(centers, i + 1, jbox) + bs0;
+                  else if (dxyz[i] > bsh) ctmp[i][0] = CEN(centers, i + 1, jbox) - bs0;
+                  else ctmp[i][0] = CEN(centers, i + 1, jbox);
+                }
+                if (nimage == 2) {
+                  ctmp[0][1] = CEN(centers, 1, jbox);
+                  ctmp[1][1] = ctmp[1][0];
+                  ctmp[0][2] = ctmp[0][0];
+                  ctmp[1][2] = CEN(centers, 2, jbox);
+                }
+                for (int k = 1; k <= (1 << nimage) - 1; k++) {
+                  double cc[2] = {ctmp[0][k - 1], ctmp[1][k - 1]};
+                  gnd_find_loctab_ind(0, &CEN(centers, 1, ibox), cc, bs, bs0, mrefinelev, ixyz);
+                  g2d_tens_prod_to_potloc(nd, norder, fj, pi_, nloctab, tl, il, ixyz, ff);
+                }
+              }
+            } else {
+              gnd_find_loctab_ind(iperiod, &CEN(centers, 1, ibox), &CEN(centers, 1, jbox), bs, bs0, mrefinelev, ixyz);
+              g2d_tens_prod_to_potloc(nd, norder, fj, pi_, nloctab, tl, il, ixyz, ff);
+            }
+          }
+        }
+        free(ff);
+      }
+    }
+  }
+  t2 = wtime();
+  timeinfo[6] += t2 - t1;
+
+  *iperiod_p = iperiod0;
+  free(xq); free(umat); free(vmat); free(wts); free(ifpwexp); free(list1); free(nlist1);
+  free(tab_loc); free(tabx_loc); free(tabxx_loc); free(ind_loc);
+  free(iaddr); free(rmlexp); free(nlistpw); free(listpw); free(tab_poly2pw); free(tab_pw2pot);
+  free(wpwmsshift); free(wpwshift);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Exported entry points (ctypes)                                            */
+/* ------------------------------------------------------------------------- */
+
+/* Same argument meaning as boxfgt (bfgt/boxfgt.f:5-8) restricted to ndim=2,
+   ifpgh=1.  pot is accumulated into.  itree's colleague arrays are rewritten
+   as the reference does. */
+void oracle_boxfgt(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
+                   int *itree, const int *iptr, const double *centers, const double *boxsize, const double *fvals,
+                   double *pot, double *timeinfo, oracle_info *info) {
+  int ip = iperiod;
+  double tinfo[20];
+  boxfgt_core(nd, delta, eps, ipoly, &ip, norder, norder * norder, nboxes, nlevels, itree, iptr, centers, boxsize,
+              fvals, pot, timeinfo ? timeinfo : tinfo, info);
+}
+
+void oracle_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+int oracle_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+/* Node families used by the leaf grid (for test harnesses). */
+void oracle_nodes(int ipoly, int n, double *x, double *umat, double *vmat, double *w) {
+  if (ipoly == 0) legeexps(2, n, x, umat, vmat, w);
+  else chebexps(2, n, x, umat, vmat, w);
+}
+
+void oracle_gauss_legendre(int n, double *x, double *w) { legeexps(1, n, x, NULL, NULL, w); }
+
+/* Per-level PW tables, for table-level comparisons. */
+void oracle_pw_tables(int ipoly, int n, int npw, const double *ws, const double *ts, double delta, double boxdim,
+                      double *tab_poly2pw, double *tab_pw2pot) {
+  double *xq = malloc(sizeof(double) * n), *u = malloc(sizeof(double) * n * n), *v = malloc(sizeof(double) * n * n),
+         *w = malloc(sizeof(double) * n);
+  if (ipoly == 0) legeexps(2, n, xq, u, v, w);
+  else chebexps(2, n, xq, u, v, w);
+  if (ipoly == 0) mk_leg2pw_tables(n, npw, ws, ts, delta, boxdim, (zc *)tab_poly2pw);
+  else mk_cheb2pw_tables(n, npw, ws, ts, delta, boxdim, (zc *)tab_poly2pw);
+  mk_pw2pot_table(n, npw, ts, xq, delta, boxdim, (zc *)tab_pw2pot);
+  free(xq); free(u); free(v); free(w);
+}
+
+/* Spherical Bessel values (for host-side table checks). */
+void oracle_besseljs(int nterms, double z, double *fjs) { besseljs3d_real(nterms, z, 1.0, fjs); }

@@ -1,0 +1,148 @@
+"""CUDA path vs the oracle, through the C ABI (boxfgt_ with host arrays, and the
+device-resident plan API).  Tolerance: relative L2 over leaf values below
+10*eps (the bar the transform is specified to), and FP64 results must also
+agree with the FP64 oracle to 1e-11 since both compute the same sums."""
+import numpy as np
+import pytest
+
+import heat2d_per_box_b200 as hb
+from oracle import oracle
+
+from conftest import gauss_sum
+from test_oracle import CASES
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def call_boxfgt(t, delta, eps, fvals=None, pot=None, nd=1):
+    fv = np.ascontiguousarray(t.fvals if fvals is None else fvals, dtype=np.float64)
+    pot = np.zeros(nd * t.npbox * t.nboxes) if pot is None else pot
+    it = t.itree.copy()
+    ti = np.zeros(20)
+    hb.boxfgt(nd, 2, delta, eps, t.ipoly, t.iperiod, t.norder, t.npbox, t.nboxes, t.nlevels, t.ltree, it, t.iptr,
+              t.centers, t.boxsize, fv, 1, pot, None, None, 0, 0, None, 0, None, None, None, ti)
+    return pot, it, ti
+
+
+GPU_CASES = CASES + [("ad16_leg_per", 1e-4, 1e-6), ("ad16_leg_per", 1e-3, 1e-9), ("ad16_leg_per", 1e-2, 1e-6)]
+
+
+@pytest.mark.parametrize("name,delta,eps", GPU_CASES)
+def test_boxfgt_matches_oracle(trees, name, delta, eps):
+    t = trees[name]
+    got, it, ti = call_boxfgt(t, delta, eps)
+    ref, info, it_ref = oracle.boxfgt(t, t.fvals, delta, eps, with_info=True)
+    lv = t.leaves()
+    err = rel_l2(got.reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv])
+    assert err < 10 * eps and err < 1e-11, err
+    np.testing.assert_array_equal(it, it_ref)       # colleagues rewritten as boxfgt does
+    assert ti[0] > 0                                 # precompute time recorded
+
+
+def test_accumulates_on_leaves_only(trees):
+    t = trees["ad_leg_per"]
+    rng = np.random.default_rng(5)
+    pot0 = rng.standard_normal(t.npbox * t.nboxes)
+    fv = t.fvals.copy()
+    nonleaf = np.nonzero(t.nchild() > 0)[0]
+    fv[nonleaf] = 1e6 * rng.standard_normal((len(nonleaf), t.npbox))   # ignored by the transform
+    got, _, _ = call_boxfgt(t, 1e-4, 1e-6, fvals=fv, pot=pot0.copy())
+    ref = oracle.boxfgt(t, t.fvals, 1e-4, 1e-6)
+    g = got.reshape(t.nboxes, -1)
+    p0 = pot0.reshape(t.nboxes, -1)
+    np.testing.assert_array_equal(g[nonleaf], p0[nonleaf])
+    lv = t.leaves()
+    assert rel_l2(g[lv] - p0[lv], ref.reshape(t.nboxes, -1)[lv]) < 1e-11
+
+
+@pytest.mark.parametrize("delta,eps", [(1e-4, 1e-6), (1e-2, 1e-9), (3e-5, 1e-6)])
+def test_multiple_densities(trees, delta, eps):
+    t = trees["ad_cheb_free"]
+    nd = 3
+    rng = np.random.default_rng(7)
+    fv = np.repeat(t.fvals[:, :, None], nd, axis=2) * rng.uniform(0.5, 2, nd)[None, None, :]
+    fv[:, :, 2] = rng.standard_normal(fv[:, :, 2].shape)
+    fv = np.ascontiguousarray(fv)
+    got, _, _ = call_boxfgt(t, delta, eps, fvals=fv, nd=nd)
+    ref = oracle.boxfgt(t, fv, delta, eps, nd=nd)
+    lv = t.leaves()
+    err = rel_l2(got.reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv])
+    assert err < 1e-11, err
+
+
+def test_plan_device_deterministic_and_graph(trees):
+    import torch
+    t = trees["ad16_leg_per"]
+    delta, eps = 1e-4, 1e-6
+    plan = hb.Plan(t, delta, eps)
+    dev = torch.device("cuda:0")
+    f = torch.from_numpy(t.fvals.reshape(-1)).to(dev)
+    p1 = torch.zeros_like(f)
+    p2 = torch.zeros_like(f)
+    plan.execute(f, p1)
+    plan.execute(f, p2)
+    torch.cuda.synchronize()
+    assert torch.equal(p1, p2)                      # fixed-order reductions: bitwise reproducible
+    p3 = torch.zeros_like(f)
+    plan.graph_capture(f, p3)
+    plan.graph_launch()
+    torch.cuda.synchronize()
+    assert torch.equal(p1, p3)
+    plan.execute(f, p1)                             # accumulates
+    torch.cuda.synchronize()
+    assert torch.allclose(p1, 2 * p2, rtol=1e-14, atol=0)
+    ref = oracle.boxfgt(t, t.fvals, delta, eps)
+    lv = t.leaves()
+    err = rel_l2(p2.cpu().numpy().reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv])
+    assert err < 1e-11
+    ms = plan.stage_ms()
+    assert ms[5] > 0
+    plan.close()
+
+
+def test_execute_host_matches(trees):
+    t = trees["uni3_leg_per"]
+    plan = hb.Plan(t, 1e-3, 1e-9)
+    pot = np.zeros(t.npbox * t.nboxes)
+    plan.execute_host(t.fvals, pot)
+    ref = oracle.boxfgt(t, t.fvals, 1e-3, 1e-9)
+    lv = t.leaves()
+    assert rel_l2(pot.reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv]) < 1e-11
+    plan.close()
+
+
+def test_config1_uniform_level5():
+    """C1: uniform level-5 tree, Legendre order 8, delta=1e-3, eps=1e-9, 3 Gaussians."""
+    g = gauss_sum(1, 3, 0.05, 0.1)
+    t = hb.build_uniform(5, g, norder=8, ipoly=0, iperiod=1)
+    got, _, _ = call_boxfgt(t, 1e-3, 1e-9)
+    ref = oracle.boxfgt(t, t.fvals, 1e-3, 1e-9)
+    lv = t.leaves()
+    assert rel_l2(got.reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv]) < 1e-11
+
+
+def test_golden_vectors_gpu():
+    import json
+    from pathlib import Path
+    g = json.loads((Path(__file__).parent / "golden" / "golden.json").read_text())
+    for case in g["cases"]:
+        gauss = np.array(case["gauss"])
+        if case["kind"] == "uniform":
+            t = hb.build_uniform(case["level"], gauss, norder=case["norder"], ipoly=case["ipoly"],
+                                 iperiod=case["iperiod"])
+        else:
+            t = hb.build_adaptive(gauss, norder=case["norder"], ipoly=case["ipoly"], iperiod=case["iperiod"],
+                                  eps=case["tree_eps"], maxlev=case["maxlev"])
+        if case.get("density") == "fourier22":
+            xy = t.grid_points()
+            t.fvals = np.sin(4 * np.pi * xy[..., 0]) * np.cos(4 * np.pi * xy[..., 1])
+        got, _, _ = call_boxfgt(t, case["delta"], case["eps"])
+        got = got.reshape(t.nboxes, -1)
+        idx = np.array(case["sample_idx"])
+        ref = np.array(case["sample_pot"])
+        err = rel_l2(got[idx[:, 0], idx[:, 1]], ref)
+        assert err < 10 * case["eps"], (case["name"], err)

@@ -1,0 +1,360 @@
+"""Benchmark: box FGT leaf points/s on the adaptive order-16 configuration.
+
+Workload (one "step" = one full boxfgt, steps 1-6, on the tree below, inputs
+resident in HBM): density = sum of 20 seeded Gaussians (centres uniform in the
+unit box, widths log-uniform in [1e-3, 1e-2], amplitudes N(0,1)); Legendre
+order 16 leaves, periodic unit box; tree uniform to level 8 and refined
+adaptively while the leaf Legendre tail exceeds 1e-10, max level 12 (~65.6k
+leaves, 16.8M points); nd = 1, delta = 1e-4, eps = 1e-6.  Synthetic data.
+
+Prints one JSON line (rank 0).  Under torchrun every rank runs its own
+independent tree (seed + rank): weak scaling, no collective on the data path;
+time = max over ranks of the device-timed region.
+
+--impl reference times the reference's CPU algorithm (the oracle: a C
+restatement of bfgt/boxfgt.f with the reference's OpenMP loops; the Fortran
+cannot be compiled in this image) on the box's host cores, same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "boxfgt leaf points/s at rel err 1e-6: split-TC batched vs plain FP64; % roofline"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+def make_tree(seed, small=False):
+    import heat2d_per_box_b200 as hb
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-0.5, 0.5, (20, 2))
+    w = np.exp(rng.uniform(np.log(1e-3), np.log(1e-2), 20))
+    a = rng.standard_normal(20)
+    g = hb.gauss_params(c, w, a)
+    minlev = 6 if small else 8
+    return hb.build_adaptive(g, norder=16, ipoly=0, iperiod=1, eps=1e-10, eta=1.0, minlev=minlev, maxlev=12)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append((time.time(), line.strip()))
+
+    def mark(self, begin):
+        if begin:
+            self.t0 = time.time()
+        else:
+            self.t1 = time.time()
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r for t, r in self.rows if self.t0 is None or (self.t0 - 0.2 <= t <= (self.t1 or t) + 0.2)]
+        if not rows:
+            rows = [r for _, r in self.rows]
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            f = [x.strip() for x in r.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+def run_reference(args, rank, world):
+    """CPU arm: the reference's algorithm (oracle) on the host cores, same workload."""
+    from oracle import oracle
+    if rank != 0:
+        return
+    t = make_tree(2)
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    delta, eps = args.delta, args.eps
+    for _ in range(args.warmup):
+        oracle.boxfgt(t, t.fvals, delta, eps)
+    npts = len(t.leaves()) * t.npbox
+    # each step is one full transform; cap the number so the arm ends in minutes
+    t0 = time.perf_counter()
+    oracle.boxfgt(t, t.fvals, delta, eps)
+    one = time.perf_counter() - t0
+    steps = max(1, min(args.steps, int(math.ceil(120.0 / max(one, 1e-3)))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        oracle.boxfgt(t, t.fvals, delta, eps)
+    el = time.perf_counter() - t0
+    v = npts * steps / el
+    line = {"metric": METRIC, "value": v, "unit": "leaf points/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": el / steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "adaptive order-16 periodic tree, 20 Gaussians, delta=1e-4, eps=1e-6",
+                       "leaves": int(len(t.leaves())), "points": int(npts), "nd": 1, "delta": delta, "eps": eps},
+            "cpu_baseline": {"value": v, "unit": "leaf points/s", "cores": threads, "kind": "port",
+                             "sample": f"{steps} full transforms of the workload tree (oracle, OpenMP "
+                                       f"{threads} threads; bfgt/boxfgt.f restated in C)"},
+            "e2e": {"value": v, "unit": "leaf points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--delta", type=float, default=1e-4)
+    ap.add_argument("--eps", type=float, default=1e-6)
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "split"])
+    ap.add_argument("--small", action="store_true", help="level-6 base tree (for profiler captures)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import heat2d_per_box_b200 as hb
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    tree = make_tree(2 + rank, small=args.small)
+    leaves = tree.leaves()
+    npts = len(leaves) * tree.npbox
+    precs = {"fp64": [hb.BFGT_PREC_FP64], "split": [hb.BFGT_PREC_SPLIT]}.get(args.precision)
+    if precs is None:
+        precs = [hb.BFGT_PREC_FP64]
+        try:
+            hb.Plan(tree, args.delta, args.eps, precision=hb.BFGT_PREC_SPLIT).close()
+            precs = [hb.BFGT_PREC_SPLIT, hb.BFGT_PREC_FP64]
+        except hb.BfgtError:
+            pass
+
+    hbm, bf16, bf16s, peak_src = peaks()
+    f = torch.from_numpy(tree.fvals.reshape(-1)).to(dev)
+    results = {}
+    stream = torch.cuda.current_stream()
+    clocks = None
+    for prec in precs:
+        plan = hb.Plan(tree, args.delta, args.eps, precision=prec)
+        pot = torch.zeros_like(f)
+        for _ in range(args.warmup):
+            plan.execute(f, pot, stream)
+        plan.reserve_events(args.steps + 8)
+        torch.cuda.synchronize()
+        plan.stage_ms()
+        sampler = ClockSampler(dev.index) if prec == precs[0] else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.4)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        if sampler:
+            sampler.mark(True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.execute(f, pot, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.mark(False)
+        ms = e0.elapsed_time(e1)
+        if dist:
+            tt = torch.tensor([ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        st = plan.stage_ms()
+        if sampler:
+            clocks = sampler.stop()
+        nst = max(st[6], 1)
+        work = plan.work()
+        info = plan.info()
+        stage_names = ["form", "reduce", "translate", "eval", "near"]
+        stage_avg = {nm: st[i] / nst for i, nm in enumerate(stage_names)}
+        results[prec] = dict(ms=ms, stage=stage_avg, work=work, info=info, plan=plan)
+        # correctness of this run against a fresh single execute is covered by the tests
+
+    main_prec = precs[0]
+    R = results[main_prec]
+    ms_step = R["ms"] / args.steps
+    value = npts * world / (ms_step * 1e-3)
+    # roofline of the dominant kernel (largest share of the step)
+    stg = R["stage"]
+    dom = max(("form", "eval", "near"), key=lambda k: stg[k])
+    w = R["work"]
+    dom_ms = stg[dom]
+    fl = {"form": w["flops_form"], "eval": w["flops_eval"], "near": w["flops_near"]}[dom]
+    by = {"form": w["bytes_form"], "eval": w["bytes_eval"], "near": w["bytes_near"]}[dom]
+    tcf = {"form": w["tc_flops_form"], "eval": w["tc_flops_eval"], "near": 0.0}[dom]
+    hbm_ach = by / (dom_ms * 1e-3) / 1e9
+    if main_prec == hb.BFGT_PREC_SPLIT and tcf > 0:
+        tc_ach = fl / (dom_ms * 1e-3) / 1e12
+        if tc_ach / bf16 >= hbm_ach / hbm:
+            roof = {"bound": "tensor", "achieved": tc_ach, "peak": bf16, "unit": "TFLOP/s", "frac": tc_ach / bf16}
+        else:
+            roof = {"bound": "hbm", "achieved": hbm_ach, "peak": hbm, "unit": "GB/s", "frac": hbm_ach / hbm}
+        roof["tensor_flops_issued_per_launch"] = tcf
+        roof["tensor_issue_rate_tflops"] = tcf / (dom_ms * 1e-3) / 1e12
+    else:
+        roof = {"bound": "hbm", "achieved": hbm_ach, "peak": hbm, "unit": "GB/s", "frac": hbm_ach / hbm}
+        roof["fp64_tflops"] = fl / (dom_ms * 1e-3) / 1e12
+        roof["fp64_frac_of_nominal_40tf"] = roof["fp64_tflops"] / 40.0
+    roof.update({"kernel": dom, "kernel_ms": dom_ms, "algorithmic_flop_per_launch": fl,
+                 "algorithmic_bytes_per_launch": by, "peak_source": peak_src, "traffic": None})
+    prof = ROOT / "profiles" / "traffic.json"
+    if prof.exists():
+        try:
+            tr = json.loads(prof.read_text()).get(f"{'split' if main_prec else 'fp64'}_{dom}")
+            if tr:
+                roof["traffic"] = tr
+        except Exception:
+            pass
+
+    # end-to-end through the C ABI with host buffers (pinned), copies inside the timed region
+    e2e = None
+    plan = R["plan"]
+    nelem = tree.nboxes * tree.npbox
+    hf = torch.from_numpy(tree.fvals.reshape(-1).copy()).pin_memory()
+    hp = torch.zeros(nelem, dtype=torch.float64).pin_memory()
+    hf_np, hp_np = hf.numpy(), hp.numpy()
+    ne = max(3, min(args.steps, 50))
+    plan.execute_host(hf_np, hp_np)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(ne):
+        plan.execute_host(hf_np, hp_np)
+    el = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([el], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        el = float(tt.item())
+    e2e = {"value": npts * world * ne / el, "unit": "leaf points/s", "h2d_bytes_per_step": 2 * nelem * 8,
+           "d2h_bytes_per_step": nelem * 8, "api": "bfgt_plan_execute_host (C ABI, pinned host arrays)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        oracle.boxfgt(tree, tree.fvals, args.delta, args.eps)
+        reps = 0
+        t0 = time.perf_counter()
+        while True:
+            oracle.boxfgt(tree, tree.fvals, args.delta, args.eps)
+            reps += 1
+            if time.perf_counter() - t0 > 10.0 or reps >= 20:
+                break
+        el = time.perf_counter() - t0
+        cpu = {"value": npts * reps / el, "unit": "leaf points/s", "cores": threads, "kind": "port",
+               "sample": f"{reps} full transforms of the same tree (oracle: bfgt/boxfgt.f restated in C, "
+                         f"OpenMP {threads} threads)"}
+
+    nlaunch_step = 4 + (1 if R["info"]["nnear_targets"] > 0 else 0)
+    line = {
+        "metric": METRIC, "value": value, "unit": "leaf points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if main_prec == hb.BFGT_PREC_FP64 else "f16-split/f32acc/f64",
+        "data": "synthetic",
+        "config": {"workload": "adaptive order-16 periodic tree, 20 Gaussians (w log-U[1e-3,1e-2], a~N(0,1)), "
+                               "uniform to level 8 then tail<1e-10, max level 12; nd=1, delta=1e-4, eps=1e-6",
+                   "leaves": int(len(leaves)), "points_per_gpu": int(npts), "nd": 1, "delta": args.delta,
+                   "eps": args.eps, "norder": 16, "npw": R["info"]["npw"], "npwlevel": R["info"]["npwlevel"],
+                   "precision": "split" if main_prec == hb.BFGT_PREC_SPLIT else "fp64",
+                   "l2": "inputs larger than L2 (leaf fvals + pot = %.0f MB per step)" % (npts * 24 / 1e6),
+                   "parallelism": f"replicas x{world} (independent trees)"},
+        "roofline": roof,
+        "stage_ms": {k: round(v, 5) for k, v in stg.items()},
+        "clocks": clocks,
+        "e2e": e2e,
+        "gpu_launches": nlaunch_step * args.steps,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    if hb.BFGT_PREC_FP64 in results and main_prec != hb.BFGT_PREC_FP64:
+        F = results[hb.BFGT_PREC_FP64]
+        line["fp64_value"] = npts * world / (F["ms"] / args.steps * 1e-3)
+        line["split_over_fp64"] = value / line["fp64_value"]
+        line["fp64_stage_ms"] = {k: round(v, 5) for k, v in F["stage"].items()}
+    for r in results.values():
+        r["plan"].close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -70,6 +70,8 @@ def lib():
     L.bfgt_plan_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
     L.bfgt_plan_stage_ms.restype = C.c_int
     L.bfgt_plan_stage_ms.argtypes = [C.c_void_p, _f64p]
+    L.bfgt_plan_reserve_events.restype = C.c_int
+    L.bfgt_plan_reserve_events.argtypes = [C.c_void_p, C.c_int]
     L.bfgt_plan_info.restype = C.c_int
     L.bfgt_plan_info.argtypes = [C.c_void_p, _i32p]
     L.bfgt_plan_work.restype = C.c_int

@@ -98,9 +98,13 @@ class Plan:
         _lib.check(self._L.bfgt_plan_graph_launch(self._h, s))
 
     def stage_ms(self):
+        """Per-stage device ms summed over the executes since the last call (see bfgt_plan_stage_ms)."""
         out = np.zeros(8)
         _lib.check(self._L.bfgt_plan_stage_ms(self._h, out))
         return out
+
+    def reserve_events(self, n):
+        _lib.check(self._L.bfgt_plan_reserve_events(self._h, int(n)))
 
     def info(self):
         out = np.zeros(16, np.int32)
@@ -110,9 +114,11 @@ class Plan:
         return {k: int(out[i]) for i, k in enumerate(keys)}
 
     def work(self):
-        out = np.zeros(4)
+        out = np.zeros(16)
         _lib.check(self._L.bfgt_plan_work(self._h, out))
-        return {"flops": out[0], "bytes": out[1], "tc_flops": out[2], "points": out[3]}
+        keys = ["flops", "bytes", "tc_flops", "points", "flops_form", "flops_eval", "flops_near", "flops_translate",
+                "bytes_form", "bytes_eval", "bytes_near", "tc_flops_form", "tc_flops_eval"]
+        return {k: float(out[i]) for i, k in enumerate(keys)}
 
     def close(self):
         if getattr(self, "_h", None):

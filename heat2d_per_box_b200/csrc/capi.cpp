@@ -174,16 +174,14 @@ int bfgt_plan_graph_launch(bfgt_plan plan, void *stream) {
 int bfgt_plan_stage_ms(bfgt_plan plan, double *out) {
   g_err.clear();
   if (!plan || !out) return fail(BFGT_ERR_ARG, "NULL argument");
-  bfgt::DevicePlan &dp = plan->dp;
-  for (int i = 0; i < 8; i++) out[i] = 0;
-  if (!dp.events) return BFGT_OK;
-  if (cudaEventSynchronize(dp.ev[5]) != cudaSuccess) return fail(BFGT_ERR_CUDA, "event sync failed");
-  float ms;
-  for (int i = 0; i < 5; i++) {
-    if (cudaEventElapsedTime(&ms, dp.ev[i], dp.ev[i + 1]) == cudaSuccess) out[i] = ms;
-  }
-  if (cudaEventElapsedTime(&ms, dp.ev[0], dp.ev[5]) == cudaSuccess) out[5] = ms;
-  cudaGetLastError();
+  if (bfgt::device_plan_stage_ms(plan->dp, out) != BFGT_OK) return fail(BFGT_ERR_CUDA, "event read-out failed");
+  return BFGT_OK;
+}
+
+int bfgt_plan_reserve_events(bfgt_plan plan, int n) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (bfgt::device_plan_reserve_events(plan->dp, n) != BFGT_OK) return fail(BFGT_ERR_CUDA, "event creation failed");
   return BFGT_OK;
 }
 
@@ -214,6 +212,15 @@ int bfgt_plan_work(bfgt_plan plan, double *out) {
   out[1] = plan->hp.bytes;
   out[2] = plan->hp.tc_flops;
   out[3] = plan->hp.points;
+  out[4] = plan->hp.flops_form;
+  out[5] = plan->hp.flops_eval;
+  out[6] = plan->hp.flops_near;
+  out[7] = plan->hp.flops_translate;
+  out[8] = plan->hp.bytes_form;
+  out[9] = plan->hp.bytes_eval;
+  out[10] = plan->hp.bytes_near;
+  out[11] = plan->hp.tc_flops_form;
+  out[12] = plan->hp.tc_flops_eval;
   return BFGT_OK;
 }
 
@@ -237,7 +244,7 @@ int bfgt_boxfgt(int nd, double delta, double eps, int ipoly, int iperiod, int no
   rc = bfgt_plan_execute_host(plan, fvals, pot, nullptr);
   if (rc == BFGT_OK && timeinfo) {
     double st[8];
-    bfgt_plan_stage_ms(plan, st);
+    bfgt::device_plan_stage_ms(plan->dp, st);
     for (int i = 0; i < 20; i++) timeinfo[i] = 0;
     timeinfo[0] = t1 - t0;           // step 0: precomputation
     timeinfo[1] = st[0] * 1e-3;      // steps 1+2: leaf -> cutoff expansions

@@ -3,7 +3,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
+#include <vector>
 
 #include "host_plan.hpp"
 
@@ -20,7 +22,10 @@ struct DevicePlan {
   double2 *PH = nullptr;        // phase tables
   long long *ph_off = nullptr;  // per level offsets into PH
   int4 *leaves = nullptr;       // {box, ox, oy, level}
-  int4 *chunks = nullptr;       // {begin, end, icut, level}
+  int4 *chunks = nullptr;       // {column begin, column end, icut, level}
+  int4 *columns = nullptr;      // {leaf begin, leaf end, ox, -}
+  int ncolumns = 0;
+  int form_tile[3] = {0, 0, 0}, eval_tile[3] = {0, 0, 0};
   int *cut_chunk_begin = nullptr, *cut_pw_begin = nullptr, *cut_pw_src = nullptr, *cut_pw_ind = nullptr;
   double2 *W = nullptr;         // cutoff shifts (nexp, 9)
   double *pw_weight = nullptr;  // (hh)
@@ -39,8 +44,9 @@ struct DevicePlan {
   double *h_stage_f = nullptr, *h_stage_p = nullptr;  // pinned
   double *d_stage_f = nullptr, *d_stage_p = nullptr;
   size_t stage_elems = 0;
-  // timing
-  cudaEvent_t ev[8] = {};
+  // timing: one set of stage events per execute since the last read-out
+  std::vector<std::array<cudaEvent_t, 6>> evsets;
+  int nrec = 0;
   bool events = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -53,5 +59,10 @@ void device_plan_destroy(DevicePlan &dp);
 // Queues the transform on stream; returns BFGT_* status.
 int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cudaStream_t stream,
                         std::string &msg);
+// Makes sure at least n event sets exist (no event creation inside timed loops).
+int device_plan_reserve_events(DevicePlan &dp, int n);
+// Sums the stage times of every execute since the last call; out[0..4] stage
+// ms, out[5] total ms, out[6] number of executes summed.
+int device_plan_stage_ms(DevicePlan &dp, double *out);
 
 }  // namespace bfgt

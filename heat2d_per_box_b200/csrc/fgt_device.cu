@@ -19,6 +19,7 @@
 //   periodic level-1 images of boxfgt.f:938-1053.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -47,8 +48,9 @@ constexpr int kWarps = 4;
 
 struct FormArgs {
   const double *fvals;
-  const int4 *leaves;
-  const int4 *chunks;
+  const int4 *leaves;   // {box, ox, oy, level}, sorted by (icut, level, ox, oy)
+  const int4 *columns;  // {leaf begin, leaf end, ox, -}
+  const int4 *chunks;   // {column begin, column end, icut, level}
   const double2 *T;
   const double2 *PH;
   const long long *ph_off;
@@ -56,113 +58,132 @@ struct FormArgs {
   int nd, n, npw, hh, nexp;
 };
 
-// One CTA per chunk (leaves with the same cutoff ancestor and level).  Warp w
-// takes leaves w, w+4, ... of the chunk; for each leaf and density it forms
-//   ff(m1,k2) = ey(k2) sum_m2 F(m1,m2) T(m2,k2)
-//   M(k1,k2) += ex(k1) sum_m1 T(m1,k1) ff(m1,k2)
-// with ex, ey the conjugate phases from the leaf to the ancestor centre.  The
-// (k1,k2) outputs are cut into TM x TN tiles dealt round-robin to the lanes.
-template <int TM, int TN>
-__global__ void __launch_bounds__(kWarps * 32) k_form_fp64(FormArgs a) {
+// Leaf values -> cutoff expansions, sum-factorised over a column of leaves.
+// One CTA per chunk (columns of one cutoff ancestor and level), one warp per
+// column.  With Ty(m2,k2) = T(m2,k2) conj(ph_oy(k2)) and
+// Tx(m1,k1) = T(m1,k1) conj(ph_ox(k1)) (ph = exp(i ts.(c_leaf-c_anc)/sqrt(delta0))),
+//   Y(m1,k2)   = sum_{leaves of the column} sum_m2 F(m1,m2) Ty(m2,k2)
+//   M(k1,k2)  += sum_m1 Tx(m1,k1) Y(m1,k2)
+// which equals sum over the column's leaves of the reference's step-1
+// expansion shifted to the ancestor (steps 1+2, boxfgt.f:728-783).  The M
+// accumulators of a warp stay in registers (NT tiles of TM x TN per lane)
+// across its columns; warps are then summed in a fixed order.
+template <int TM, int TN, int NT>
+__global__ void __launch_bounds__(kWarps * 32, 3) k_form_fp64(FormArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int4 ch = a.chunks[blockIdx.x];
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double2 *sT = reinterpret_cast<double2 *>(smem_raw);  // [m][k], n x npw
-  const size_t per_warp = (size_t)npw * hh + (size_t)n * hh + npw + hh + (npb + 1) / 2;
-  double2 *wb = sT + (size_t)n * npw + per_warp * warp;
-  double2 *sM = wb;                      // [k2][k1]
-  double2 *sff = sM + (size_t)npw * hh;  // [m1][k2]
-  double2 *sex = sff + (size_t)n * hh;
-  double2 *sey = sex + npw;
-  double *sF = reinterpret_cast<double *>(sey + hh);  // [m2][m1]
+  double2 *sRed = sT + (size_t)n * npw;                  // npw x hh, [k2][k1]
+  const size_t per_warp = (size_t)n * hh + npw + hh + (npb + 1) / 2;
+  double2 *wb = sRed + (size_t)npw * hh + per_warp * warp;
+  double2 *sY = wb;                    // [m1][k2]
+  double2 *sphx = sY + (size_t)n * hh;
+  double2 *sphy = sphx + npw;
+  double *sF = reinterpret_cast<double *>(sphy + hh);  // [m2][m1]
 
   const double2 *Tg = a.T + (size_t)n * npw * ch.w;
   for (int i = threadIdx.x; i < n * npw; i += blockDim.x) {
-    int m = i % n, k = i / n;
+    const int m = i % n, k = i / n;
     sT[m * npw + k] = Tg[i];
   }
   __syncthreads();
+  const long long phoff = a.ph_off[ch.w];
   const int ntm = (npw + TM - 1) / TM, ntn = (hh + TN - 1) / TN, ntiles = ntm * ntn;
   for (int ind = 0; ind < nd; ind++) {
-    for (int e = lane; e < npw * hh; e += 32) sM[e] = make_double2(0, 0);
-    __syncwarp();
-    for (int li = ch.x + warp; li < ch.y; li += kWarps) {
-      const int4 lf = a.leaves[li];
-      const double *fv = a.fvals + (size_t)lf.x * nd * npb;
-      for (int j = lane; j < npb; j += 32) sF[j] = fv[ind + (size_t)nd * j];
-      const double2 *phx = a.PH + a.ph_off[lf.w] + (size_t)lf.y * npw;
-      const double2 *phy = a.PH + a.ph_off[lf.w] + (size_t)lf.z * npw;
+    double2 M[NT][TM][TN];
+#pragma unroll
+    for (int t = 0; t < NT; t++)
+#pragma unroll
+      for (int i = 0; i < TM; i++)
+#pragma unroll
+        for (int j = 0; j < TN; j++) M[t][i][j] = make_double2(0, 0);
+    for (int c = ch.x + warp; c < ch.y; c += kWarps) {
+      const int4 col = a.columns[c];
+      for (int e = lane; e < n * hh; e += 32) sY[e] = make_double2(0, 0);
+      const double2 *phx = a.PH + phoff + (size_t)col.z * npw;
       for (int k = lane; k < npw; k += 32) {
-        double2 p = phx[k];
-        sex[k] = make_double2(p.x, -p.y);
+        const double2 p = phx[k];
+        sphx[k] = make_double2(p.x, -p.y);
       }
-      for (int k = lane; k < hh; k += 32) {
-        double2 p = phy[k];
-        sey[k] = make_double2(p.x, -p.y);
-      }
-      __syncwarp();
-      for (int o = lane; o < n * hh; o += 32) {
-        const int m1 = o / hh, k2 = o - m1 * hh;
-        double2 acc = make_double2(0, 0);
-        for (int m2 = 0; m2 < n; m2++) {
-          const double f = sF[m1 + n * m2];
-          const double2 t = sT[m2 * npw + k2];
-          acc.x = fma(f, t.x, acc.x);
-          acc.y = fma(f, t.y, acc.y);
+      for (int li = col.x; li < col.y; li++) {
+        const int4 lf = a.leaves[li];
+        const double *fv = a.fvals + (size_t)lf.x * nd * npb;
+        __syncwarp();
+        for (int j = lane; j < npb; j += 32) sF[j] = fv[ind + (size_t)nd * j];
+        const double2 *phy = a.PH + phoff + (size_t)lf.z * npw;
+        for (int k = lane; k < hh; k += 32) {
+          const double2 p = phy[k];
+          sphy[k] = make_double2(p.x, -p.y);
         }
-        sff[m1 * hh + k2] = cmul(acc, sey[k2]);
+        __syncwarp();
+        for (int o = lane; o < n * hh; o += 32) {
+          const int m1 = o / hh, k2 = o - m1 * hh;
+          double2 acc = make_double2(0, 0);
+#pragma unroll 4
+          for (int m2 = 0; m2 < n; m2++) {
+            const double f = sF[m1 + n * m2];
+            const double2 t = sT[m2 * npw + k2];
+            acc.x = fma(f, t.x, acc.x);
+            acc.y = fma(f, t.y, acc.y);
+          }
+          const double2 v = cmul(acc, sphy[k2]);
+          sY[o].x += v.x;
+          sY[o].y += v.y;
+        }
       }
       __syncwarp();
-      for (int tile = lane; tile < ntiles; tile += 32) {
+#pragma unroll
+      for (int t = 0; t < NT; t++) {
+        const int tile = lane + 32 * t;
+        if (tile >= ntiles) continue;
         const int k1b = (tile % ntm) * TM, k2b = (tile / ntm) * TN;
-        double2 P[TM][TN];
+        double2 ph[TM];
 #pragma unroll
-        for (int i = 0; i < TM; i++)
-#pragma unroll
-          for (int j = 0; j < TN; j++) P[i][j] = make_double2(0, 0);
+        for (int i = 0; i < TM; i++) ph[i] = (k1b + i < npw) ? sphx[k1b + i] : make_double2(0, 0);
+#pragma unroll 2
         for (int m1 = 0; m1 < n; m1++) {
           double2 av[TM], bv[TN];
 #pragma unroll
-          for (int i = 0; i < TM; i++) av[i] = (k1b + i < npw) ? sT[m1 * npw + k1b + i] : make_double2(0, 0);
+          for (int i = 0; i < TM; i++) av[i] = cmul((k1b + i < npw) ? sT[m1 * npw + k1b + i] : make_double2(0, 0), ph[i]);
 #pragma unroll
-          for (int j = 0; j < TN; j++) bv[j] = (k2b + j < hh) ? sff[m1 * hh + k2b + j] : make_double2(0, 0);
+          for (int j = 0; j < TN; j++) bv[j] = (k2b + j < hh) ? sY[m1 * hh + k2b + j] : make_double2(0, 0);
 #pragma unroll
           for (int i = 0; i < TM; i++)
 #pragma unroll
-            for (int j = 0; j < TN; j++) cfma(P[i][j], av[i], bv[j]);
-        }
-#pragma unroll
-        for (int i = 0; i < TM; i++) {
-          const int k1 = k1b + i;
-          if (k1 >= npw) continue;
-          const double2 ex = sex[k1];
-#pragma unroll
-          for (int j = 0; j < TN; j++) {
-            const int k2 = k2b + j;
-            if (k2 >= hh) continue;
-            double2 &m = sM[k2 * npw + k1];
-            const double2 v = cmul(ex, P[i][j]);
-            m.x += v.x;
-            m.y += v.y;
-          }
+            for (int j = 0; j < TN; j++) cfma(M[t][i][j], av[i], bv[j]);
         }
       }
       __syncwarp();
     }
-    __syncthreads();
-    // fixed-order reduction of the warps' partial expansions
-    double2 *out = a.Mpart + ((size_t)blockIdx.x * nd + ind) * a.nexp;
-    const double2 *w0 = sT + (size_t)n * npw;
-    for (int e = threadIdx.x; e < a.nexp; e += blockDim.x) {
-      double2 s = make_double2(0, 0);
-      for (int w = 0; w < kWarps; w++) {
-        const double2 v = w0[per_warp * w + e];
-        s.x += v.x;
-        s.y += v.y;
+    // fixed-order sum of the warps' accumulators: warp 0 stores, 1..3 add
+    for (int w = 0; w < kWarps; w++) {
+      if (warp == w) {
+#pragma unroll
+        for (int t = 0; t < NT; t++) {
+          const int tile = lane + 32 * t;
+          if (tile >= ntiles) continue;
+          const int k1b = (tile % ntm) * TM, k2b = (tile / ntm) * TN;
+#pragma unroll
+          for (int i = 0; i < TM; i++)
+#pragma unroll
+            for (int j = 0; j < TN; j++) {
+              if (k1b + i >= npw || k2b + j >= hh) continue;
+              double2 &r = sRed[(k2b + j) * npw + k1b + i];
+              if (w == 0) {
+                r = M[t][i][j];
+              } else {
+                r.x += M[t][i][j].x;
+                r.y += M[t][i][j].y;
+              }
+            }
+        }
       }
-      out[e] = s;
+      __syncthreads();
     }
+    double2 *out = a.Mpart + ((size_t)blockIdx.x * nd + ind) * a.nexp;
+    for (int e = threadIdx.x; e < a.nexp; e += blockDim.x) out[e] = sRed[e];
     __syncthreads();
   }
 }
@@ -204,6 +225,7 @@ __global__ void k_translate(const double2 *__restrict__ M, const int *__restrict
 struct EvalArgs {
   double *pot;
   const int4 *leaves;
+  const int4 *columns;
   const int4 *chunks;
   const double2 *E;
   const double2 *PH;
@@ -213,88 +235,106 @@ struct EvalArgs {
   int nd, n, npw, hh, nexp;
 };
 
-// One CTA per chunk.  For each leaf and density:
-//   L'(m1,m2) = L(m1,m2) ex(m1) ey(m2) w(m2)        (split phases, FP64)
-//   G(k1,m2)  = sum_m1 E(m1,k1) L'(m1,m2)
-//   pot(k1,k2) += 2 Re sum_m2 E(m2,k2) G(k1,m2)
-template <int GM, int GN>
+// Cutoff expansions -> leaf values (steps 4+5, boxfgt.f:845-900), sum-factorised
+// over a column: one warp per column computes
+//   H(k1,m2) = sum_m1 E(m1,k1) ph_ox(m1) L(m1,m2)          (once per column)
+// and for each leaf of the column
+//   pot(k1,k2) += 2 Re sum_m2 H(k1,m2) w(m2) ph_oy(m2) E(m2,k2)
+// with w = 1/2 on the zero frequency of an odd npw (g2d_pw2pot).
+template <int GM, int GN, int NG>
 __global__ void __launch_bounds__(kWarps * 32) k_eval_fp64(EvalArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int4 ch = a.chunks[blockIdx.x];
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double2 *sE = reinterpret_cast<double2 *>(smem_raw);  // [m][k] (npw x n, k fastest)
-  double2 *sL = sE + (size_t)npw * n;                    // [m2][m1]
-  const size_t per_warp = (size_t)npw * hh + (size_t)n * hh + npw + hh;
+  double2 *sL = sE + (size_t)npw * n;                    // [m1][m2]
+  const size_t per_warp = (size_t)n * hh + npw + hh;
   double2 *wb = sL + (size_t)npw * hh + per_warp * warp;
-  double2 *sLp = wb;                     // [m1][m2]
-  double2 *sG = sLp + (size_t)npw * hh;  // [m2][k1]
-  double2 *sex = sG + (size_t)n * hh;
-  double2 *sey = sex + npw;
+  double2 *sHp = wb;                    // [m2][k1]
+  double2 *sphx = sHp + (size_t)n * hh;
+  double2 *sphy = sphx + npw;
   const double2 *Eg = a.E + (size_t)n * npw * ch.w;  // Fortran (npw, n)
   for (int i = threadIdx.x; i < n * npw; i += blockDim.x) {
     const int m = i % npw, k = i / npw;
     sE[m * n + k] = Eg[i];
   }
+  const long long phoff = a.ph_off[ch.w];
   const int ntm = (n + GM - 1) / GM, ntn = (hh + GN - 1) / GN, ntiles = ntm * ntn;
   for (int ind = 0; ind < nd; ind++) {
     const double2 *Lg = a.L + ((size_t)ch.z * nd + ind) * a.nexp;
-    for (int e = threadIdx.x; e < a.nexp; e += blockDim.x) sL[e] = Lg[e];
+    for (int e = threadIdx.x; e < a.nexp; e += blockDim.x) {
+      const int m2 = e / npw, m1 = e - m2 * npw;
+      sL[m1 * hh + m2] = Lg[e];
+    }
     __syncthreads();
-    for (int li = ch.x + warp; li < ch.y; li += kWarps) {
-      const int4 lf = a.leaves[li];
-      const double2 *phx = a.PH + a.ph_off[lf.w] + (size_t)lf.y * npw;
-      const double2 *phy = a.PH + a.ph_off[lf.w] + (size_t)lf.z * npw;
-      for (int k = lane; k < npw; k += 32) sex[k] = phx[k];
-      for (int k = lane; k < hh; k += 32) {
-        double2 p = phy[k];
-        const double w = a.pw_weight[k];
-        sey[k] = make_double2(p.x * w, p.y * w);
-      }
+    for (int c = ch.x + warp; c < ch.y; c += kWarps) {
+      const int4 col = a.columns[c];
+      const double2 *phx = a.PH + phoff + (size_t)col.z * npw;
+      for (int k = lane; k < npw; k += 32) sphx[k] = phx[k];
       __syncwarp();
-      for (int e = lane; e < npw * hh; e += 32) {
-        const int m2 = e / npw, m1 = e - m2 * npw;
-        sLp[m1 * hh + m2] = cmul(cmul(sL[e], sex[m1]), sey[m2]);
-      }
-      __syncwarp();
-      for (int tile = lane; tile < ntiles; tile += 32) {
-        const int k1b = (tile % ntm) * GM, m2b = (tile / ntm) * GN;
-        double2 G[GM][GN];
+      double2 H[NG][GM][GN];
+#pragma unroll
+      for (int t = 0; t < NG; t++) {
 #pragma unroll
         for (int i = 0; i < GM; i++)
 #pragma unroll
-          for (int j = 0; j < GN; j++) G[i][j] = make_double2(0, 0);
+          for (int j = 0; j < GN; j++) H[t][i][j] = make_double2(0, 0);
+        const int tile = lane + 32 * t;
+        if (tile >= ntiles) continue;
+        const int k1b = (tile % ntm) * GM, m2b = (tile / ntm) * GN;
+#pragma unroll 2
         for (int m1 = 0; m1 < npw; m1++) {
+          const double2 p = sphx[m1];
           double2 av[GM], bv[GN];
 #pragma unroll
-          for (int i = 0; i < GM; i++) av[i] = (k1b + i < n) ? sE[m1 * n + k1b + i] : make_double2(0, 0);
+          for (int i = 0; i < GM; i++) av[i] = cmul((k1b + i < n) ? sE[m1 * n + k1b + i] : make_double2(0, 0), p);
 #pragma unroll
-          for (int j = 0; j < GN; j++) bv[j] = (m2b + j < hh) ? sLp[m1 * hh + m2b + j] : make_double2(0, 0);
+          for (int j = 0; j < GN; j++) bv[j] = (m2b + j < hh) ? sL[m1 * hh + m2b + j] : make_double2(0, 0);
 #pragma unroll
           for (int i = 0; i < GM; i++)
 #pragma unroll
-            for (int j = 0; j < GN; j++) cfma(G[i][j], av[i], bv[j]);
-        }
-#pragma unroll
-        for (int i = 0; i < GM; i++) {
-          if (k1b + i >= n) continue;
-#pragma unroll
-          for (int j = 0; j < GN; j++)
-            if (m2b + j < hh) sG[(m2b + j) * n + k1b + i] = G[i][j];
+            for (int j = 0; j < GN; j++) cfma(H[t][i][j], av[i], bv[j]);
         }
       }
-      __syncwarp();
-      double *pb = a.pot + (size_t)lf.x * nd * npb;
-      for (int o = lane; o < npb; o += 32) {
-        const int k1 = o % n, k2 = o / n;
-        double acc = 0;
-        for (int m2 = 0; m2 < hh; m2++) {
-          const double2 e = sE[m2 * n + k2];
-          const double2 g = sG[m2 * n + k1];
-          acc = fma(e.x, g.x, acc);
-          acc = fma(-e.y, g.y, acc);
+      for (int li = col.x; li < col.y; li++) {
+        const int4 lf = a.leaves[li];
+        const double2 *phy = a.PH + phoff + (size_t)lf.z * npw;
+        __syncwarp();
+        for (int k = lane; k < hh; k += 32) {
+          const double2 p = phy[k];
+          const double w = a.pw_weight[k];
+          sphy[k] = make_double2(p.x * w, p.y * w);
         }
-        pb[ind + (size_t)nd * o] += 2 * acc;
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < NG; t++) {
+          const int tile = lane + 32 * t;
+          if (tile >= ntiles) continue;
+          const int k1b = (tile % ntm) * GM, m2b = (tile / ntm) * GN;
+#pragma unroll
+          for (int j = 0; j < GN; j++) {
+            if (m2b + j >= hh) continue;
+            const double2 p = sphy[m2b + j];
+#pragma unroll
+            for (int i = 0; i < GM; i++)
+              if (k1b + i < n) sHp[(m2b + j) * n + k1b + i] = cmul(H[t][i][j], p);
+          }
+        }
+        __syncwarp();
+        double *pb = a.pot + (size_t)lf.x * nd * npb;
+        for (int o = lane; o < npb; o += 32) {
+          const int k1 = o % n, k2 = o / n;
+          double acc = 0;
+#pragma unroll 4
+          for (int m2 = 0; m2 < hh; m2++) {
+            const double2 e = sE[m2 * n + k2];
+            const double2 g = sHp[m2 * n + k1];
+            acc = fma(e.x, g.x, acc);
+            acc = fma(-e.y, g.y, acc);
+          }
+          pb[ind + (size_t)nd * o] += 2 * acc;
+        }
       }
       __syncwarp();
     }
@@ -302,19 +342,21 @@ __global__ void __launch_bounds__(kWarps * 32) k_eval_fp64(EvalArgs a) {
   }
 }
 
-// tile shape with the fewest wasted lane-slots for an a x b output
+// tile shape (and tiles per lane) with the fewest wasted lane-slots for an
+// a x b output, at most maxnt tiles per lane
 struct TileChoice {
-  int tm, tn;
+  int tm, tn, nt;
 };
 inline TileChoice best_tile(int a, int b, const TileChoice *cands, int nc) {
-  TileChoice best = cands[0];
+  TileChoice best{0, 0, 0};
   double beff = -1;
   for (int i = 0; i < nc; i++) {
     const int tm = cands[i].tm, tn = cands[i].tn;
     const int tiles = ((a + tm - 1) / tm) * ((b + tn - 1) / tn);
-    const int passes = (tiles + 31) / 32;
-    const double eff = (double)a * b / (32.0 * passes * tm * tn);
-    if (eff > beff + 1e-9 || (std::abs(eff - beff) <= 1e-9 && tm * tn > best.tm * best.tn)) {
+    const int nt = (tiles + 31) / 32;
+    if (nt != cands[i].nt) continue;
+    const double eff = (double)a * b / (32.0 * nt * tm * tn);
+    if (eff > beff + 1e-9) {
       beff = eff;
       best = cands[i];
     }
@@ -322,42 +364,45 @@ inline TileChoice best_tile(int a, int b, const TileChoice *cands, int nc) {
   return best;
 }
 
-const TileChoice kFormTiles[] = {{4, 4}, {5, 4}, {4, 5}, {5, 5}, {6, 6}, {8, 4}};
-const TileChoice kEvalTiles[] = {{1, 5}, {2, 5}, {2, 4}, {4, 4}, {2, 8}, {4, 5}};
+const TileChoice kFormTiles[] = {{4, 4, 1}, {5, 4, 1}, {4, 5, 1}, {5, 5, 1}, {4, 4, 2}, {5, 5, 2}, {6, 4, 2},
+                                 {4, 6, 2}, {6, 6, 2}, {8, 4, 2}, {6, 6, 3}, {8, 8, 2}};
+const TileChoice kEvalTiles[] = {{1, 5, 1}, {2, 5, 1}, {2, 4, 1}, {4, 4, 1}, {2, 8, 1}, {4, 5, 1}, {2, 5, 2},
+                                 {4, 4, 2}, {4, 5, 2}, {4, 8, 2}, {4, 8, 3}, {8, 8, 2}};
+constexpr int kNFormTiles = sizeof(kFormTiles) / sizeof(kFormTiles[0]);
+constexpr int kNEvalTiles = sizeof(kEvalTiles) / sizeof(kEvalTiles[0]);
 
-void launch_form_fp64(const TileChoice &t, int grid, size_t smem, cudaStream_t s, const FormArgs &a) {
-#define FORM_CASE(M_, N_)                                                                    \
-  if (t.tm == M_ && t.tn == N_) {                                                            \
-    k_form_fp64<M_, N_><<<grid, kWarps * 32, smem, s>>>(a);                                  \
-    return;                                                                                  \
+#define FORM_LIST(X) X(4, 4, 1) X(5, 4, 1) X(4, 5, 1) X(5, 5, 1) X(4, 4, 2) X(5, 5, 2) X(6, 4, 2) X(4, 6, 2) X(6, 6, 2) X(8, 4, 2) X(6, 6, 3) X(8, 8, 2)
+#define EVAL_LIST(X) X(1, 5, 1) X(2, 5, 1) X(2, 4, 1) X(4, 4, 1) X(2, 8, 1) X(4, 5, 1) X(2, 5, 2) X(4, 4, 2) X(4, 5, 2) X(4, 8, 2) X(4, 8, 3) X(8, 8, 2)
+
+bool launch_form_fp64(const TileChoice &t, int grid, size_t smem, cudaStream_t s, const FormArgs &a) {
+#define FORM_CASE(M_, N_, T_)                                      \
+  if (t.tm == M_ && t.tn == N_ && t.nt == T_) {                    \
+    k_form_fp64<M_, N_, T_><<<grid, kWarps * 32, smem, s>>>(a);    \
+    return true;                                                   \
   }
-  FORM_CASE(4, 4) FORM_CASE(5, 4) FORM_CASE(4, 5) FORM_CASE(5, 5) FORM_CASE(6, 6) FORM_CASE(8, 4)
+  FORM_LIST(FORM_CASE)
 #undef FORM_CASE
+  return false;
 }
 
-void launch_eval_fp64(const TileChoice &t, int grid, size_t smem, cudaStream_t s, const EvalArgs &a) {
-#define EVAL_CASE(M_, N_)                                                                    \
-  if (t.tm == M_ && t.tn == N_) {                                                            \
-    k_eval_fp64<M_, N_><<<grid, kWarps * 32, smem, s>>>(a);                                  \
-    return;                                                                                  \
+bool launch_eval_fp64(const TileChoice &t, int grid, size_t smem, cudaStream_t s, const EvalArgs &a) {
+#define EVAL_CASE(M_, N_, T_)                                      \
+  if (t.tm == M_ && t.tn == N_ && t.nt == T_) {                    \
+    k_eval_fp64<M_, N_, T_><<<grid, kWarps * 32, smem, s>>>(a);    \
+    return true;                                                   \
   }
-  EVAL_CASE(1, 5) EVAL_CASE(2, 5) EVAL_CASE(2, 4) EVAL_CASE(4, 4) EVAL_CASE(2, 8) EVAL_CASE(4, 5)
+  EVAL_LIST(EVAL_CASE)
 #undef EVAL_CASE
+  return false;
 }
 
 void set_smem_attrs(int bytes) {
-  cudaFuncSetAttribute(k_form_fp64<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_form_fp64<5, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_form_fp64<4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_form_fp64<5, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_form_fp64<6, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_form_fp64<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_eval_fp64<1, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_eval_fp64<2, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_eval_fp64<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_eval_fp64<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_eval_fp64<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_eval_fp64<4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+#define FORM_ATTR(M_, N_, T_) cudaFuncSetAttribute(k_form_fp64<M_, N_, T_>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+#define EVAL_ATTR(M_, N_, T_) cudaFuncSetAttribute(k_eval_fp64<M_, N_, T_>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  FORM_LIST(FORM_ATTR)
+  EVAL_LIST(EVAL_ATTR)
+#undef FORM_ATTR
+#undef EVAL_ATTR
 }
 
 struct NearArgs {
@@ -489,11 +534,14 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     chk(upload(dp.W, W, msg));
     std::vector<long long> po(hp.phase_off.begin(), hp.phase_off.end());
     chk(upload(dp.ph_off, po, msg));
-    std::vector<int4> lv(hp.leaves.size()), cv(hp.chunks.size());
+    std::vector<int4> lv(hp.leaves.size()), cv(hp.chunks.size()), colv(hp.columns.size());
     for (size_t i = 0; i < lv.size(); i++) lv[i] = make_int4(hp.leaves[i].box, hp.leaves[i].ox, hp.leaves[i].oy, hp.leaves[i].level);
     for (size_t i = 0; i < cv.size(); i++) cv[i] = make_int4(hp.chunks[i].begin, hp.chunks[i].end, hp.chunks[i].icut, hp.chunks[i].level);
+    for (size_t i = 0; i < colv.size(); i++) colv[i] = make_int4(hp.columns[i].begin, hp.columns[i].end, hp.columns[i].ox, 0);
     chk(upload(dp.leaves, lv, msg));
     chk(upload(dp.chunks, cv, msg));
+    chk(upload(dp.columns, colv, msg));
+    dp.ncolumns = (int)colv.size();
     chk(upload(dp.cut_chunk_begin, hp.cut_chunk_begin, msg));
     chk(upload(dp.cut_pw_begin, hp.cut_pw_begin, msg));
     chk(upload(dp.cut_pw_src, hp.cut_pw_src, msg));
@@ -504,10 +552,18 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     chk(alloc_bytes((void **)&dp.M, ex * dp.ncut, msg));
     chk(alloc_bytes((void **)&dp.L, ex * dp.ncut, msg));
     const int npb = n * n;
-    dp.smem_form = sizeof(double2) * ((size_t)n * dp.npw +
-                                      (size_t)kWarps * ((size_t)dp.npw * dp.hh + (size_t)n * dp.hh + dp.npw + dp.hh + (npb + 1) / 2));
+    dp.smem_form = sizeof(double2) * ((size_t)n * dp.npw + (size_t)dp.npw * dp.hh +
+                                      (size_t)kWarps * ((size_t)n * dp.hh + dp.npw + dp.hh + (npb + 1) / 2));
     dp.smem_eval = sizeof(double2) * ((size_t)n * dp.npw + (size_t)dp.npw * dp.hh +
-                                      (size_t)kWarps * ((size_t)dp.npw * dp.hh + (size_t)n * dp.hh + dp.npw + dp.hh));
+                                      (size_t)kWarps * ((size_t)n * dp.hh + dp.npw + dp.hh));
+    const TileChoice ft = best_tile(dp.npw, dp.hh, kFormTiles, kNFormTiles);
+    const TileChoice et = best_tile(n, dp.hh, kEvalTiles, kNEvalTiles);
+    dp.form_tile[0] = ft.tm, dp.form_tile[1] = ft.tn, dp.form_tile[2] = ft.nt;
+    dp.eval_tile[0] = et.tm, dp.eval_tile[1] = et.tn, dp.eval_tile[2] = et.nt;
+    if (rc == BFGT_OK && (ft.nt == 0 || et.nt == 0)) {
+      msg = "npw=" + std::to_string(dp.npw) + " with norder=" + std::to_string(n) + " exceeds the built FP64 tile shapes";
+      rc = BFGT_ERR_CAPACITY;
+    }
     if (rc == BFGT_OK && dp.precision == BFGT_PREC_SPLIT) rc = split_plan_create(dp, hp, msg);
   }
   dp.nnf = (int)hp.nf_target.size();
@@ -532,8 +588,8 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   if (rc == BFGT_OK) {
     set_smem_attrs((int)smax);
     cudaFuncSetAttribute(k_near_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
-    for (int i = 0; i < 8; i++) cudaEventCreate(&dp.ev[i]);
     dp.events = true;
+    device_plan_reserve_events(dp, 8);
     if (cudaGetLastError() != cudaSuccess) {
       msg = "CUDA error while creating the plan";
       rc = BFGT_ERR_CUDA;
@@ -545,7 +601,7 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
 void device_plan_destroy(DevicePlan &dp) {
   if (dp.graph_exec) cudaGraphExecDestroy(dp.graph_exec);
   if (dp.graph) cudaGraphDestroy(dp.graph);
-  void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.cut_chunk_begin, dp.cut_pw_begin,
+  void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.columns, dp.cut_chunk_begin, dp.cut_pw_begin,
                   dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.Mpart, dp.M, dp.L, dp.Tsplit, dp.Esplit,
                   dp.Tscale, dp.Escale, dp.nf_target, dp.nf_level, dp.nf_begin, dp.nf_src, dp.nf_ixy,
                   dp.tab_loc, dp.ind_loc, dp.d_stage_f, dp.d_stage_p};
@@ -553,44 +609,77 @@ void device_plan_destroy(DevicePlan &dp) {
     if (p) cudaFree(p);
   if (dp.h_stage_f) cudaFreeHost(dp.h_stage_f);
   if (dp.h_stage_p) cudaFreeHost(dp.h_stage_p);
-  if (dp.events)
-    for (int i = 0; i < 8; i++) cudaEventDestroy(dp.ev[i]);
+  for (auto &es : dp.evsets)
+    for (cudaEvent_t e : es) cudaEventDestroy(e);
   dp = DevicePlan();
+}
+
+int device_plan_reserve_events(DevicePlan &dp, int n) {
+  while ((int)dp.evsets.size() < n) {
+    std::array<cudaEvent_t, 6> es;
+    for (auto &e : es)
+      if (cudaEventCreate(&e) != cudaSuccess) return BFGT_ERR_CUDA;
+    dp.evsets.push_back(es);
+  }
+  return BFGT_OK;
+}
+
+int device_plan_stage_ms(DevicePlan &dp, double *out) {
+  for (int i = 0; i < 8; i++) out[i] = 0;
+  if (dp.nrec == 0) return BFGT_OK;
+  const int nr = std::min<int>(dp.nrec, (int)dp.evsets.size());
+  if (cudaEventSynchronize(dp.evsets[nr - 1][5]) != cudaSuccess) return BFGT_ERR_CUDA;
+  for (int r = 0; r < nr; r++) {
+    float ms;
+    for (int i = 0; i < 5; i++)
+      if (cudaEventElapsedTime(&ms, dp.evsets[r][i], dp.evsets[r][i + 1]) == cudaSuccess) out[i] += ms;
+    if (cudaEventElapsedTime(&ms, dp.evsets[r][0], dp.evsets[r][5]) == cudaSuccess) out[5] += ms;
+  }
+  out[6] = nr;
+  dp.nrec = 0;
+  cudaGetLastError();
+  return BFGT_OK;
 }
 
 int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cudaStream_t s, std::string &msg) {
   const int nthreads = kWarps * 32;
-  if (dp.events) cudaEventRecord(dp.ev[0], s);
+  cudaEvent_t *ev = nullptr;
+  if (dp.events) {
+    if (dp.nrec >= (int)dp.evsets.size() && dp.evsets.size() < 65536) device_plan_reserve_events(dp, dp.nrec + 1);
+    ev = dp.evsets[dp.nrec % dp.evsets.size()].data();
+    dp.nrec++;
+  }
+  if (ev) cudaEventRecord(ev[0], s);
   if (!dp.direct_only && dp.nchunks > 0) {
     if (dp.precision == BFGT_PREC_SPLIT) {
       split_form(dp, d_fvals, s);
     } else {
-      FormArgs fa{d_fvals, dp.leaves, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
-      launch_form_fp64(best_tile(dp.npw, dp.hh, kFormTiles, 6), dp.nchunks, dp.smem_form, s, fa);
+      FormArgs fa{d_fvals, dp.leaves, dp.columns, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
+      launch_form_fp64(TileChoice{dp.form_tile[0], dp.form_tile[1], dp.form_tile[2]}, dp.nchunks, dp.smem_form, s, fa);
     }
-    if (dp.events) cudaEventRecord(dp.ev[1], s);
+    if (ev) cudaEventRecord(ev[1], s);
     const int zb = (dp.nexp + 255) / 256;
     k_reduce<<<dim3(dp.ncut, dp.nd, zb), 256, 0, s>>>(dp.Mpart, dp.cut_chunk_begin, dp.M, dp.nd, dp.nexp);
-    if (dp.events) cudaEventRecord(dp.ev[2], s);
+    if (ev) cudaEventRecord(ev[2], s);
     k_translate<<<dim3(dp.ncut, dp.nd, zb), 256, 0, s>>>(dp.M, dp.cut_pw_begin, dp.cut_pw_src, dp.cut_pw_ind,
                                                          dp.W, dp.L, dp.nd, dp.nexp);
-    if (dp.events) cudaEventRecord(dp.ev[3], s);
+    if (ev) cudaEventRecord(ev[3], s);
     if (dp.precision == BFGT_PREC_SPLIT) {
       split_eval(dp, d_pot, s);
     } else {
-      EvalArgs ea{d_pot, dp.leaves, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
-      launch_eval_fp64(best_tile(dp.n, dp.hh, kEvalTiles, 6), dp.nchunks, dp.smem_eval, s, ea);
+      EvalArgs ea{d_pot, dp.leaves, dp.columns, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
+      launch_eval_fp64(TileChoice{dp.eval_tile[0], dp.eval_tile[1], dp.eval_tile[2]}, dp.nchunks, dp.smem_eval, s, ea);
     }
-    if (dp.events) cudaEventRecord(dp.ev[4], s);
-  } else if (dp.events) {
-    for (int i = 1; i <= 4; i++) cudaEventRecord(dp.ev[i], s);
+    if (ev) cudaEventRecord(ev[4], s);
+  } else if (ev) {
+    for (int i = 1; i <= 4; i++) cudaEventRecord(ev[i], s);
   }
   if (dp.nnf > 0) {
     NearArgs na{d_fvals, d_pot, dp.nf_target, dp.nf_level, dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc,
                 dp.ind_loc, dp.nnf, dp.nd, dp.n};
     k_near_fp64<<<(dp.nnf + kWarps - 1) / kWarps, nthreads, dp.smem_near, s>>>(na);
   }
-  if (dp.events) cudaEventRecord(dp.ev[5], s);
+  if (ev) cudaEventRecord(ev[5], s);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     msg = std::string("kernel launch failed: ") + cudaGetErrorString(e);

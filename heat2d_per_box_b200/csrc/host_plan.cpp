@@ -1041,17 +1041,38 @@ void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, doub
       int ax = anc[x.box], ay = anc[y.box];
       if (ax != ay) return ax < ay;
       if (x.level != y.level) return x.level < y.level;
-      return x.box < y.box;
+      if (x.ox != y.ox) return x.ox < y.ox;
+      return x.oy < y.oy;
     });
-    const int CH = 32;
+    // columns (same ancestor, level, ox) and chunks of columns (same ancestor
+    // and level; at most kChunkCols columns and about kChunkLeaves leaves)
+    const int kChunkCols = 8, kChunkLeaves = 64;
+    hp.columns.clear();
+    for (size_t i = 0; i < hp.leaves.size();) {
+      size_t j = i;
+      while (j < hp.leaves.size() && anc[hp.leaves[j].box] == anc[hp.leaves[i].box] &&
+             hp.leaves[j].level == hp.leaves[i].level && hp.leaves[j].ox == hp.leaves[i].ox)
+        j++;
+      hp.columns.push_back(Column{(int)i, (int)j, hp.leaves[i].ox});
+      i = j;
+    }
     hp.chunks.clear();
     hp.cut_chunk_begin.assign(ncut + 1, 0);
-    for (size_t i = 0; i < hp.leaves.size();) {
-      int ic = anc[hp.leaves[i].box], lv = hp.leaves[i].level;
-      size_t j = i;
-      while (j < hp.leaves.size() && anc[hp.leaves[j].box] == ic && hp.leaves[j].level == lv && (int)(j - i) < CH) j++;
-      hp.chunks.push_back(Chunk{(int)i, (int)j, ic, lv});
-      i = j;
+    for (size_t c = 0; c < hp.columns.size();) {
+      const PwLeaf &l0 = hp.leaves[hp.columns[c].begin];
+      const int ic = anc[l0.box], lv = l0.level;
+      size_t e = c;
+      int nleaf = 0;
+      while (e < hp.columns.size()) {
+        const PwLeaf &le = hp.leaves[hp.columns[e].begin];
+        if (anc[le.box] != ic || le.level != lv || (int)(e - c) >= kChunkCols) break;
+        const int nl = hp.columns[e].end - hp.columns[e].begin;
+        if (e > c && nleaf + nl > kChunkLeaves) break;
+        nleaf += nl;
+        e++;
+      }
+      hp.chunks.push_back(Chunk{(int)c, (int)e, ic, lv});
+      c = e;
     }
     {
       size_t c = 0;
@@ -1162,10 +1183,16 @@ void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, doub
     const double nn = n;
     double fl = 0;
     const double npwd = hp.npw, hd = hp.hh;
-    fl += (double)hp.leaves.size() * nd * (4 * nn * nn * hd + 8 * nn * hd * npwd);  // leaf -> PW
-    fl += (double)hp.leaves.size() * nd * (8 * nn * hd * npwd + 4 * nn * nn * hd);  // PW -> leaf
-    fl += (double)hp.leaves.size() * nd * 2 * 8 * hp.nexp;                          // folded shifts
-    fl += (double)hp.cut_pw_src.size() * nd * 8 * hp.nexp;                          // cutoff translations
+    const double nl = (double)hp.leaves.size() * nd;
+    const double ncl = (double)hp.columns.size() * nd;
+    // leaf values -> y contraction per leaf, x contraction once per column
+    hp.flops_form = nl * (4 * nn * nn * hd + 6 * nn * hd) + ncl * (8 * nn * hd * npwd + 6 * nn * npwd);
+    // x contraction once per column, y contraction (real part) per leaf
+    hp.flops_eval = ncl * (8 * nn * hd * npwd + 6 * nn * npwd) + nl * (4 * nn * nn * hd + 6 * nn * hd);
+    hp.flops_translate = (double)hp.cut_pw_src.size() * nd * 8 * hp.nexp;
+    hp.bytes_form = nl * nn * nn * 8;    // leaf values read
+    hp.bytes_eval = nl * nn * nn * 16;   // pot read + write
+    fl += hp.flops_form + hp.flops_eval + hp.flops_translate;
     for (size_t tg = 0; tg < hp.nf_target.size(); tg++) {
       const int *il = &hp.ind_loc[(size_t)2 * (n + 1) * 13 * hp.nf_level[tg]];
       auto band = [&](int k) {
@@ -1177,9 +1204,11 @@ void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, doub
         // banded x then y contraction of one near-field pair
         double nx = band(hp.nf_ix[e]), ny = band(hp.nf_iy[e]);
         if (nx == 0 || ny == 0) continue;
-        fl += nd * 2.0 * (nx * nn * nn + nx * ny * nn);
+        hp.flops_near += nd * 2.0 * (nx * nn * nn + nx * ny * nn);
       }
     }
+    fl += hp.flops_near;
+    hp.bytes_near = (double)hp.nf_target.size() * nd * nn * nn * 16 + (double)hp.nf_src.size() * nd * nn * nn * 8;
     hp.flops = fl;
     double leafpts = 0;
     for (int l = 0; l <= nlevels; l++)

@@ -40,9 +40,18 @@ struct PwLeaf {
   int level;
 };
 
-// A run of PW leaves with the same cutoff ancestor and level.
-struct Chunk {
+// A column: the PW leaves of one cutoff ancestor and level that share the
+// x-offset ox (so they differ only in oy), stored contiguously in the sorted
+// PwLeaf array.
+struct Column {
   int begin, end;  // into the sorted PwLeaf array
+  int ox;
+};
+
+// A unit of work for one CTA: consecutive columns of one cutoff ancestor and
+// level.
+struct Chunk {
+  int begin, end;  // into the column array
   int icut;        // cutoff box index
   int level;
 };
@@ -76,8 +85,9 @@ struct HostPlan {
   std::vector<int> cut_chunk_begin;          // ncut+1 offsets into chunks
   std::vector<int> cut_pw_begin;             // ncut+1 offsets into cut_pw_src/ind
   std::vector<int> cut_pw_src, cut_pw_ind;   // source cutoff index, shift index 0..8
-  std::vector<PwLeaf> leaves;                // sorted by (icut, level, box)
-  std::vector<Chunk> chunks;
+  std::vector<PwLeaf> leaves;                // sorted by (icut, level, ox, oy)
+  std::vector<Column> columns;               // sorted by (icut, level, ox)
+  std::vector<Chunk> chunks;                 // groups of columns (one CTA each)
   std::vector<cplx> phase;                   // per level: (2^d offsets, npw)
   std::vector<int64_t> phase_off;            // per level offset into phase
   std::vector<double> pw_weight;             // (hh): 1, or 1/2 on the zero frequency of odd npw
@@ -86,6 +96,9 @@ struct HostPlan {
   std::vector<int> nf_src, nf_ix, nf_iy;
   // work accounting
   double flops = 0, bytes = 0, tc_flops = 0, points = 0;
+  double flops_form = 0, flops_eval = 0, flops_near = 0, flops_translate = 0;
+  double bytes_form = 0, bytes_eval = 0, bytes_near = 0;  // compulsory HBM bytes per stage
+  double tc_flops_form = 0, tc_flops_eval = 0;           // tensor-core FLOP issued (split mode)
 };
 
 // Builds the host plan; itree's colleague arrays are recomputed in place.

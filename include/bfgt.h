@@ -94,9 +94,16 @@ int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, voi
 int bfgt_plan_graph_capture(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream);
 int bfgt_plan_graph_launch(bfgt_plan plan, void *stream);
 
-/* Per-stage device milliseconds of the last bfgt_plan_execute on this plan
-   (CUDA events; the stage order matches timeinfo(2:7)). out must hold 8. */
+/* Device milliseconds per stage, summed over every bfgt_plan_execute on this
+   plan since the previous call (CUDA events recorded on the execute stream):
+   out[0] leaf values -> cutoff expansions (steps 1+2), out[1] fixed-order
+   reduction, out[2] cutoff translation (step 3), out[3] cutoff expansions ->
+   leaf values (steps 4+5), out[4] near field (step 6), out[5] total, out[6]
+   number of executes summed.  Waits for the last of them.  out must hold 8. */
 int bfgt_plan_stage_ms(bfgt_plan plan, double *out);
+
+/* Creates n sets of stage events ahead of a timed loop (one set per execute). */
+int bfgt_plan_reserve_events(bfgt_plan plan, int n);
 
 /* Plan scalars: out[0]=npwlevel (boxfgt.f:137-150), out[1]=npw, out[2]=nlevstart,
    out[3]=nlevend, out[4]=regime (0 periodic Fourier, 1 PW + near field,
@@ -106,9 +113,13 @@ int bfgt_plan_stage_ms(bfgt_plan plan, double *out);
    out must hold 16 ints. */
 int bfgt_plan_info(bfgt_plan plan, int *out);
 
-/* Algorithmic FP64 work of one execute: out[0]=FLOP, out[1]=compulsory HBM
-   bytes (leaf fvals read + pot read/write), out[2]=tensor-core FLOP issued
-   (split mode; counts every slice product), out[3]=leaf points x nd. */
+/* Algorithmic work of one execute (every real operation counted once, split
+   slices not multiplied): out[0]=FLOP, out[1]=compulsory HBM bytes (leaf fvals
+   read + pot read/write), out[2]=tensor-core FLOP issued (split mode; every
+   slice product counted), out[3]=leaf points x nd, out[4..7]=FLOP of the form,
+   eval, near-field and translation stages, out[8..10]=compulsory bytes of the
+   form, eval and near-field stages, out[11..12]=tensor-core FLOP issued by the
+   form and eval stages.  out must hold 16. */
 int bfgt_plan_work(bfgt_plan plan, double *out);
 
 int bfgt_plan_destroy(bfgt_plan plan);

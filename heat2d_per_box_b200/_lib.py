@@ -76,6 +76,8 @@ def lib():
     L.bfgt_plan_info.argtypes = [C.c_void_p, _i32p]
     L.bfgt_plan_work.restype = C.c_int
     L.bfgt_plan_work.argtypes = [C.c_void_p, _f64p]
+    L.bfgt_plan_check.restype = C.c_int
+    L.bfgt_plan_check.argtypes = [C.c_void_p]
     L.bfgt_plan_destroy.restype = C.c_int
     L.bfgt_plan_destroy.argtypes = [C.c_void_p]
     L.bfgt_host_plan_dump.restype = C.c_int

@@ -97,6 +97,10 @@ class Plan:
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         _lib.check(self._L.bfgt_plan_graph_launch(self._h, s))
 
+    def check(self):
+        """Waits for the device; raises BfgtError if a bounded device wait timed out."""
+        _lib.check(self._L.bfgt_plan_check(self._h))
+
     def stage_ms(self):
         """Per-stage device ms summed over the executes since the last call (see bfgt_plan_stage_ms)."""
         out = np.zeros(8)

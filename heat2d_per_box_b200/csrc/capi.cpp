@@ -12,6 +12,7 @@
 #include "../../include/bfgt.h"
 #include "device_plan.hpp"
 #include "host_plan.hpp"
+#include "split_kernels.cuh"
 
 struct bfgt_plan_s {
   bfgt::HostPlan hp;
@@ -219,8 +220,19 @@ int bfgt_plan_work(bfgt_plan plan, double *out) {
   out[8] = plan->hp.bytes_form;
   out[9] = plan->hp.bytes_eval;
   out[10] = plan->hp.bytes_near;
-  out[11] = plan->hp.tc_flops_form;
-  out[12] = plan->hp.tc_flops_eval;
+  out[11] = plan->dp.split.tc_flops_form;
+  out[12] = plan->dp.split.tc_flops_eval;
+  out[2] = out[11] + out[12];
+  return BFGT_OK;
+}
+
+int bfgt_plan_check(bfgt_plan plan) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(BFGT_ERR_CUDA, std::string("device error: ") + cudaGetErrorString(cudaGetLastError()));
+  int rc = bfgt::split_check(plan->dp);
+  if (rc == BFGT_ERR_TIMEOUT) return fail(rc, "a bounded device-side wait gave up (tensor-core pipeline)");
+  if (rc != BFGT_OK) return fail(rc, "error flag read-out failed");
   return BFGT_OK;
 }
 
@@ -242,6 +254,7 @@ int bfgt_boxfgt(int nd, double delta, double eps, int ipoly, int iperiod, int no
   if (rc != BFGT_OK) return rc;
   double t1 = now_s();
   rc = bfgt_plan_execute_host(plan, fvals, pot, nullptr);
+  if (rc == BFGT_OK) rc = bfgt_plan_check(plan);
   if (rc == BFGT_OK && timeinfo) {
     double st[8];
     bfgt::device_plan_stage_ms(plan->dp, st);

@@ -11,6 +11,21 @@
 
 namespace bfgt {
 
+// Tensor-core (split precision) part of a plan.
+struct SplitPlan {
+  int cpc = 0, KA = 0, NP = 0, KH = 0, KE = 0, NB = 0, nt = 0, nchunks = 0;
+  int4 *chunks = nullptr;
+  int *step_begin = nullptr, *steps = nullptr;
+  uint16_t *TyB = nullptr, *EyB = nullptr;
+  double2 *Ex = nullptr;
+  long long *tyb_off = nullptr, *eyb_off = nullptr, *ex_off = nullptr;
+  long long tyb_tile = 0, eyb_tile = 0;
+  int *err = nullptr;
+  uint32_t wait_iters = 0;
+  size_t smem_form = 0, smem_eval = 0;
+  double tc_flops_form = 0, tc_flops_eval = 0;
+};
+
 struct DevicePlan {
   int device = 0;
   int nd = 1, n = 0, npw = 0, hh = 0, nexp = 0, nlevels = 0, nboxes = 0, precision = 0;
@@ -32,9 +47,7 @@ struct DevicePlan {
   double2 *Mpart = nullptr;     // (nchunks, nd, nexp)
   double2 *M = nullptr;         // (ncut, nd, nexp)
   double2 *L = nullptr;         // (ncut, nd, nexp)
-  // split-precision scratch (FP16 operand slices of the level tables)
-  void *Tsplit = nullptr, *Esplit = nullptr;
-  double *Tscale = nullptr, *Escale = nullptr;
+  SplitPlan split;
   // near field
   int *nf_target = nullptr, *nf_level = nullptr, *nf_begin = nullptr, *nf_src = nullptr;
   int2 *nf_ixy = nullptr;

@@ -601,10 +601,10 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
 void device_plan_destroy(DevicePlan &dp) {
   if (dp.graph_exec) cudaGraphExecDestroy(dp.graph_exec);
   if (dp.graph) cudaGraphDestroy(dp.graph);
+  split_plan_destroy(dp);
   void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.columns, dp.cut_chunk_begin, dp.cut_pw_begin,
-                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.Mpart, dp.M, dp.L, dp.Tsplit, dp.Esplit,
-                  dp.Tscale, dp.Escale, dp.nf_target, dp.nf_level, dp.nf_begin, dp.nf_src, dp.nf_ixy,
-                  dp.tab_loc, dp.ind_loc, dp.d_stage_f, dp.d_stage_p};
+                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.Mpart, dp.M, dp.L, dp.nf_target, dp.nf_level,
+                  dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.d_stage_f, dp.d_stage_p};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (dp.h_stage_f) cudaFreeHost(dp.h_stage_f);

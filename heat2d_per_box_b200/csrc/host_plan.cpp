@@ -1053,7 +1053,7 @@ void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, doub
       while (j < hp.leaves.size() && anc[hp.leaves[j].box] == anc[hp.leaves[i].box] &&
              hp.leaves[j].level == hp.leaves[i].level && hp.leaves[j].ox == hp.leaves[i].ox)
         j++;
-      hp.columns.push_back(Column{(int)i, (int)j, hp.leaves[i].ox});
+      hp.columns.push_back(Column{(int)i, (int)j, hp.leaves[i].ox, anc[hp.leaves[i].box], hp.leaves[i].level});
       i = j;
     }
     hp.chunks.clear();

@@ -46,6 +46,7 @@ struct PwLeaf {
 struct Column {
   int begin, end;  // into the sorted PwLeaf array
   int ox;
+  int icut, level;
 };
 
 // A unit of work for one CTA: consecutive columns of one cutoff ancestor and

@@ -1,14 +1,659 @@
-// Split-precision (tensor-core) plane-wave kernels.
+// Split-precision plane-wave kernels on the sm_100a tensor cores (tcgen05).
+//
+// Same sum-factorised scheme as the FP64 kernels (fgt_device.cu): a CTA takes
+// up to 128/n columns of one cutoff ancestor and level and walks the
+// y-offsets oy present in them.  The per-leaf contractions are tensor-core
+// GEMMs with M = 128 rows = (column slot, leaf grid index):
+//   form:  D[(slot,m1), (re/im,k2)] += F_{slot,oy}(m1,m2) * Ty_oy(m2,(re/im,k2))
+//   eval:  D[(slot,k1), k2] = [Hr|Hi](k1,(re/im,m2)) * [Eyr;-Eyi]((re/im,m2),k2)
+// where Ty_oy = T conj(phase_oy) and Ey_oy = w E phase_oy are per-offset tables
+// precomputed in FP64 on the host.  Every operand is split into three BF16
+// slices (x = s0 + s1 + s2, ~2^-24 relative); the six slice products with
+// i+j <= 2 are accumulated in FP32 in tensor memory, the leading product s0*s0
+// in its own accumulator and the five correction products in a second one,
+// and the two are summed in FP64.  The once-per-column contractions (x
+// direction) and all cross-leaf sums run in FP64 on the CUDA cores; the
+// plane-wave phases stay FP64 throughout.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "../../include/bfgt.h"
 #include "split_kernels.cuh"
+#include "tc_sm100.cuh"
 
 namespace bfgt {
 
-int split_plan_create(DevicePlan &, const HostPlan &, std::string &msg) {
-  msg = "split precision is not built in this library";
-  return BFGT_ERR_ARG;
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kRows = 128;                // MMA M
+constexpr uint32_t kWaitIters = 1u << 26;  // bounded spin on an mbarrier
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-void split_form(DevicePlan &, const double *, cudaStream_t) {}
-void split_eval(DevicePlan &, double *, cudaStream_t) {}
+
+struct FormTcArgs {
+  const double *fvals;
+  const int4 *chunks;      // {column begin, column end, icut, level}
+  const int *step_begin;   // nchunks + 1
+  const int *steps;        // stride 1 + cpc: oy, then box per slot (-1: no leaf)
+  const int4 *columns;     // {leaf begin, leaf end, ox, -}
+  const uint16_t *TyB;     // per (level, oy): 3 slices x NP rows x KA, K-major core layout
+  const long long *tyb_off;
+  long long tyb_tile;      // uint16 elements per (level, oy) tile
+  const double2 *T;        // tab_poly2pw, per level (n, npw)
+  const double2 *PH;
+  const long long *ph_off;
+  double2 *Mpart;
+  int *err;
+  int nd, n, npw, hh, nexp, cpc, NP, KA;
+  uint32_t wait_iters;
+};
+
+// 16-byte copy of a global tile into shared memory
+__device__ __forceinline__ void copy_tile(unsigned char *dst, const uint16_t *src, int bytes) {
+  const uint4 *s = reinterpret_cast<const uint4 *>(src);
+  uint4 *d = reinterpret_cast<uint4 *>(dst);
+  for (int i = threadIdx.x; i < bytes / 16; i += blockDim.x) d[i] = s[i];
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);  // [0],[1] operand buffers, [2] drain
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 64);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int4 ch = a.chunks[blockIdx.x];
+  const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, NP = a.NP, KA = a.KA;
+  const int ncol = ch.y - ch.x;
+  const int abytes = 3 * kRows * KA * 2, bbytes = 3 * NP * KA * 2, bufbytes = abytes + bbytes;
+  const int ybytes = kRows * hh * 16;
+  const int ubytes = ((std::max(2 * bufbytes, ybytes) + 1023) / 1024) * 1024;
+  unsigned char *U = smem + 1024;
+  double2 *sY = reinterpret_cast<double2 *>(U);  // after the tensor-core loop: [row][k2]
+  double2 *sT = reinterpret_cast<double2 *>(U + ubytes);  // [m][k] n x npw
+  double2 *sphx = sT + (size_t)n * npw;                    // [slot][k] conj(phase_ox)
+
+  if (warp == 0) tc::tmem_alloc(tmem_slot, 128);
+  if (tid == 0) {
+    tc::mbar_init(&mbar[0], 1);
+    tc::mbar_init(&mbar[1], 1);
+    tc::mbar_init(&mbar[2], 1);
+    tc::fence_mbar_init();
+  }
+  const double2 *Tg = a.T + (size_t)n * npw * ch.w;
+  for (int i = tid; i < n * npw; i += kThreads) {
+    const int m = i % n, k = i / n;
+    sT[m * npw + k] = Tg[i];
+  }
+  const long long phoff = a.ph_off[ch.w];
+  for (int i = tid; i < ncol * npw; i += kThreads) {
+    const int slot = i / npw, k = i - slot * npw;
+    const double2 p = a.PH[phoff + (size_t)a.columns[ch.x + slot].z * npw + k];
+    sphx[i] = make_double2(p.x, -p.y);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t tD0 = tmem, tD1 = tmem + (uint32_t)NP;
+  const uint32_t idesc = tc::idesc_bf16_f32(kRows, NP);
+  const int sb = a.step_begin[blockIdx.x], se = a.step_begin[blockIdx.x + 1], nsteps = se - sb;
+  const int stride = 1 + cpc;
+  const uint16_t *tyb = a.TyB + a.tyb_off[ch.w];
+  bool ok = true;
+  const int r = tid, rslot = r / n, rm1 = r - rslot * n;
+
+  for (int ind = 0; ind < nd; ind++) {
+    for (int s = 0; s < nsteps; s++) {
+      const int g = ind * nsteps + s, b = g & 1;
+      if (g >= 2 && ok && !tc::mbar_wait(&mbar[b], ((g >> 1) - 1) & 1, a.wait_iters)) {
+        ok = false;
+        atomicExch(a.err, 1);
+      }
+      const int *st = a.steps + (size_t)(sb + s) * stride;
+      unsigned char *Ab = U + b * bufbytes, *Bb = Ab + abytes;
+      {
+        // A row r = (slot, m1): F(m1, m2) for m2 = 0..n-1, zero-padded to KA
+        const int box = (rslot < cpc) ? st[1 + rslot] : -1;
+        const double *fv = a.fvals + (size_t)(box < 0 ? 0 : box) * nd * npb + ind + (size_t)nd * rm1;
+        for (int h = 0; h < KA / 8; h++) {
+          uint16_t s0[8], s1[8], s2[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const int k = 8 * h + q;
+            const double v = (box >= 0 && k < n) ? fv[(size_t)nd * n * k] : 0.0;
+            tc::split3_bf16(v, s0[q], s1[q], s2[q]);
+          }
+          const uint32_t off = tc::kmajor_off(r, 8 * h, kRows);
+          *reinterpret_cast<uint4 *>(Ab + off) = *reinterpret_cast<uint4 *>(s0);
+          *reinterpret_cast<uint4 *>(Ab + kRows * KA * 2 + off) = *reinterpret_cast<uint4 *>(s1);
+          *reinterpret_cast<uint4 *>(Ab + 2 * kRows * KA * 2 + off) = *reinterpret_cast<uint4 *>(s2);
+        }
+      }
+      copy_tile(Bb, tyb + (size_t)st[0] * a.tyb_tile, bbytes);
+      tc::fence_async_smem();
+      tc::fence_before_sync();
+      __syncthreads();
+      if (tid == 0 && ok) {
+        tc::fence_after_sync();
+        const uint32_t aA = tc::smem_u32(Ab), aB = tc::smem_u32(Bb);
+        const uint32_t lboA = (kRows / 8) * 128, lboB = (NP / 8) * 128;
+        for (int kk = 0; kk < KA / 16; kk++) {
+          uint64_t ad[3], bd[3];
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            ad[c] = tc::smem_desc(aA + c * kRows * KA * 2 + kk * 2 * lboA, lboA, 128);
+            bd[c] = tc::smem_desc(aB + c * NP * KA * 2 + kk * 2 * lboB, lboB, 128);
+          }
+          const uint32_t acc = (s > 0 || kk > 0) ? 1u : 0u;
+          tc::mma_bf16(tD0, ad[0], bd[0], idesc, acc);
+          tc::mma_bf16(tD1, ad[0], bd[1], idesc, acc);
+          tc::mma_bf16(tD1, ad[1], bd[0], idesc, 1u);
+          tc::mma_bf16(tD1, ad[0], bd[2], idesc, 1u);
+          tc::mma_bf16(tD1, ad[1], bd[1], idesc, 1u);
+          tc::mma_bf16(tD1, ad[2], bd[0], idesc, 1u);
+        }
+        tc::commit(&mbar[b]);
+      }
+    }
+    if (nsteps > 0) {
+      const int gl = ind * nsteps + nsteps - 1;
+      if (ok && !tc::mbar_wait(&mbar[gl & 1], (gl >> 1) & 1, a.wait_iters)) {
+        ok = false;
+        atomicExch(a.err, 1);
+      }
+    }
+    tc::fence_after_sync();
+    // read the two accumulators of this thread's row and sum them in FP64
+    {
+      const uint32_t lanebase = (uint32_t)(32 * warp) << 16;
+      for (int j0 = 0; j0 < NP; j0 += 16) {
+        float v0[16], v1[16];
+        tc::tmem_ld16(tD0 + lanebase + j0, v0);
+        tc::tmem_ld16(tD1 + lanebase + j0, v1);
+        tc::tmem_ld_wait();
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          const int j = j0 + i;
+          const double y = ok ? (double)v0[i] + (double)v1[i] : 0.0;
+          if (j < hh) sY[r * hh + j].x = y;
+          else if (j < 2 * hh) sY[r * hh + (j - hh)].y = y;
+        }
+      }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    // x contraction (FP64): M(k1,k2) = sum_{slot,m1} T(m1,k1) conj(ph_ox(k1)) Y(slot,m1,k2)
+    {
+      const int ntm = (npw + 1) / 2, ntn = (hh + 3) / 4, ntiles = ntm * ntn;
+      double2 *out = a.Mpart + ((size_t)blockIdx.x * nd + ind) * a.nexp;
+#pragma unroll
+      for (int t = 0; t < NT; t++) {
+        const int tile = tid + kThreads * t;
+        if (tile >= ntiles) continue;
+        const int k1b = (tile % ntm) * 2, k2b = (tile / ntm) * 4;
+        double2 acc[2][4];
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++) acc[i][j] = make_double2(0, 0);
+        for (int slot = 0; slot < ncol; slot++) {
+          double2 ph[2];
+#pragma unroll
+          for (int i = 0; i < 2; i++) ph[i] = (k1b + i < npw) ? sphx[slot * npw + k1b + i] : make_double2(0, 0);
+          for (int m1 = 0; m1 < n; m1++) {
+            double2 av[2], bv[4];
+#pragma unroll
+            for (int i = 0; i < 2; i++) av[i] = zmul((k1b + i < npw) ? sT[m1 * npw + k1b + i] : make_double2(0, 0), ph[i]);
+#pragma unroll
+            for (int j = 0; j < 4; j++) bv[j] = (k2b + j < hh) ? sY[(slot * n + m1) * hh + k2b + j] : make_double2(0, 0);
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+              for (int j = 0; j < 4; j++) {
+                acc[i][j].x = fma(av[i].x, bv[j].x, acc[i][j].x);
+                acc[i][j].x = fma(-av[i].y, bv[j].y, acc[i][j].x);
+                acc[i][j].y = fma(av[i].x, bv[j].y, acc[i][j].y);
+                acc[i][j].y = fma(av[i].y, bv[j].x, acc[i][j].y);
+              }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (k1b + i < npw && k2b + j < hh) out[(size_t)(k2b + j) * npw + k1b + i] = acc[i][j];
+      }
+    }
+    __syncthreads();
+  }
+  // drain: no tensor-core operation of this CTA may be in flight when TMEM is freed
+  if (tid == 0) tc::commit(&mbar[2]);
+  if (!tc::mbar_wait(&mbar[2], 0, kWaitIters)) atomicExch(a.err, 2);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 128);
+}
+
+struct EvalTcArgs {
+  double *pot;
+  const int4 *chunks;
+  const int *step_begin;
+  const int *steps;
+  const int4 *columns;
+  const uint16_t *EyB;     // per (level, oy): 3 slices x NB rows x KE, K-major core layout
+  const long long *eyb_off;
+  long long eyb_tile;
+  const double2 *Ex;       // per (level, ox): E(m1,k1) phase_ox(m1), [m1][k1]
+  const long long *ex_off;
+  const double2 *L;
+  int *err;
+  int nd, n, npw, hh, nexp, cpc, NB, KE, KH;
+  uint32_t wait_iters;
+};
+
+__global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 64);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int4 ch = a.chunks[blockIdx.x];
+  const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, NB = a.NB, KE = a.KE, KH = a.KH;
+  const int ncol = ch.y - ch.x;
+  const int abytes = 3 * kRows * KE * 2, bbytes = 3 * NB * KE * 2;
+  unsigned char *sA = smem + 1024;
+  unsigned char *sB = sA + ((abytes + 1023) / 1024) * 1024;  // two buffers
+  double2 *sL = reinterpret_cast<double2 *>(sB + ((2 * bbytes + 1023) / 1024) * 1024);  // [m1][m2]
+  (void)lane;
+
+  if (warp == 0) tc::tmem_alloc(tmem_slot, 64);
+  if (tid == 0) {
+    tc::mbar_init(&mbar[0], 1);
+    tc::mbar_init(&mbar[1], 1);
+    tc::mbar_init(&mbar[2], 1);
+    tc::fence_mbar_init();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = tc::idesc_bf16_f32(kRows, NB);
+  const int sb = a.step_begin[blockIdx.x], se = a.step_begin[blockIdx.x + 1], nsteps = se - sb;
+  const int stride = 1 + cpc;
+  const uint16_t *eyb = a.EyB + a.eyb_off[ch.w];
+  const double2 *exl = a.Ex + a.ex_off[ch.w];
+  bool ok = true;
+  const int r = tid, rslot = r / n, rk1 = r - rslot * n;
+  const uint32_t lanebase = (uint32_t)(32 * warp) << 16;
+
+  // wait for the MMAs of global step g (density ind, step s), add 2 Re(...) into pot
+  auto readout = [&](int ind, int s, int g) {
+    const int b = g & 1;
+    if (ok && !tc::mbar_wait(&mbar[b], (g >> 1) & 1, a.wait_iters)) {
+      ok = false;
+      atomicExch(a.err, 1);
+    }
+    tc::fence_after_sync();
+    float v0[16], v1[16];
+    tc::tmem_ld16(tmem + lanebase + (uint32_t)(b * 2 * NB), v0);
+    tc::tmem_ld16(tmem + lanebase + (uint32_t)(b * 2 * NB + NB), v1);
+    tc::tmem_ld_wait();
+    const int *st = a.steps + (size_t)(sb + s) * stride;
+    const int box = st[1 + rslot];
+    if (ok && box >= 0) {
+      double *pb = a.pot + (size_t)box * nd * npb + ind;
+      for (int k2 = 0; k2 < n; k2++) pb[(size_t)nd * (rk1 + n * k2)] += 2.0 * ((double)v0[k2] + (double)v1[k2]);
+    }
+    tc::fence_before_sync();
+  };
+
+  for (int ind = 0; ind < nd; ind++) {
+    const double2 *Lg = a.L + ((size_t)ch.z * nd + ind) * a.nexp;
+    for (int e = tid; e < a.nexp; e += kThreads) {
+      const int m2 = e / npw, m1 = e - m2 * npw;
+      sL[m1 * hh + m2] = Lg[e];
+    }
+    __syncthreads();
+    // H(k1,m2) = sum_m1 Ex_ox(m1,k1) L(m1,m2) for row r = (slot, k1), sliced into the A operand
+    {
+      const bool live = rslot < ncol;
+      const double2 *ex = live ? exl + (size_t)a.columns[ch.x + rslot].z * npw * n : exl;
+      for (int mb = 0; mb < KH; mb += 8) {
+        double2 acc[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[j] = make_double2(0, 0);
+        if (live) {
+          for (int m1 = 0; m1 < npw; m1++) {
+            const double2 e = ex[(size_t)m1 * n + rk1];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              const double2 l = (mb + j < hh) ? sL[m1 * hh + mb + j] : make_double2(0, 0);
+              acc[j].x = fma(e.x, l.x, acc[j].x);
+              acc[j].x = fma(-e.y, l.y, acc[j].x);
+              acc[j].y = fma(e.x, l.y, acc[j].y);
+              acc[j].y = fma(e.y, l.x, acc[j].y);
+            }
+          }
+        }
+        uint16_t re0[8], re1[8], re2[8], im0[8], im1[8], im2[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          tc::split3_bf16((mb + j < hh) ? acc[j].x : 0.0, re0[j], re1[j], re2[j]);
+          tc::split3_bf16((mb + j < hh) ? acc[j].y : 0.0, im0[j], im1[j], im2[j]);
+        }
+        const uint32_t ore = tc::kmajor_off(r, mb, kRows), oim = tc::kmajor_off(r, KH + mb, kRows);
+        *reinterpret_cast<uint4 *>(sA + ore) = *reinterpret_cast<uint4 *>(re0);
+        *reinterpret_cast<uint4 *>(sA + kRows * KE * 2 + ore) = *reinterpret_cast<uint4 *>(re1);
+        *reinterpret_cast<uint4 *>(sA + 2 * kRows * KE * 2 + ore) = *reinterpret_cast<uint4 *>(re2);
+        *reinterpret_cast<uint4 *>(sA + oim) = *reinterpret_cast<uint4 *>(im0);
+        *reinterpret_cast<uint4 *>(sA + kRows * KE * 2 + oim) = *reinterpret_cast<uint4 *>(im1);
+        *reinterpret_cast<uint4 *>(sA + 2 * kRows * KE * 2 + oim) = *reinterpret_cast<uint4 *>(im2);
+      }
+      for (int k = 2 * KH; k < KE; k += 8) {  // zero K padding
+        const uint32_t o = tc::kmajor_off(r, k, kRows);
+        const uint4 z = make_uint4(0, 0, 0, 0);
+        *reinterpret_cast<uint4 *>(sA + o) = z;
+        *reinterpret_cast<uint4 *>(sA + kRows * KE * 2 + o) = z;
+        *reinterpret_cast<uint4 *>(sA + 2 * kRows * KE * 2 + o) = z;
+      }
+    }
+    for (int s = 0; s < nsteps; s++) {
+      const int g = ind * nsteps + s, b = g & 1;
+      const int *st = a.steps + (size_t)(sb + s) * stride;
+      unsigned char *Bb = sB + b * bbytes;
+      copy_tile(Bb, eyb + (size_t)st[0] * a.eyb_tile, bbytes);
+      tc::fence_async_smem();
+      tc::fence_before_sync();
+      __syncthreads();
+      if (tid == 0 && ok) {
+        tc::fence_after_sync();
+        const uint32_t aA = tc::smem_u32(sA), aB = tc::smem_u32(Bb);
+        const uint32_t lboA = (kRows / 8) * 128, lboB = (NB / 8) * 128;
+        const uint32_t d0 = tmem + (uint32_t)(b * 2 * NB), d1 = d0 + (uint32_t)NB;
+        for (int kk = 0; kk < KE / 16; kk++) {
+          uint64_t ad[3], bd[3];
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            ad[c] = tc::smem_desc(aA + c * kRows * KE * 2 + kk * 2 * lboA, lboA, 128);
+            bd[c] = tc::smem_desc(aB + c * NB * KE * 2 + kk * 2 * lboB, lboB, 128);
+          }
+          const uint32_t acc = kk > 0 ? 1u : 0u;
+          tc::mma_bf16(d0, ad[0], bd[0], idesc, acc);
+          tc::mma_bf16(d1, ad[0], bd[1], idesc, acc);
+          tc::mma_bf16(d1, ad[1], bd[0], idesc, 1u);
+          tc::mma_bf16(d1, ad[0], bd[2], idesc, 1u);
+          tc::mma_bf16(d1, ad[1], bd[1], idesc, 1u);
+          tc::mma_bf16(d1, ad[2], bd[0], idesc, 1u);
+        }
+        tc::commit(&mbar[b]);
+      }
+      if (s >= 1) readout(ind, s - 1, g - 1);
+    }
+    if (nsteps > 0) readout(ind, nsteps - 1, ind * nsteps + nsteps - 1);
+    __syncthreads();
+  }
+  if (tid == 0) tc::commit(&mbar[2]);
+  if (!tc::mbar_wait(&mbar[2], 0, kWaitIters)) atomicExch(a.err, 2);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 64);
+}
+
+// ---- host-side table preparation -----------------------------------------
+
+uint16_t bf16_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);  // inf / nan
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+float bf16_to_float(uint16_t b) {
+  uint32_t u = (uint32_t)b << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+void split3_host(double v, uint16_t *s) {
+  s[0] = bf16_bits((float)v);
+  const double r1 = v - (double)bf16_to_float(s[0]);
+  s[1] = bf16_bits((float)r1);
+  const double r2 = r1 - (double)bf16_to_float(s[1]);
+  s[2] = bf16_bits((float)r2);
+}
+size_t kmajor_off_host(int r, int k, int R) {
+  return (size_t)((((k >> 3) * (R >> 3) + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+template <typename T>
+int upload_vec(T *&d, const std::vector<T> &v, std::string &msg) {
+  d = nullptr;
+  if (v.empty()) return BFGT_OK;
+  if (cudaMalloc(&d, sizeof(T) * v.size()) != cudaSuccess) {
+    msg = "cudaMalloc failed (split tables)";
+    return BFGT_ERR_OOM;
+  }
+  if (cudaMemcpy(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    msg = "cudaMemcpy failed (split tables)";
+    return BFGT_ERR_CUDA;
+  }
+  return BFGT_OK;
+}
+
+inline cplx cmulh(cplx a, cplx b) { return cplx{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+
+}  // namespace
+
+int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
+  const int n = hp.norder, npw = hp.npw, hh = hp.hh, nl = hp.nlevels, ls = hp.nlevstart;
+  if (n != 8 && n != 16) {
+    msg = "split precision supports norder 8 and 16";
+    return BFGT_ERR_CAPACITY;
+  }
+  if (hh > 32) {
+    msg = "split precision supports npw <= 64";
+    return BFGT_ERR_CAPACITY;
+  }
+  SplitPlan &sp = dp.split;
+  sp.cpc = kRows / n;
+  sp.KA = 16;
+  sp.NP = ((2 * hh + 15) / 16) * 16;
+  sp.KH = ((hh + 7) / 8) * 8;
+  sp.KE = ((2 * sp.KH + 15) / 16) * 16;
+  sp.NB = 16;
+  // chunks of up to cpc columns of one (icut, level), and their oy steps
+  std::vector<int4> chunks;
+  std::vector<int> step_begin(1, 0), steps;
+  std::vector<int> cut_chunk_begin(hp.cut_box.size() + 1, 0);
+  const std::vector<Column> &cols = hp.columns;
+  for (size_t c = 0; c < cols.size();) {
+    size_t e = c;
+    while (e < cols.size() && cols[e].icut == cols[c].icut && cols[e].level == cols[c].level && (int)(e - c) < sp.cpc) e++;
+    chunks.push_back(make_int4((int)c, (int)e, cols[c].icut, cols[c].level));
+    std::vector<size_t> ptr(e - c);
+    for (size_t q = c; q < e; q++) ptr[q - c] = cols[q].begin;
+    for (;;) {
+      int oy = INT32_MAX;
+      for (size_t q = c; q < e; q++)
+        if (ptr[q - c] < (size_t)cols[q].end) oy = std::min(oy, hp.leaves[ptr[q - c]].oy);
+      if (oy == INT32_MAX) break;
+      steps.push_back(oy);
+      for (int slot = 0; slot < sp.cpc; slot++) {
+        size_t q = c + slot;
+        if (q < e && ptr[slot] < (size_t)cols[q].end && hp.leaves[ptr[slot]].oy == oy) {
+          steps.push_back(hp.leaves[ptr[slot]].box);
+          ptr[slot]++;
+        } else {
+          steps.push_back(-1);
+        }
+      }
+    }
+    step_begin.push_back((int)(steps.size() / (1 + sp.cpc)));
+    c = e;
+  }
+  {
+    size_t c = 0;
+    for (size_t ic = 0; ic < hp.cut_box.size(); ic++) {
+      cut_chunk_begin[ic] = (int)c;
+      while (c < chunks.size() && chunks[c].z == (int)ic) c++;
+    }
+    cut_chunk_begin[hp.cut_box.size()] = (int)c;
+  }
+  // per (level, offset) operand tables
+  const long long tyt = 3LL * sp.NP * sp.KA, eyt = 3LL * sp.NB * sp.KE;
+  std::vector<long long> tyoff(nl + 1, 0), eyoff(nl + 1, 0), exoff(nl + 1, 0);
+  long long nty = 0, ney = 0, nex = 0;
+  for (int l = ls; l <= nl; l++) {
+    const long long S = 1LL << (l - ls);
+    tyoff[l] = nty;
+    eyoff[l] = ney;
+    exoff[l] = nex;
+    nty += S * tyt;
+    ney += S * eyt;
+    nex += S * (long long)npw * n;
+  }
+  std::vector<uint16_t> TyB((size_t)nty, 0), EyB((size_t)ney, 0);
+  std::vector<double2> Ex((size_t)nex);
+  for (int l = ls; l <= nl; l++) {
+    const long long S = 1LL << (l - ls);
+    const cplx *T = &hp.tab_poly2pw[(size_t)n * npw * l];
+    const cplx *E = &hp.tab_pw2pot[(size_t)n * npw * l];
+    for (long long o = 0; o < S; o++) {
+      const cplx *ph = &hp.phase[(size_t)hp.phase_off[l] + (size_t)o * npw];
+      uint16_t *ty = &TyB[(size_t)(tyoff[l] + o * tyt)];
+      const size_t ts = (size_t)sp.NP * sp.KA;  // elements per slice
+      for (int k2 = 0; k2 < hh; k2++)
+        for (int m2 = 0; m2 < n; m2++) {
+          const cplx t = cmulh(T[m2 + (size_t)n * k2], cplx{ph[k2].re, -ph[k2].im});
+          uint16_t sr[3], si[3];
+          split3_host(t.re, sr);
+          split3_host(t.im, si);
+          for (int c = 0; c < 3; c++) {
+            *(uint16_t *)((char *)(ty + c * ts) + kmajor_off_host(k2, m2, sp.NP)) = sr[c];
+            *(uint16_t *)((char *)(ty + c * ts) + kmajor_off_host(hh + k2, m2, sp.NP)) = si[c];
+          }
+        }
+      uint16_t *ey = &EyB[(size_t)(eyoff[l] + o * eyt)];
+      const size_t es = (size_t)sp.NB * sp.KE;
+      for (int k2 = 0; k2 < n; k2++)
+        for (int m2 = 0; m2 < hh; m2++) {
+          const cplx e0 = cmulh(E[m2 + (size_t)npw * k2], ph[m2]);
+          const double w = hp.pw_weight[m2];
+          uint16_t sr[3], si[3];
+          split3_host(w * e0.re, sr);
+          split3_host(-w * e0.im, si);
+          for (int c = 0; c < 3; c++) {
+            *(uint16_t *)((char *)(ey + c * es) + kmajor_off_host(k2, m2, sp.NB)) = sr[c];
+            *(uint16_t *)((char *)(ey + c * es) + kmajor_off_host(k2, sp.KH + m2, sp.NB)) = si[c];
+          }
+        }
+      double2 *ex = &Ex[(size_t)(exoff[l] + o * (long long)npw * n)];
+      for (int m1 = 0; m1 < npw; m1++)
+        for (int k1 = 0; k1 < n; k1++) {
+          const cplx v = cmulh(E[m1 + (size_t)npw * k1], ph[m1]);
+          ex[(size_t)m1 * n + k1] = make_double2(v.re, v.im);
+        }
+    }
+  }
+  sp.tyb_tile = tyt;
+  sp.eyb_tile = eyt;
+  sp.nchunks = (int)chunks.size();
+  int rc = BFGT_OK;
+  auto chk = [&](int x) {
+    if (rc == BFGT_OK && x != BFGT_OK) rc = x;
+  };
+  chk(upload_vec(sp.chunks, chunks, msg));
+  chk(upload_vec(sp.step_begin, step_begin, msg));
+  chk(upload_vec(sp.steps, steps, msg));
+  chk(upload_vec(sp.TyB, TyB, msg));
+  chk(upload_vec(sp.EyB, EyB, msg));
+  chk(upload_vec(sp.Ex, Ex, msg));
+  chk(upload_vec(sp.tyb_off, tyoff, msg));
+  chk(upload_vec(sp.eyb_off, eyoff, msg));
+  chk(upload_vec(sp.ex_off, exoff, msg));
+  std::vector<int> zero(4, 0);
+  chk(upload_vec(sp.err, zero, msg));
+  if (rc != BFGT_OK) return rc;
+  // the reduction and the rest of the pipeline use the tensor-core chunking
+  if (dp.Mpart) cudaFree(dp.Mpart);
+  dp.Mpart = nullptr;
+  if (cudaMalloc(&dp.Mpart, sizeof(double2) * (size_t)dp.nd * dp.nexp * std::max<size_t>(chunks.size(), 1)) != cudaSuccess) {
+    msg = "cudaMalloc failed (split partial expansions)";
+    return BFGT_ERR_OOM;
+  }
+  if (dp.cut_chunk_begin) cudaFree(dp.cut_chunk_begin);
+  chk(upload_vec(dp.cut_chunk_begin, cut_chunk_begin, msg));
+  dp.nchunks = (int)chunks.size();
+  // shared memory
+  {
+    const int abytes = 3 * kRows * sp.KA * 2, bbytes = 3 * sp.NP * sp.KA * 2;
+    const int ybytes = kRows * hh * 16;
+    const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 1023) / 1024) * 1024;
+    sp.smem_form = 1024 + ubytes + sizeof(double2) * ((size_t)n * npw + (size_t)sp.cpc * npw);
+    const int eab = 3 * kRows * sp.KE * 2, ebb = 3 * sp.NB * sp.KE * 2;
+    sp.smem_eval = 1024 + ((eab + 1023) / 1024) * 1024 + ((2 * ebb + 1023) / 1024) * 1024 + sizeof(double2) * (size_t)npw * hh;
+  }
+  const int ntiles = ((npw + 1) / 2) * ((hh + 3) / 4);
+  sp.nt = (ntiles + kThreads - 1) / kThreads;
+  if (sp.nt > 2) {
+    msg = "split precision: x-contraction tile count exceeds the built kernels";
+    return BFGT_ERR_CAPACITY;
+  }
+  if (sp.smem_form > 227 * 1024 || sp.smem_eval > 227 * 1024) {
+    msg = "split precision: shared memory need exceeds 227 KB";
+    return BFGT_ERR_CAPACITY;
+  }
+  cudaFuncSetAttribute(k_form_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaFuncSetAttribute(k_form_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaFuncSetAttribute(k_eval_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  sp.wait_iters = kWaitIters;
+  // tensor-core FLOP issued per transform (every slice product counted)
+  const double nsteps_total = (double)(steps.size() / (1 + sp.cpc));
+  sp.tc_flops_form = nsteps_total * hp.nd * 6.0 * (sp.KA / 16) * 2.0 * kRows * sp.NP * 16;
+  sp.tc_flops_eval = nsteps_total * hp.nd * 6.0 * (sp.KE / 16) * 2.0 * kRows * sp.NB * 16;
+  return rc;
+}
+
+void split_plan_destroy(DevicePlan &dp) {
+  SplitPlan &sp = dp.split;
+  void *ptrs[] = {sp.chunks, sp.step_begin, sp.steps, sp.TyB, sp.EyB, sp.Ex, sp.tyb_off, sp.eyb_off, sp.ex_off, sp.err};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  sp = SplitPlan();
+}
+
+void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
+  SplitPlan &sp = dp.split;
+  FormTcArgs a{d_fvals, sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.TyB, sp.tyb_off, sp.tyb_tile, dp.T,
+               dp.PH, dp.ph_off, dp.Mpart, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NP, sp.KA,
+               sp.wait_iters};
+  if (sp.nt == 1) k_form_tc<1><<<sp.nchunks, kThreads, sp.smem_form, s>>>(a);
+  else k_form_tc<2><<<sp.nchunks, kThreads, sp.smem_form, s>>>(a);
+}
+
+void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
+  SplitPlan &sp = dp.split;
+  EvalTcArgs a{d_pot, sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, sp.Ex,
+               sp.ex_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
+               sp.wait_iters};
+  k_eval_tc<<<sp.nchunks, kThreads, sp.smem_eval, s>>>(a);
+}
+
+int split_check(DevicePlan &dp) {
+  if (!dp.split.err) return BFGT_OK;
+  int h[4] = {0, 0, 0, 0};
+  if (cudaMemcpy(h, dp.split.err, sizeof(int) * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return BFGT_ERR_CUDA;
+  if (h[0]) {
+    cudaMemset(dp.split.err, 0, sizeof(int) * 4);
+    return BFGT_ERR_TIMEOUT;
+  }
+  return BFGT_OK;
+}
 
 }  // namespace bfgt

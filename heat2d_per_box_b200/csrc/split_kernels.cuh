@@ -14,5 +14,9 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);
 void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s);
 // cutoff expansions -> leaf values, accumulated into pot (same as k_eval_fp64)
 void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s);
+void split_plan_destroy(DevicePlan &dp);
+// Reads and clears the device error flag of the tensor-core kernels (waits
+// for the device); BFGT_ERR_TIMEOUT if a bounded wait gave up.
+int split_check(DevicePlan &dp);
 
 }  // namespace bfgt

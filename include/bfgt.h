@@ -122,6 +122,12 @@ int bfgt_plan_info(bfgt_plan plan, int *out);
    form and eval stages.  out must hold 16. */
 int bfgt_plan_work(bfgt_plan plan, double *out);
 
+/* Waits for the device and reports failures of earlier executes on this plan:
+   BFGT_ERR_TIMEOUT if a bounded device-side wait of the tensor-core pipeline
+   gave up (the results of that execute are not valid), BFGT_ERR_CUDA on a
+   device error.  Clears the flag. */
+int bfgt_plan_check(bfgt_plan plan);
+
 int bfgt_plan_destroy(bfgt_plan plan);
 
 /* ---- host-side plan introspection (no device needed) ------------------- */

@@ -1,0 +1,85 @@
+"""Split-precision tensor-core path (tcgen05, BF16x3 slices) vs the FP64 oracle.
+
+Specified bar: relative L2 error over leaf values <= 1e-6 against the FP64
+oracle (and <= 10*eps where eps >= 1e-7)."""
+import numpy as np
+import pytest
+
+import heat2d_per_box_b200 as hb
+from oracle import oracle
+
+from conftest import gauss_sum
+
+pytestmark = pytest.mark.gpu
+
+SPLIT_TOL = 1e-6
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def run_split(t, delta, eps, fvals=None, nd=1, pot0=None):
+    import torch
+    plan = hb.Plan(t, delta, eps, nd=nd, precision=hb.BFGT_PREC_SPLIT)
+    fv = t.fvals if fvals is None else fvals
+    f = torch.from_numpy(np.ascontiguousarray(fv).reshape(-1)).cuda()
+    p = torch.zeros_like(f) if pot0 is None else torch.from_numpy(pot0.copy()).cuda()
+    plan.execute(f, p)
+    plan.check()
+    out = p.cpu().numpy()
+    info = plan.info()
+    plan.close()
+    return out, info
+
+
+CASES = [("ad16_leg_per", 1e-4, 1e-6), ("ad16_leg_per", 1e-3, 1e-9), ("ad16_leg_per", 1e-2, 1e-6),
+         ("ad_leg_per", 1e-4, 1e-6), ("ad_cheb_free", 1e-4, 1e-9), ("uni3_leg_per", 1e-3, 1e-9),
+         ("uni3_cheb_per", 1e-2, 1e-6)]
+
+
+@pytest.mark.parametrize("name,delta,eps", CASES)
+def test_split_matches_oracle(trees, name, delta, eps):
+    t = trees[name]
+    got, info = run_split(t, delta, eps)
+    ref = oracle.boxfgt(t, t.fvals, delta, eps)
+    lv = t.leaves()
+    err = rel_l2(got.reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv])
+    tol = SPLIT_TOL if eps < 1e-7 else min(SPLIT_TOL, 10 * eps)
+    assert err < tol, (err, info)
+
+
+def test_split_benchmark_statistics_tree():
+    """Adaptive order-16 tree with the benchmark's density statistics (smaller base level)."""
+    rng = np.random.default_rng(2)
+    g = hb.gauss_params(rng.uniform(-0.5, 0.5, (20, 2)), np.exp(rng.uniform(np.log(1e-3), np.log(1e-2), 20)),
+                        rng.standard_normal(20))
+    t = hb.build_adaptive(g, norder=16, ipoly=0, iperiod=1, eps=1e-10, eta=1.0, minlev=6, maxlev=12)
+    for delta, eps in [(1e-4, 1e-6), (1e-2, 1e-6), (1e-4, 1e-9)]:
+        got, info = run_split(t, delta, eps)
+        ref = oracle.boxfgt(t, t.fvals, delta, eps)
+        lv = t.leaves()
+        err = rel_l2(got.reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv])
+        assert err < SPLIT_TOL, (delta, eps, err, info)
+
+
+def test_split_multiple_densities_and_accumulate(trees):
+    t = trees["ad16_leg_per"]
+    nd = 2
+    rng = np.random.default_rng(3)
+    fv = np.stack([t.fvals, rng.standard_normal(t.fvals.shape)], axis=2)
+    pot0 = rng.standard_normal(t.nboxes * t.npbox * nd)
+    got, _ = run_split(t, 1e-4, 1e-6, fvals=fv, nd=nd, pot0=pot0)
+    ref = oracle.boxfgt(t, fv, 1e-4, 1e-6, nd=nd)
+    lv = t.leaves()
+    g = (got - pot0).reshape(t.nboxes, -1)[lv]
+    assert rel_l2(g, ref.reshape(t.nboxes, -1)[lv]) < SPLIT_TOL
+    nonleaf = np.nonzero(t.nchild() > 0)[0]
+    np.testing.assert_array_equal(got.reshape(t.nboxes, -1)[nonleaf], pot0.reshape(t.nboxes, -1)[nonleaf])
+
+
+def test_split_deterministic(trees):
+    t = trees["ad16_leg_per"]
+    a, _ = run_split(t, 1e-4, 1e-6)
+    b, _ = run_split(t, 1e-4, 1e-6)
+    np.testing.assert_array_equal(a, b)

@@ -17,8 +17,7 @@ struct SplitPlan {
   int4 *chunks = nullptr;
   int *step_begin = nullptr, *steps = nullptr;
   uint16_t *TyB = nullptr, *EyB = nullptr;
-  double2 *Ex = nullptr;
-  long long *tyb_off = nullptr, *eyb_off = nullptr, *ex_off = nullptr;
+  long long *tyb_off = nullptr, *eyb_off = nullptr;
   long long tyb_tile = 0, eyb_tile = 0;
   int *err = nullptr;
   uint32_t wait_iters = 0;

@@ -109,34 +109,59 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
   bool ok = true;
   const int r = tid, rslot = r / n, rm1 = r - rslot * n;
 
+  // per-thread share of a B tile (16-byte pieces)
+  const int bpieces = bbytes / 16;
+  constexpr int kMaxPieces = 4;  // bbytes <= 3*64*16*2 = 6 KB -> 384 pieces / 128 threads = 3
   for (int ind = 0; ind < nd; ind++) {
+    // software pipeline: the leaf values and the B tile of step s+1 are
+    // loaded into registers while step s is converted and multiplied
+    double fnext[16];
+    uint4 bnext[kMaxPieces];
+    auto load_step = [&](int s2) {
+      const int *st2 = a.steps + (size_t)(sb + s2) * stride;
+      const int box = st2[1 + rslot];
+      const double *fv = a.fvals + (size_t)(box < 0 ? 0 : box) * nd * npb + ind + (size_t)nd * rm1;
+#pragma unroll
+      for (int k = 0; k < 16; k++) fnext[k] = (box >= 0 && k < n) ? fv[(size_t)nd * n * k] : 0.0;
+      const uint4 *src = reinterpret_cast<const uint4 *>(tyb + (size_t)st2[0] * a.tyb_tile);
+#pragma unroll
+      for (int q = 0; q < kMaxPieces; q++) {
+        const int i = tid + kThreads * q;
+        if (i < bpieces) bnext[q] = src[i];
+      }
+    };
+    if (nsteps > 0) load_step(0);
     for (int s = 0; s < nsteps; s++) {
       const int g = ind * nsteps + s, b = g & 1;
+      double fcur[16];
+      uint4 bcur[kMaxPieces];
+#pragma unroll
+      for (int k = 0; k < 16; k++) fcur[k] = fnext[k];
+#pragma unroll
+      for (int q = 0; q < kMaxPieces; q++) bcur[q] = bnext[q];
+      if (s + 1 < nsteps) load_step(s + 1);
       if (g >= 2 && ok && !tc::mbar_wait(&mbar[b], ((g >> 1) - 1) & 1, a.wait_iters)) {
         ok = false;
         atomicExch(a.err, 1);
       }
-      const int *st = a.steps + (size_t)(sb + s) * stride;
       unsigned char *Ab = U + b * bufbytes, *Bb = Ab + abytes;
-      {
-        // A row r = (slot, m1): F(m1, m2) for m2 = 0..n-1, zero-padded to KA
-        const int box = (rslot < cpc) ? st[1 + rslot] : -1;
-        const double *fv = a.fvals + (size_t)(box < 0 ? 0 : box) * nd * npb + ind + (size_t)nd * rm1;
-        for (int h = 0; h < KA / 8; h++) {
-          uint16_t s0[8], s1[8], s2[8];
+      // A row r = (slot, m1): F(m1, m2) for m2 = 0..n-1, zero-padded to KA
 #pragma unroll
-          for (int q = 0; q < 8; q++) {
-            const int k = 8 * h + q;
-            const double v = (box >= 0 && k < n) ? fv[(size_t)nd * n * k] : 0.0;
-            tc::split3_bf16(v, s0[q], s1[q], s2[q]);
-          }
-          const uint32_t off = tc::kmajor_off(r, 8 * h, kRows);
-          *reinterpret_cast<uint4 *>(Ab + off) = *reinterpret_cast<uint4 *>(s0);
-          *reinterpret_cast<uint4 *>(Ab + kRows * KA * 2 + off) = *reinterpret_cast<uint4 *>(s1);
-          *reinterpret_cast<uint4 *>(Ab + 2 * kRows * KA * 2 + off) = *reinterpret_cast<uint4 *>(s2);
-        }
+      for (int h = 0; h < 2; h++) {
+        if (h >= KA / 8) break;
+        uint16_t s0[8], s1[8], s2[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) tc::split3_bf16(fcur[8 * h + q], s0[q], s1[q], s2[q]);
+        const uint32_t off = tc::kmajor_off(r, 8 * h, kRows);
+        *reinterpret_cast<uint4 *>(Ab + off) = *reinterpret_cast<uint4 *>(s0);
+        *reinterpret_cast<uint4 *>(Ab + kRows * KA * 2 + off) = *reinterpret_cast<uint4 *>(s1);
+        *reinterpret_cast<uint4 *>(Ab + 2 * kRows * KA * 2 + off) = *reinterpret_cast<uint4 *>(s2);
       }
-      copy_tile(Bb, tyb + (size_t)st[0] * a.tyb_tile, bbytes);
+#pragma unroll
+      for (int q = 0; q < kMaxPieces; q++) {
+        const int i = tid + kThreads * q;
+        if (i < bpieces) reinterpret_cast<uint4 *>(Bb)[i] = bcur[q];
+      }
       tc::fence_async_smem();
       tc::fence_before_sync();
       __syncthreads();
@@ -250,8 +275,9 @@ struct EvalTcArgs {
   const uint16_t *EyB;     // per (level, oy): 3 slices x NB rows x KE, K-major core layout
   const long long *eyb_off;
   long long eyb_tile;
-  const double2 *Ex;       // per (level, ox): E(m1,k1) phase_ox(m1), [m1][k1]
-  const long long *ex_off;
+  const double2 *E;        // tab_pw2pot, per level (npw, n)
+  const double2 *PH;
+  const long long *ph_off;
   const double2 *L;
   int *err;
   int nd, n, npw, hh, nexp, cpc, NB, KE, KH;
@@ -270,6 +296,8 @@ __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
   unsigned char *sA = smem + 1024;
   unsigned char *sB = sA + ((abytes + 1023) / 1024) * 1024;  // two buffers
   double2 *sL = reinterpret_cast<double2 *>(sB + ((2 * bbytes + 1023) / 1024) * 1024);  // [m1][m2]
+  double2 *sE = sL + (size_t)npw * hh;                                                    // [m1][k1]
+  double2 *sph = sE + (size_t)npw * n;                                                    // [slot][m1]
   (void)lane;
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, 64);
@@ -287,7 +315,15 @@ __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
   const int sb = a.step_begin[blockIdx.x], se = a.step_begin[blockIdx.x + 1], nsteps = se - sb;
   const int stride = 1 + cpc;
   const uint16_t *eyb = a.EyB + a.eyb_off[ch.w];
-  const double2 *exl = a.Ex + a.ex_off[ch.w];
+  // E(m1,k1) of this level and the x phases of the chunk's columns (FP64)
+  for (int i = tid; i < npw * n; i += kThreads) {
+    const int m = i % npw, k = i / npw;
+    sE[m * n + k] = a.E[(size_t)n * npw * ch.w + i];
+  }
+  for (int i = tid; i < ncol * npw; i += kThreads) {
+    const int slot = i / npw, m = i - slot * npw;
+    sph[i] = a.PH[a.ph_off[ch.w] + (size_t)a.columns[ch.x + slot].z * npw + m];
+  }
   bool ok = true;
   const int r = tid, rslot = r / n, rk1 = r - rslot * n;
   const uint32_t lanebase = (uint32_t)(32 * warp) << 16;
@@ -295,6 +331,12 @@ __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
   // wait for the MMAs of global step g (density ind, step s), add 2 Re(...) into pot
   auto readout = [&](int ind, int s, int g) {
     const int b = g & 1;
+    const int *st = a.steps + (size_t)(sb + s) * stride;
+    const int box = st[1 + rslot];
+    double *pb = a.pot + (size_t)(box < 0 ? 0 : box) * nd * npb + ind + (size_t)nd * rk1;
+    double pv[16];
+#pragma unroll
+    for (int k2 = 0; k2 < 16; k2++) pv[k2] = (box >= 0 && k2 < n) ? pb[(size_t)nd * n * k2] : 0.0;
     if (ok && !tc::mbar_wait(&mbar[b], (g >> 1) & 1, a.wait_iters)) {
       ok = false;
       atomicExch(a.err, 1);
@@ -304,11 +346,10 @@ __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
     tc::tmem_ld16(tmem + lanebase + (uint32_t)(b * 2 * NB), v0);
     tc::tmem_ld16(tmem + lanebase + (uint32_t)(b * 2 * NB + NB), v1);
     tc::tmem_ld_wait();
-    const int *st = a.steps + (size_t)(sb + s) * stride;
-    const int box = st[1 + rslot];
     if (ok && box >= 0) {
-      double *pb = a.pot + (size_t)box * nd * npb + ind;
-      for (int k2 = 0; k2 < n; k2++) pb[(size_t)nd * (rk1 + n * k2)] += 2.0 * ((double)v0[k2] + (double)v1[k2]);
+#pragma unroll
+      for (int k2 = 0; k2 < 16; k2++)
+        if (k2 < n) pb[(size_t)nd * n * k2] = pv[k2] + 2.0 * ((double)v0[k2] + (double)v1[k2]);
     }
     tc::fence_before_sync();
   };
@@ -320,17 +361,17 @@ __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
       sL[m1 * hh + m2] = Lg[e];
     }
     __syncthreads();
-    // H(k1,m2) = sum_m1 Ex_ox(m1,k1) L(m1,m2) for row r = (slot, k1), sliced into the A operand
+    // H(k1,m2) = sum_m1 E(m1,k1) phase_ox(m1) L(m1,m2) for row r = (slot, k1), sliced into the A operand
     {
       const bool live = rslot < ncol;
-      const double2 *ex = live ? exl + (size_t)a.columns[ch.x + rslot].z * npw * n : exl;
       for (int mb = 0; mb < KH; mb += 8) {
         double2 acc[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) acc[j] = make_double2(0, 0);
         if (live) {
+#pragma unroll 2
           for (int m1 = 0; m1 < npw; m1++) {
-            const double2 e = ex[(size_t)m1 * n + rk1];
+            const double2 e = zmul(sE[m1 * n + rk1], sph[rslot * npw + m1]);
 #pragma unroll
             for (int j = 0; j < 8; j++) {
               const double2 l = (mb + j < hh) ? sL[m1 * hh + mb + j] : make_double2(0, 0);
@@ -363,11 +404,31 @@ __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
         *reinterpret_cast<uint4 *>(sA + 2 * kRows * KE * 2 + o) = z;
       }
     }
+    const int bpieces = bbytes / 16;
+    constexpr int kMaxPieces = 4;
+    uint4 bnext[kMaxPieces];
+    auto load_tile = [&](int s2) {
+      const int *st2 = a.steps + (size_t)(sb + s2) * stride;
+      const uint4 *src = reinterpret_cast<const uint4 *>(eyb + (size_t)st2[0] * a.eyb_tile);
+#pragma unroll
+      for (int q = 0; q < kMaxPieces; q++) {
+        const int i = tid + kThreads * q;
+        if (i < bpieces) bnext[q] = src[i];
+      }
+    };
+    if (nsteps > 0) load_tile(0);
     for (int s = 0; s < nsteps; s++) {
       const int g = ind * nsteps + s, b = g & 1;
-      const int *st = a.steps + (size_t)(sb + s) * stride;
       unsigned char *Bb = sB + b * bbytes;
-      copy_tile(Bb, eyb + (size_t)st[0] * a.eyb_tile, bbytes);
+      uint4 bcur[kMaxPieces];
+#pragma unroll
+      for (int q = 0; q < kMaxPieces; q++) bcur[q] = bnext[q];
+      if (s + 1 < nsteps) load_tile(s + 1);
+#pragma unroll
+      for (int q = 0; q < kMaxPieces; q++) {
+        const int i = tid + kThreads * q;
+        if (i < bpieces) reinterpret_cast<uint4 *>(Bb)[i] = bcur[q];
+      }
       tc::fence_async_smem();
       tc::fence_before_sync();
       __syncthreads();
@@ -507,19 +568,16 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   }
   // per (level, offset) operand tables
   const long long tyt = 3LL * sp.NP * sp.KA, eyt = 3LL * sp.NB * sp.KE;
-  std::vector<long long> tyoff(nl + 1, 0), eyoff(nl + 1, 0), exoff(nl + 1, 0);
-  long long nty = 0, ney = 0, nex = 0;
+  std::vector<long long> tyoff(nl + 1, 0), eyoff(nl + 1, 0);
+  long long nty = 0, ney = 0;
   for (int l = ls; l <= nl; l++) {
     const long long S = 1LL << (l - ls);
     tyoff[l] = nty;
     eyoff[l] = ney;
-    exoff[l] = nex;
     nty += S * tyt;
     ney += S * eyt;
-    nex += S * (long long)npw * n;
   }
   std::vector<uint16_t> TyB((size_t)nty, 0), EyB((size_t)ney, 0);
-  std::vector<double2> Ex((size_t)nex);
   for (int l = ls; l <= nl; l++) {
     const long long S = 1LL << (l - ls);
     const cplx *T = &hp.tab_poly2pw[(size_t)n * npw * l];
@@ -553,12 +611,6 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
             *(uint16_t *)((char *)(ey + c * es) + kmajor_off_host(k2, sp.KH + m2, sp.NB)) = si[c];
           }
         }
-      double2 *ex = &Ex[(size_t)(exoff[l] + o * (long long)npw * n)];
-      for (int m1 = 0; m1 < npw; m1++)
-        for (int k1 = 0; k1 < n; k1++) {
-          const cplx v = cmulh(E[m1 + (size_t)npw * k1], ph[m1]);
-          ex[(size_t)m1 * n + k1] = make_double2(v.re, v.im);
-        }
     }
   }
   sp.tyb_tile = tyt;
@@ -573,10 +625,8 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   chk(upload_vec(sp.steps, steps, msg));
   chk(upload_vec(sp.TyB, TyB, msg));
   chk(upload_vec(sp.EyB, EyB, msg));
-  chk(upload_vec(sp.Ex, Ex, msg));
   chk(upload_vec(sp.tyb_off, tyoff, msg));
   chk(upload_vec(sp.eyb_off, eyoff, msg));
-  chk(upload_vec(sp.ex_off, exoff, msg));
   std::vector<int> zero(4, 0);
   chk(upload_vec(sp.err, zero, msg));
   if (rc != BFGT_OK) return rc;
@@ -597,7 +647,8 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 1023) / 1024) * 1024;
     sp.smem_form = 1024 + ubytes + sizeof(double2) * ((size_t)n * npw + (size_t)sp.cpc * npw);
     const int eab = 3 * kRows * sp.KE * 2, ebb = 3 * sp.NB * sp.KE * 2;
-    sp.smem_eval = 1024 + ((eab + 1023) / 1024) * 1024 + ((2 * ebb + 1023) / 1024) * 1024 + sizeof(double2) * (size_t)npw * hh;
+    sp.smem_eval = 1024 + ((eab + 1023) / 1024) * 1024 + ((2 * ebb + 1023) / 1024) * 1024 +
+                   sizeof(double2) * ((size_t)npw * hh + (size_t)npw * n + (size_t)sp.cpc * npw);
   }
   const int ntiles = ((npw + 1) / 2) * ((hh + 3) / 4);
   sp.nt = (ntiles + kThreads - 1) / kThreads;
@@ -622,7 +673,7 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
 
 void split_plan_destroy(DevicePlan &dp) {
   SplitPlan &sp = dp.split;
-  void *ptrs[] = {sp.chunks, sp.step_begin, sp.steps, sp.TyB, sp.EyB, sp.Ex, sp.tyb_off, sp.eyb_off, sp.ex_off, sp.err};
+  void *ptrs[] = {sp.chunks, sp.step_begin, sp.steps, sp.TyB, sp.EyB, sp.tyb_off, sp.eyb_off, sp.err};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   sp = SplitPlan();
@@ -639,8 +690,8 @@ void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
 
 void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
   SplitPlan &sp = dp.split;
-  EvalTcArgs a{d_pot, sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, sp.Ex,
-               sp.ex_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
+  EvalTcArgs a{d_pot, sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, dp.E,
+               dp.PH, dp.ph_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
                sp.wait_iters};
   k_eval_tc<<<sp.nchunks, kThreads, sp.smem_eval, s>>>(a);
 }

@@ -76,6 +76,12 @@ def lib():
     L.bfgt_plan_info.argtypes = [C.c_void_p, _i32p]
     L.bfgt_plan_work.restype = C.c_int
     L.bfgt_plan_work.argtypes = [C.c_void_p, _f64p]
+    L.bfgt_plan_execute_noalloc.restype = C.c_int
+    L.bfgt_plan_execute_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.bfgt_noalloc_scratch_bytes.restype = C.c_int
+    L.bfgt_noalloc_scratch_bytes.argtypes = [C.POINTER(C.c_size_t)]
+    L.bfgt_plan_noalloc_need.restype = C.c_int
+    L.bfgt_plan_noalloc_need.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
     L.bfgt_plan_check.restype = C.c_int
     L.bfgt_plan_check.argtypes = [C.c_void_p]
     L.bfgt_plan_destroy.restype = C.c_int

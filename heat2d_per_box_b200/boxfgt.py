@@ -81,6 +81,17 @@ class Plan:
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         _lib.check(self._L.bfgt_plan_execute(self._h, self._ptr(d_fvals), self._ptr(d_pot), s))
 
+    def execute_noalloc(self, d_fvals, d_pot, stream=None):
+        """Same transform as execute(), with no device allocation: the plane-wave
+        scratch comes from the library's static per-GPU array (see bfgt.h)."""
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_plan_execute_noalloc(self._h, self._ptr(d_fvals), self._ptr(d_pot), s))
+
+    def noalloc_need(self):
+        v = C.c_size_t()
+        _lib.check(self._L.bfgt_plan_noalloc_need(self._h, C.byref(v)))
+        return int(v.value)
+
     def execute_host(self, fvals, pot, stream=None):
         fv = np.ascontiguousarray(fvals, np.float64)
         if not (isinstance(pot, np.ndarray) and pot.dtype == np.float64 and pot.flags.c_contiguous):

@@ -13,12 +13,8 @@
 #include "device_plan.hpp"
 #include "host_plan.hpp"
 #include "split_kernels.cuh"
+#include "plan_internal.hpp"
 
-struct bfgt_plan_s {
-  bfgt::HostPlan hp;
-  bfgt::DevicePlan dp;
-  double stage_ms[8] = {0};
-};
 
 struct bfgt_tree_s {
   std::unique_ptr<bfgt::TreeData> t;
@@ -61,6 +57,15 @@ double now_s() {
 }
 
 }  // namespace
+
+// used by noalloc.cu to report through bfgt_last_error
+int bfgt_record_error(int code, const char *msg) {
+  if (code == BFGT_OK) {
+    g_err.clear();
+    return BFGT_OK;
+  }
+  return fail(code, msg ? msg : "");
+}
 
 extern "C" {
 

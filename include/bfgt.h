@@ -89,6 +89,21 @@ int bfgt_plan_execute(bfgt_plan plan, const double *d_fvals, double *d_pot, void
    result into the host pot (the reference-facing form of a planned call). */
 int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, void *stream);
 
+/* No counterpart in the reference (the Fortran boxfgt allocates its own
+   workspace on every call).  Runs the same transform as bfgt_plan_execute
+   without allocating anything: the plane-wave scratch (partial expansions of
+   the leaf chunks and the cutoff-box expansions) comes from one static device
+   array of bfgt_noalloc_scratch_bytes() (32 MiB) per GPU, held until exit.
+   For callers that may not allocate device memory while they step, e.g.
+   inside their own graph capture or under an allocator that owns the device.
+   Plans whose scratch need (bfgt_plan_noalloc_need) exceeds the array are
+   rejected with BFGT_ERR_CAPACITY.  The first call on a device looks up the
+   array's address (cudaGetSymbolAddress) and should come before any stream
+   capture; calls that overlap on the GPU share, and race on, the array. */
+int bfgt_plan_execute_noalloc(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream);
+int bfgt_noalloc_scratch_bytes(size_t *bytes);
+int bfgt_plan_noalloc_need(bfgt_plan plan, size_t *bytes);
+
 /* Capture bfgt_plan_execute for these device buffers into a CUDA graph and
    replay it with bfgt_plan_graph_launch. */
 int bfgt_plan_graph_capture(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream);

@@ -43,9 +43,14 @@ struct DevicePlan {
   int *cut_chunk_begin = nullptr, *cut_pw_begin = nullptr, *cut_pw_src = nullptr, *cut_pw_ind = nullptr;
   double2 *W = nullptr;         // cutoff shifts (nexp, 9)
   double *pw_weight = nullptr;  // (hh)
-  double2 *Mpart = nullptr;     // (nchunks, nd, nexp)
-  double2 *M = nullptr;         // (ncut, nd, nexp)
-  double2 *L = nullptr;         // (ncut, nd, nexp)
+  double2 *Mpart = nullptr;     // (nchunks, nd, nexp) partial expansions per chunk
+  double2 *M = nullptr;         // (ncut, nd, nexp) cutoff-box expansions
+  double2 *L = nullptr;         // (ncut, nd, nexp) cutoff-box local expansions
+  double2 *G = nullptr;         // (ngroups, nd, nexp) group sums (boxes with > 32 chunks)
+  int *gcnt = nullptr, *bcnt = nullptr, *chunk_group = nullptr, *box_groups = nullptr;
+  int4 *groups = nullptr;
+  int ngroups = 0;
+  bool multi_group = false;
   SplitPlan split;
   // near field
   int *nf_target = nullptr, *nf_level = nullptr, *nf_begin = nullptr, *nf_src = nullptr;
@@ -64,6 +69,10 @@ struct DevicePlan {
   cudaGraphExec_t graph_exec = nullptr;
   size_t smem_form = 0, smem_eval = 0, smem_near = 0;
 };
+
+struct ReduceArgs;
+// (Re)builds the reduction groups for a chunk list sorted by cutoff box.
+int build_reduce_groups(DevicePlan &dp, const std::vector<int> &cut_of_chunk, std::string &msg);
 
 // Allocates and uploads; returns a BFGT_* status and fills msg on failure.
 int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);

@@ -8,7 +8,8 @@
 //   ancestor is one phase exp(-i ts.(c_leaf - c_anc)/sqrt(delta0)), taken from
 //   a precomputed FP64 phase table, and each leaf's expansion is added
 //   straight into its ancestor's expansion.  Partial sums per chunk of leaves
-//   are reduced in a fixed order (k_reduce), so the result is deterministic.
+//   are summed in a fixed chunk order by the last CTA of each cutoff box, so
+//   the result is deterministic.
 //   step 3 (mp -> loc at the cutoff level, boxfgt.f:805-822) is k_translate.
 //   step 4 (split, boxfgt.f:845-863, gnd_shiftpw_loc bfgt_pwrouts.f:1905-1941)
 //   and step 5 (loc PW -> values, boxfgt.f:884-900, g2d_pw2pot
@@ -28,6 +29,7 @@
 
 #include "../../include/bfgt.h"
 #include "device_plan.hpp"
+#include "fgt_common.cuh"
 #include "split_kernels.cuh"
 
 namespace bfgt {
@@ -55,6 +57,7 @@ struct FormArgs {
   const double2 *PH;
   const long long *ph_off;
   double2 *Mpart;
+  ReduceArgs red;
   int nd, n, npw, hh, nexp;
 };
 
@@ -68,6 +71,28 @@ struct FormArgs {
 // expansion shifted to the ancestor (steps 1+2, boxfgt.f:728-783).  The M
 // accumulators of a warp stay in registers (NT tiles of TM x TN per lane)
 // across its columns; warps are then summed in a fixed order.
+// L(icut) = M(icut) + sum over its plane-wave list of M(src) * W(shift)
+// (mp -> loc at the cutoff level, boxfgt.f:805-822), one thread per element.
+__global__ void k_translate(const double2 *__restrict__ M, const int *__restrict__ pw_begin,
+                            const int *__restrict__ pw_src, const int *__restrict__ pw_ind,
+                            const double2 *__restrict__ W, double2 *__restrict__ L, int ncut, int nd, int nexp) {
+  const size_t per = (size_t)nd * nexp;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= per * ncut) return;
+  const int icut = (int)(idx / per);
+  const size_t r = idx - (size_t)icut * per;
+  const int e = (int)(r % nexp);
+  double2 s = M[idx];
+  for (int j = pw_begin[icut]; j < pw_begin[icut + 1]; j++) {
+    const double2 m = M[(size_t)pw_src[j] * per + r];
+    const double2 w = W[(size_t)pw_ind[j] * nexp + e];
+    s.x += m.x * w.x - m.y * w.y;
+    s.y += m.x * w.y + m.y * w.x;
+  }
+  L[idx] = s;
+}
+
+
 template <int TM, int TN, int NT>
 __global__ void __launch_bounds__(kWarps * 32, 3) k_form_fp64(FormArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -186,40 +211,8 @@ __global__ void __launch_bounds__(kWarps * 32, 3) k_form_fp64(FormArgs a) {
     for (int e = threadIdx.x; e < a.nexp; e += blockDim.x) out[e] = sRed[e];
     __syncthreads();
   }
-}
-
-// M(icut, ind, :) = sum over the cutoff box's chunks, in chunk order
-__global__ void k_reduce(const double2 *__restrict__ Mpart, const int *__restrict__ cut_chunk_begin,
-                         double2 *__restrict__ M, int nd, int nexp) {
-  const int ic = blockIdx.x, ind = blockIdx.y;
-  const int c0 = cut_chunk_begin[ic], c1 = cut_chunk_begin[ic + 1];
-  for (int e = blockIdx.z * blockDim.x + threadIdx.x; e < nexp; e += gridDim.z * blockDim.x) {
-    double2 s = make_double2(0, 0);
-    for (int c = c0; c < c1; c++) {
-      const double2 v = Mpart[((size_t)c * nd + ind) * nexp + e];
-      s.x += v.x;
-      s.y += v.y;
-    }
-    M[((size_t)ic * nd + ind) * nexp + e] = s;
-  }
-}
-
-// L(icut) = M(icut) + sum_{listpw} M(src) * W(shift)   (boxfgt.f:805-822)
-__global__ void k_translate(const double2 *__restrict__ M, const int *__restrict__ pw_begin,
-                            const int *__restrict__ pw_src, const int *__restrict__ pw_ind,
-                            const double2 *__restrict__ W, double2 *__restrict__ L, int nd, int nexp) {
-  const int ic = blockIdx.x, ind = blockIdx.y;
-  const int j0 = pw_begin[ic], j1 = pw_begin[ic + 1];
-  for (int e = blockIdx.z * blockDim.x + threadIdx.x; e < nexp; e += gridDim.z * blockDim.x) {
-    double2 s = M[((size_t)ic * nd + ind) * nexp + e];
-    for (int j = j0; j < j1; j++) {
-      const double2 m = M[((size_t)pw_src[j] * nd + ind) * nexp + e];
-      const double2 w = W[(size_t)pw_ind[j] * nexp + e];
-      s.x += m.x * w.x - m.y * w.y;
-      s.y += m.x * w.y + m.y * w.x;
-    }
-    L[((size_t)ic * nd + ind) * nexp + e] = s;
-  }
+  __shared__ int s_last;
+  finish_cutoff_box(a.red, blockIdx.x, nd, a.nexp, &s_last);
 }
 
 struct EvalArgs {
@@ -497,6 +490,57 @@ int alloc_bytes(void **p, size_t bytes, std::string &msg) {
 
 }  // namespace
 
+// Groups of at most 32 chunks per cutoff box for the fixed-order reduction
+// done at the end of the form kernels (fgt_common.cuh).
+int build_reduce_groups(DevicePlan &dp, const std::vector<int> &cut_of_chunk, std::string &msg) {
+  const void *old[] = {dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups};
+  for (const void *p : old)
+    if (p) cudaFree(const_cast<void *>(p));
+  dp.G = nullptr;
+  dp.gcnt = dp.bcnt = dp.chunk_group = dp.box_groups = nullptr;
+  dp.groups = nullptr;
+  const int nch = (int)cut_of_chunk.size();
+  std::vector<int> chunk_group(std::max(nch, 1), 0), box_groups(dp.ncut + 1, 0);
+  std::vector<int4> groups;
+  int c = 0;
+  for (int ic = 0; ic < dp.ncut; ic++) {
+    box_groups[ic] = (int)groups.size();
+    int c1 = c;
+    while (c1 < nch && cut_of_chunk[c1] == ic) c1++;
+    for (int g0 = c; g0 < c1; g0 += 32) {
+      const int g1 = std::min(g0 + 32, c1);
+      for (int q = g0; q < g1; q++) chunk_group[q] = (int)groups.size();
+      groups.push_back(make_int4(g0, g1, ic, 0));
+    }
+    c = c1;
+  }
+  box_groups[dp.ncut] = (int)groups.size();
+  if (c != nch) {
+    msg = "chunks are not sorted by cutoff box";
+    return BFGT_ERR_TREE;
+  }
+  bool multi = false;
+  for (int ic = 0; ic < dp.ncut; ic++) multi = multi || (box_groups[ic + 1] - box_groups[ic] > 1);
+  dp.ngroups = (int)groups.size();
+  dp.multi_group = multi;
+  int rc = BFGT_OK;
+  auto chk = [&](int r) {
+    if (rc == BFGT_OK && r != BFGT_OK) rc = r;
+  };
+  std::vector<int> zg(std::max(dp.ngroups, 1), 0), zb(std::max(dp.ncut, 1), 0);
+  chk(upload(dp.chunk_group, chunk_group, msg));
+  chk(upload(dp.groups, groups, msg));
+  chk(upload(dp.box_groups, box_groups, msg));
+  chk(upload(dp.gcnt, zg, msg));
+  chk(upload(dp.bcnt, zb, msg));
+  if (multi) chk(alloc_bytes((void **)&dp.G, sizeof(double2) * (size_t)dp.nd * dp.nexp * dp.ngroups, msg));
+  return rc;
+}
+
+ReduceArgs reduce_args(const DevicePlan &dp) {
+  return ReduceArgs{dp.Mpart, dp.G, dp.M, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups};
+}
+
 int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -551,6 +595,12 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     chk(alloc_bytes((void **)&dp.Mpart, ex * dp.nchunks, msg));
     chk(alloc_bytes((void **)&dp.M, ex * dp.ncut, msg));
     chk(alloc_bytes((void **)&dp.L, ex * dp.ncut, msg));
+    if (rc == BFGT_OK) cudaMemset(dp.M, 0, ex * dp.ncut);  // boxes without PW leaves keep zero
+    {
+      std::vector<int> cut_of_chunk(hp.chunks.size());
+      for (size_t c = 0; c < hp.chunks.size(); c++) cut_of_chunk[c] = hp.chunks[c].icut;
+      chk(build_reduce_groups(dp, cut_of_chunk, msg));
+    }
     const int npb = n * n;
     dp.smem_form = sizeof(double2) * ((size_t)n * dp.npw + (size_t)dp.npw * dp.hh +
                                       (size_t)kWarps * ((size_t)n * dp.hh + dp.npw + dp.hh + (npb + 1) / 2));
@@ -580,7 +630,8 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     chk(upload(dp.ind_loc, hp.ind_loc, msg));
     dp.smem_near = sizeof(double) * (size_t)kWarps * 3 * n * n;
   }
-  const size_t smax = 227 * 1024;
+  // the 227 KB per-block limit minus room for the kernels' static shared variables
+  const size_t smax = 227 * 1024 - 1024;
   if (rc == BFGT_OK && (dp.smem_form > smax || dp.smem_eval > smax || dp.smem_near > smax)) {
     msg = "npw/norder need more than 227 KB of shared memory per block";
     rc = BFGT_ERR_CAPACITY;
@@ -603,7 +654,7 @@ void device_plan_destroy(DevicePlan &dp) {
   if (dp.graph) cudaGraphDestroy(dp.graph);
   split_plan_destroy(dp);
   void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.columns, dp.cut_chunk_begin, dp.cut_pw_begin,
-                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.Mpart, dp.M, dp.L, dp.nf_target, dp.nf_level,
+                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.Mpart, dp.M, dp.L, dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups, dp.nf_target, dp.nf_level,
                   dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.d_stage_f, dp.d_stage_p};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -654,20 +705,24 @@ int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cu
     if (dp.precision == BFGT_PREC_SPLIT) {
       split_form(dp, d_fvals, s);
     } else {
-      FormArgs fa{d_fvals, dp.leaves, dp.columns, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
+      FormArgs fa{d_fvals, dp.leaves, dp.columns, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, reduce_args(dp),
+                  dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
       launch_form_fp64(TileChoice{dp.form_tile[0], dp.form_tile[1], dp.form_tile[2]}, dp.nchunks, dp.smem_form, s, fa);
     }
+    // the merge to the cutoff level finishes inside the form kernels
     if (ev) cudaEventRecord(ev[1], s);
-    const int zb = (dp.nexp + 255) / 256;
-    k_reduce<<<dim3(dp.ncut, dp.nd, zb), 256, 0, s>>>(dp.Mpart, dp.cut_chunk_begin, dp.M, dp.nd, dp.nexp);
     if (ev) cudaEventRecord(ev[2], s);
-    k_translate<<<dim3(dp.ncut, dp.nd, zb), 256, 0, s>>>(dp.M, dp.cut_pw_begin, dp.cut_pw_src, dp.cut_pw_ind,
-                                                         dp.W, dp.L, dp.nd, dp.nexp);
+    {
+      const size_t tot = (size_t)dp.ncut * dp.nd * dp.nexp;
+      k_translate<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(dp.M, dp.cut_pw_begin, dp.cut_pw_src, dp.cut_pw_ind,
+                                                                 dp.W, dp.L, dp.ncut, dp.nd, dp.nexp);
+    }
     if (ev) cudaEventRecord(ev[3], s);
     if (dp.precision == BFGT_PREC_SPLIT) {
       split_eval(dp, d_pot, s);
     } else {
-      EvalArgs ea{d_pot, dp.leaves, dp.columns, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
+      EvalArgs ea{d_pot, dp.leaves, dp.columns, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n,
+                  dp.npw, dp.hh, dp.nexp};
       launch_eval_fp64(TileChoice{dp.eval_tile[0], dp.eval_tile[1], dp.eval_tile[2]}, dp.nchunks, dp.smem_eval, s, ea);
     }
     if (ev) cudaEventRecord(ev[4], s);

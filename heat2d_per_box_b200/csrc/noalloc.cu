@@ -6,17 +6,18 @@
 // reserves its pools at start-up), must not have the library allocate during
 // the stepping loop.  bfgt_plan_execute_noalloc runs the same kernels as
 // bfgt_plan_execute, but takes the plane-wave scratch it needs (the partial
-// expansions of every chunk of leaves and the expansions of the cutoff boxes)
-// from one file-scope device array of fixed size instead of the plan's own
-// buffers.  It calls no allocating routine.
+// expansions of every chunk of leaves, their group sums and the expansions of
+// the cutoff boxes) from one file-scope device array of fixed size instead of
+// the plan's own buffers.  It calls no allocating routine.
 //
 // The array holds kNoallocScratchBytes on every GPU that loads this library,
 // until the process exits.  On the first call on a device this file resolves
 // the array's device address with cudaGetSymbolAddress (with that device
 // current); make that first call before any stream capture.  Every call shares
 // the array: calls that overlap on the GPU (other streams, other threads)
-// race on it.  Each call writes every element it later reads, so nothing has
-// to be cleared between calls.
+// race on it.  Each call writes every element it later reads, except the
+// expansions of cutoff boxes that hold no plane-wave leaf, which no kernel
+// reads; nothing has to be cleared between calls.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -64,7 +65,8 @@ extern "C" int bfgt_noalloc_scratch_bytes(size_t *bytes) {
 extern "C" int bfgt_plan_noalloc_need(bfgt_plan plan, size_t *bytes) {
   if (!plan || !bytes) return BFGT_ERR_ARG;
   const bfgt::DevicePlan &dp = plan->dp;
-  *bytes = sizeof(double2) * (size_t)dp.nd * dp.nexp * ((size_t)dp.nchunks + 2 * (size_t)dp.ncut);
+  *bytes = sizeof(double2) * (size_t)dp.nd * dp.nexp *
+           ((size_t)dp.nchunks + 2 * (size_t)dp.ncut + (dp.multi_group ? (size_t)dp.ngroups : 0));
   return BFGT_OK;
 }
 
@@ -102,6 +104,7 @@ extern "C" int bfgt_plan_execute_noalloc(bfgt_plan plan, const double *d_fvals, 
   view.Mpart = sc;
   view.M = sc + ex * (size_t)dp.nchunks;
   view.L = view.M + ex * (size_t)dp.ncut;
+  view.G = dp.multi_group ? view.L + ex * (size_t)dp.ncut : nullptr;
   rc = bfgt::device_plan_execute(view, d_fvals, d_pot, (cudaStream_t)stream, msg);
   if (rc != BFGT_OK) return bfgt_record_error(rc, msg.c_str());
   bfgt_record_error(BFGT_OK, "");

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/bfgt.h"
+#include "fgt_common.cuh"
 #include "split_kernels.cuh"
 #include "tc_sm100.cuh"
 
@@ -32,6 +33,9 @@ namespace {
 constexpr int kThreads = 128;
 constexpr int kRows = 128;                // MMA M
 constexpr uint32_t kWaitIters = 1u << 26;  // bounded spin on an mbarrier
+// dynamic shared memory opt-in: the 227 KB per-block limit minus room for the
+// kernels' static shared variables
+constexpr int kMaxDynSmem = 227 * 1024 - 1024;
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -50,6 +54,7 @@ struct FormTcArgs {
   const double2 *PH;
   const long long *ph_off;
   double2 *Mpart;
+  ReduceArgs red;
   int *err;
   int nd, n, npw, hh, nexp, cpc, NP, KA;
   uint32_t wait_iters;
@@ -64,20 +69,19 @@ __device__ __forceinline__ void copy_tile(unsigned char *dst, const uint16_t *sr
 
 template <int NT>
 __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
-  extern __shared__ __align__(1024) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);  // [0],[1] operand buffers, [2] drain
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 64);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int4 ch = a.chunks[blockIdx.x];
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, NP = a.NP, KA = a.KA;
   const int ncol = ch.y - ch.x;
   const int abytes = 3 * kRows * KA * 2, bbytes = 3 * NP * KA * 2, bufbytes = abytes + bbytes;
   const int ybytes = kRows * hh * 16;
-  const int ubytes = ((std::max(2 * bufbytes, ybytes) + 1023) / 1024) * 1024;
-  unsigned char *U = smem + 1024;
+  const int ubytes = ((std::max(2 * bufbytes, ybytes) + 127) / 128) * 128;
+  unsigned char *U = smem + 128;
   double2 *sY = reinterpret_cast<double2 *>(U);  // after the tensor-core loop: [row][k2]
   double2 *sT = reinterpret_cast<double2 *>(U + ubytes);  // [m][k] n x npw
-  double2 *sphx = sT + (size_t)n * npw;                    // [slot][k] conj(phase_ox)
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, 128);
   if (tid == 0) {
@@ -92,11 +96,6 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
     sT[m * npw + k] = Tg[i];
   }
   const long long phoff = a.ph_off[ch.w];
-  for (int i = tid; i < ncol * npw; i += kThreads) {
-    const int slot = i / npw, k = i - slot * npw;
-    const double2 p = a.PH[phoff + (size_t)a.columns[ch.x + slot].z * npw + k];
-    sphx[i] = make_double2(p.x, -p.y);
-  }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
@@ -230,8 +229,12 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
           for (int j = 0; j < 4; j++) acc[i][j] = make_double2(0, 0);
         for (int slot = 0; slot < ncol; slot++) {
           double2 ph[2];
+          const double2 *phs = a.PH + phoff + (size_t)a.columns[ch.x + slot].z * npw;
 #pragma unroll
-          for (int i = 0; i < 2; i++) ph[i] = (k1b + i < npw) ? sphx[slot * npw + k1b + i] : make_double2(0, 0);
+          for (int i = 0; i < 2; i++) {
+            const double2 p = (k1b + i < npw) ? phs[k1b + i] : make_double2(0, 0);
+            ph[i] = make_double2(p.x, -p.y);
+          }
           for (int m1 = 0; m1 < n; m1++) {
             double2 av[2], bv[4];
 #pragma unroll
@@ -264,6 +267,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tmem, 128);
+  finish_cutoff_box(a.red, blockIdx.x, nd, a.nexp, reinterpret_cast<int *>(smem + 68));
 }
 
 struct EvalTcArgs {
@@ -285,7 +289,7 @@ struct EvalTcArgs {
 };
 
 __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
-  extern __shared__ __align__(1024) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 64);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -293,9 +297,9 @@ __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, NB = a.NB, KE = a.KE, KH = a.KH;
   const int ncol = ch.y - ch.x;
   const int abytes = 3 * kRows * KE * 2, bbytes = 3 * NB * KE * 2;
-  unsigned char *sA = smem + 1024;
-  unsigned char *sB = sA + ((abytes + 1023) / 1024) * 1024;  // two buffers
-  double2 *sL = reinterpret_cast<double2 *>(sB + ((2 * bbytes + 1023) / 1024) * 1024);  // [m1][m2]
+  unsigned char *sA = smem + 128;
+  unsigned char *sB = sA + ((abytes + 127) / 128) * 128;  // two buffers
+  double2 *sL = reinterpret_cast<double2 *>(sB + ((2 * bbytes + 127) / 128) * 128);  // [m1][m2]
   double2 *sE = sL + (size_t)npw * hh;                                                    // [m1][k1]
   double2 *sph = sE + (size_t)npw * n;                                                    // [slot][m1]
   (void)lane;
@@ -531,7 +535,6 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   // chunks of up to cpc columns of one (icut, level), and their oy steps
   std::vector<int4> chunks;
   std::vector<int> step_begin(1, 0), steps;
-  std::vector<int> cut_chunk_begin(hp.cut_box.size() + 1, 0);
   const std::vector<Column> &cols = hp.columns;
   for (size_t c = 0; c < cols.size();) {
     size_t e = c;
@@ -557,14 +560,6 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     }
     step_begin.push_back((int)(steps.size() / (1 + sp.cpc)));
     c = e;
-  }
-  {
-    size_t c = 0;
-    for (size_t ic = 0; ic < hp.cut_box.size(); ic++) {
-      cut_chunk_begin[ic] = (int)c;
-      while (c < chunks.size() && chunks[c].z == (int)ic) c++;
-    }
-    cut_chunk_begin[hp.cut_box.size()] = (int)c;
   }
   // per (level, offset) operand tables
   const long long tyt = 3LL * sp.NP * sp.KA, eyt = 3LL * sp.NB * sp.KE;
@@ -637,17 +632,21 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     msg = "cudaMalloc failed (split partial expansions)";
     return BFGT_ERR_OOM;
   }
-  if (dp.cut_chunk_begin) cudaFree(dp.cut_chunk_begin);
-  chk(upload_vec(dp.cut_chunk_begin, cut_chunk_begin, msg));
+  {
+    std::vector<int> cut_of_chunk(chunks.size());
+    for (size_t c = 0; c < chunks.size(); c++) cut_of_chunk[c] = chunks[c].z;
+    dp.nchunks = (int)chunks.size();
+    chk(build_reduce_groups(dp, cut_of_chunk, msg));
+  }
   dp.nchunks = (int)chunks.size();
   // shared memory
   {
     const int abytes = 3 * kRows * sp.KA * 2, bbytes = 3 * sp.NP * sp.KA * 2;
     const int ybytes = kRows * hh * 16;
-    const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 1023) / 1024) * 1024;
-    sp.smem_form = 1024 + ubytes + sizeof(double2) * ((size_t)n * npw + (size_t)sp.cpc * npw);
+    const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 127) / 128) * 128;
+    sp.smem_form = 128 + ubytes + sizeof(double2) * (size_t)n * npw;
     const int eab = 3 * kRows * sp.KE * 2, ebb = 3 * sp.NB * sp.KE * 2;
-    sp.smem_eval = 1024 + ((eab + 1023) / 1024) * 1024 + ((2 * ebb + 1023) / 1024) * 1024 +
+    sp.smem_eval = 128 + ((eab + 127) / 128) * 128 + ((2 * ebb + 127) / 128) * 128 +
                    sizeof(double2) * ((size_t)npw * hh + (size_t)npw * n + (size_t)sp.cpc * npw);
   }
   const int ntiles = ((npw + 1) / 2) * ((hh + 3) / 4);
@@ -656,13 +655,13 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     msg = "split precision: x-contraction tile count exceeds the built kernels";
     return BFGT_ERR_CAPACITY;
   }
-  if (sp.smem_form > 227 * 1024 || sp.smem_eval > 227 * 1024) {
+  if (sp.smem_form > (size_t)kMaxDynSmem || sp.smem_eval > (size_t)kMaxDynSmem) {
     msg = "split precision: shared memory need exceeds 227 KB";
     return BFGT_ERR_CAPACITY;
   }
-  cudaFuncSetAttribute(k_form_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  cudaFuncSetAttribute(k_form_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  cudaFuncSetAttribute(k_eval_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaFuncSetAttribute(k_form_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_form_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_eval_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
   sp.wait_iters = kWaitIters;
   // tensor-core FLOP issued per transform (every slice product counted)
   const double nsteps_total = (double)(steps.size() / (1 + sp.cpc));
@@ -682,8 +681,8 @@ void split_plan_destroy(DevicePlan &dp) {
 void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
   SplitPlan &sp = dp.split;
   FormTcArgs a{d_fvals, sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.TyB, sp.tyb_off, sp.tyb_tile, dp.T,
-               dp.PH, dp.ph_off, dp.Mpart, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NP, sp.KA,
-               sp.wait_iters};
+               dp.PH, dp.ph_off, dp.Mpart, reduce_args(dp), sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc,
+               sp.NP, sp.KA, sp.wait_iters};
   if (sp.nt == 1) k_form_tc<1><<<sp.nchunks, kThreads, sp.smem_form, s>>>(a);
   else k_form_tc<2><<<sp.nchunks, kThreads, sp.smem_form, s>>>(a);
 }

@@ -5,8 +5,11 @@
 #include <string>
 
 #include "device_plan.hpp"
+#include "fgt_common.cuh"
 
 namespace bfgt {
+
+ReduceArgs reduce_args(const DevicePlan &dp);
 
 // Uploads the FP16 operand slices of the level tables; BFGT_* status.
 int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);

@@ -8,7 +8,8 @@
 //   eval:  D[(slot,k1), k2] = [Hr|Hi](k1,(re/im,m2)) * [Eyr;-Eyi]((re/im,m2),k2)
 // where Ty_oy = T conj(phase_oy) and Ey_oy = w E phase_oy are per-offset tables
 // precomputed in FP64 on the host.  Every operand is split into three BF16
-// slices (x = s0 + s1 + s2, ~2^-24 relative); the six slice products with
+// slices (x = s0 + s1 + s2: the tables exactly to ~2^-27 relative, the leaf
+// values and H through FP32, to 2^-24); the six slice products with
 // i+j <= 2 are accumulated in FP32 in tensor memory, the leading product s0*s0
 // in its own accumulator and the five correction products in a second one,
 // and the two are summed in FP64.  The once-per-column contractions (x
@@ -148,9 +149,9 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         if (h >= KA / 8) break;
-        uint16_t s0[8], s1[8], s2[8];
+        uint32_t s0[4], s1[4], s2[4];
 #pragma unroll
-        for (int q = 0; q < 8; q++) tc::split3_bf16(fcur[8 * h + q], s0[q], s1[q], s2[q]);
+        for (int q = 0; q < 4; q++) tc::split3_bf16x2(fcur[8 * h + 2 * q], fcur[8 * h + 2 * q + 1], s0[q], s1[q], s2[q]);
         const uint32_t off = tc::kmajor_off(r, 8 * h, kRows);
         *reinterpret_cast<uint4 *>(Ab + off) = *reinterpret_cast<uint4 *>(s0);
         *reinterpret_cast<uint4 *>(Ab + kRows * KA * 2 + off) = *reinterpret_cast<uint4 *>(s1);
@@ -386,11 +387,12 @@ __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
             }
           }
         }
-        uint16_t re0[8], re1[8], re2[8], im0[8], im1[8], im2[8];
+        uint32_t re0[4], re1[4], re2[4], im0[4], im1[4], im2[4];
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-          tc::split3_bf16((mb + j < hh) ? acc[j].x : 0.0, re0[j], re1[j], re2[j]);
-          tc::split3_bf16((mb + j < hh) ? acc[j].y : 0.0, im0[j], im1[j], im2[j]);
+        for (int j = 0; j < 4; j++) {
+          const bool v0 = mb + 2 * j < hh, v1 = mb + 2 * j + 1 < hh;
+          tc::split3_bf16x2(v0 ? acc[2 * j].x : 0.0, v1 ? acc[2 * j + 1].x : 0.0, re0[j], re1[j], re2[j]);
+          tc::split3_bf16x2(v0 ? acc[2 * j].y : 0.0, v1 ? acc[2 * j + 1].y : 0.0, im0[j], im1[j], im2[j]);
         }
         const uint32_t ore = tc::kmajor_off(r, mb, kRows), oim = tc::kmajor_off(r, KH + mb, kRows);
         *reinterpret_cast<uint4 *>(sA + ore) = *reinterpret_cast<uint4 *>(re0);

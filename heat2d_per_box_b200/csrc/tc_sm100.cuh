@@ -102,16 +102,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint3
   return false;
 }
 
-// FP64 value -> three BF16 slices whose sum reproduces it to ~2^-24 relative
-__device__ __forceinline__ void split3_bf16(double v, uint16_t &s0, uint16_t &s1, uint16_t &s2) {
-  const __nv_bfloat16 a = __double2bfloat16(v);
-  const double r1 = v - (double)__bfloat162float(a);
-  const __nv_bfloat16 b = __double2bfloat16(r1);
-  const double r2 = r1 - (double)__bfloat162float(b);
-  const __nv_bfloat16 c = __double2bfloat16(r2);
-  s0 = __bfloat16_as_ushort(a);
-  s1 = __bfloat16_as_ushort(b);
-  s2 = __bfloat16_as_ushort(c);
+__device__ __forceinline__ uint32_t bf162_bits(__nv_bfloat162 h) { return *reinterpret_cast<uint32_t *>(&h); }
+
+// Two FP64 values -> three packed BF16x2 slices.  The values are rounded to
+// FP32 first (relative error 2^-24); the FP32 value is then split exactly:
+// each difference below is exact in FP32 (the operands agree in their leading
+// bits), and the last remainder has at most 6 significant bits, so
+// s0 + s1 + s2 reproduces the FP32 value.  Element v0 goes to the low half
+// (the lower address of a packed pair).
+__device__ __forceinline__ void split3_bf16x2(double v0, double v1, uint32_t &p0, uint32_t &p1, uint32_t &p2) {
+  const float a0 = __double2float_rn(v0), a1 = __double2float_rn(v1);
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a0, a1);
+  const float2 hf = __bfloat1622float2(h);
+  const float r0 = a0 - hf.x, r1 = a1 - hf.y;
+  const __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
+  const float2 mf = __bfloat1622float2(m);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
+  p0 = bf162_bits(h);
+  p1 = bf162_bits(m);
+  p2 = bf162_bits(l);
 }
 
 }  // namespace tc

@@ -84,6 +84,8 @@ def lib():
     L.bfgt_plan_noalloc_need.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
     L.bfgt_plan_check.restype = C.c_int
     L.bfgt_plan_check.argtypes = [C.c_void_p]
+    L.bfgt_plan_set_wait_limit.restype = C.c_int
+    L.bfgt_plan_set_wait_limit.argtypes = [C.c_void_p, C.c_uint]
     L.bfgt_plan_destroy.restype = C.c_int
     L.bfgt_plan_destroy.argtypes = [C.c_void_p]
     L.bfgt_host_plan_dump.restype = C.c_int

@@ -108,6 +108,10 @@ class Plan:
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         _lib.check(self._L.bfgt_plan_graph_launch(self._h, s))
 
+    def set_wait_limit(self, polls=None):
+        """Poll limit of the bounded device waits (None restores the default)."""
+        _lib.check(self._L.bfgt_plan_set_wait_limit(self._h, 0xFFFFFFFF if polls is None else int(polls)))
+
     def check(self):
         """Waits for the device; raises BfgtError if a bounded device wait timed out."""
         _lib.check(self._L.bfgt_plan_check(self._h))
@@ -125,14 +129,15 @@ class Plan:
         out = np.zeros(16, np.int32)
         _lib.check(self._L.bfgt_plan_info(self._h, out))
         keys = ["npwlevel", "npw", "nlevstart", "nlevend", "regime", "nleafbox", "npwleaves", "nnear_targets",
-                "nnear_pairs", "mnlist1", "iperiod_int", "nchunks"]
+                "nnear_pairs", "mnlist1", "iperiod_int", "nchunks", "launches"]
         return {k: int(out[i]) for i, k in enumerate(keys)}
 
     def work(self):
         out = np.zeros(16)
         _lib.check(self._L.bfgt_plan_work(self._h, out))
         keys = ["flops", "bytes", "tc_flops", "points", "flops_form", "flops_eval", "flops_near", "flops_translate",
-                "bytes_form", "bytes_eval", "bytes_near", "tc_flops_form", "tc_flops_eval"]
+                "bytes_form", "bytes_eval", "bytes_near", "tc_flops_form", "tc_flops_eval", "host_h2d_bytes",
+                "host_d2h_bytes"]
         return {k: float(out[i]) for i, k in enumerate(keys)}
 
     def close(self):

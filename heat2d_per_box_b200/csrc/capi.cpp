@@ -82,6 +82,14 @@ int bfgt_plan_create(bfgt_plan *plan, int nd, double delta, double eps, int ipol
   try {
     bfgt::TreeView t = make_view(nboxes, nlevels, ltree, itree, iptr, centers, boxsize);
     bfgt::build_host_plan(p->hp, t, nd, delta, eps, ipoly, iperiod, norder, precision);
+    constexpr int kMaxGap = 64;  // non-leaf boxes copied rather than starting a new run
+    for (int b = 1; b <= nboxes; b++) {
+      if (t.nchild(b) != 0) continue;
+      if (!p->leaf_runs.empty() && b - 1 - p->leaf_runs.back().second <= kMaxGap)
+        p->leaf_runs.back().second = b;
+      else
+        p->leaf_runs.emplace_back(b - 1, b);
+    }
   } catch (const std::exception &e) {
     return fail(BFGT_ERR_TREE, e.what());
   }
@@ -124,14 +132,22 @@ int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, voi
     }
     dp.stage_elems = elems;
   }
-  if (cudaMemcpyAsync(dp.d_stage_f, fvals, elems * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(dp.d_stage_p, pot, elems * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
+  // only the leaf boxes are read (fvals) and accumulated into (pot)
+  const size_t per = (size_t)dp.nd * dp.n * dp.n;
+  for (const auto &r : plan->leaf_runs) {
+    const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
+    if (cudaMemcpyAsync(dp.d_stage_f + o, fvals + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dp.d_stage_p + o, pot + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
+  }
   std::string msg;
   int rc = bfgt::device_plan_execute(dp, dp.d_stage_f, dp.d_stage_p, s, msg);
   if (rc != BFGT_OK) return fail(rc, msg);
-  if (cudaMemcpyAsync(pot, dp.d_stage_p, elems * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
-    return fail(BFGT_ERR_CUDA, "device-to-host copy failed");
+  for (const auto &r : plan->leaf_runs) {
+    const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
+    if (cudaMemcpyAsync(pot + o, dp.d_stage_p + o, c, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      return fail(BFGT_ERR_CUDA, "device-to-host copy failed");
+  }
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(BFGT_ERR_CUDA, std::string("transform failed: ") + cudaGetErrorString(cudaGetLastError()));
   return BFGT_OK;
 }
@@ -207,7 +223,8 @@ int bfgt_plan_info(bfgt_plan plan, int *out) {
   out[8] = (int)h.nf_src.size();
   out[9] = h.mnlist1;
   out[10] = h.iperiod_int;
-  out[11] = (int)h.chunks.size();
+  out[11] = plan->dp.nchunks;
+  out[12] = (!plan->dp.direct_only && plan->dp.nchunks > 0 ? 3 : 0) + (plan->dp.nnf > 0 ? 1 : 0);
   return BFGT_OK;
 }
 
@@ -228,6 +245,10 @@ int bfgt_plan_work(bfgt_plan plan, double *out) {
   out[11] = plan->dp.split.tc_flops_form;
   out[12] = plan->dp.split.tc_flops_eval;
   out[2] = out[11] + out[12];
+  double run_bytes = 0;
+  for (const auto &r : plan->leaf_runs) run_bytes += 8.0 * plan->dp.nd * plan->dp.n * plan->dp.n * (r.second - r.first);
+  out[13] = 2 * run_bytes;  // bfgt_plan_execute_host: fvals and pot up
+  out[14] = run_bytes;      // and pot down
   return BFGT_OK;
 }
 
@@ -238,6 +259,13 @@ int bfgt_plan_check(bfgt_plan plan) {
   int rc = bfgt::split_check(plan->dp);
   if (rc == BFGT_ERR_TIMEOUT) return fail(rc, "a bounded device-side wait gave up (tensor-core pipeline)");
   if (rc != BFGT_OK) return fail(rc, "error flag read-out failed");
+  return BFGT_OK;
+}
+
+int bfgt_plan_set_wait_limit(bfgt_plan plan, unsigned int polls) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  plan->dp.split.wait_iters = polls == 0xFFFFFFFFu ? bfgt::split_default_wait_iters() : polls;
   return BFGT_OK;
 }
 

@@ -3,8 +3,16 @@
 #include "device_plan.hpp"
 #include "host_plan.hpp"
 
+#include <utility>
+#include <vector>
+
 struct bfgt_plan_s {
   bfgt::HostPlan hp;
   bfgt::DevicePlan dp;
   double stage_ms[8] = {0};
+  // [first, last) 0-based box ranges that hold every leaf box; the host-array
+  // entry point moves only these (runs separated by a few non-leaf boxes are
+  // merged, so a range may include some non-leaf boxes, which the transform
+  // neither reads nor writes)
+  std::vector<std::pair<int, int>> leaf_runs;
 };

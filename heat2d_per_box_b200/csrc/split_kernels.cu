@@ -697,6 +697,8 @@ void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
   k_eval_tc<<<sp.nchunks, kThreads, sp.smem_eval, s>>>(a);
 }
 
+unsigned int split_default_wait_iters() { return kWaitIters; }
+
 int split_check(DevicePlan &dp) {
   if (!dp.split.err) return BFGT_OK;
   int h[4] = {0, 0, 0, 0};

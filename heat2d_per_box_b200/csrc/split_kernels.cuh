@@ -11,7 +11,7 @@ namespace bfgt {
 
 ReduceArgs reduce_args(const DevicePlan &dp);
 
-// Uploads the FP16 operand slices of the level tables; BFGT_* status.
+// Uploads the BF16 operand slices of the level tables; BFGT_* status.
 int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);
 // leaf values -> partial cutoff expansions (same output as k_form_fp64)
 void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s);
@@ -21,5 +21,7 @@ void split_plan_destroy(DevicePlan &dp);
 // Reads and clears the device error flag of the tensor-core kernels (waits
 // for the device); BFGT_ERR_TIMEOUT if a bounded wait gave up.
 int split_check(DevicePlan &dp);
+// Poll limit of every bounded mbarrier wait unless a plan sets its own.
+unsigned int split_default_wait_iters();
 
 }  // namespace bfgt

@@ -124,8 +124,9 @@ int bfgt_plan_reserve_events(bfgt_plan plan, int n);
    out[3]=nlevend, out[4]=regime (0 periodic Fourier, 1 PW + near field,
    2 near field only), out[5]=nleafbox, out[6]=number of PW leaves,
    out[7]=number of near-field target leaves, out[8]=number of near-field
-   interactions, out[9]=mnlist1, out[10]=internal iperiod, out[11]=nchunks.
-   out must hold 16 ints. */
+   interactions, out[9]=mnlist1, out[10]=internal iperiod, out[11]=number of
+   plane-wave chunks (CTAs of the form and eval kernels), out[12]=kernel
+   launches per execute.  out must hold 16 ints. */
 int bfgt_plan_info(bfgt_plan plan, int *out);
 
 /* Algorithmic work of one execute (every real operation counted once, split
@@ -134,7 +135,8 @@ int bfgt_plan_info(bfgt_plan plan, int *out);
    slice product counted), out[3]=leaf points x nd, out[4..7]=FLOP of the form,
    eval, near-field and translation stages, out[8..10]=compulsory bytes of the
    form, eval and near-field stages, out[11..12]=tensor-core FLOP issued by the
-   form and eval stages.  out must hold 16. */
+   form and eval stages, out[13..14]=bytes bfgt_plan_execute_host moves host to
+   device and device to host (leaf boxes only).  out must hold 16. */
 int bfgt_plan_work(bfgt_plan plan, double *out);
 
 /* Waits for the device and reports failures of earlier executes on this plan:
@@ -142,6 +144,15 @@ int bfgt_plan_work(bfgt_plan plan, double *out);
    gave up (the results of that execute are not valid), BFGT_ERR_CUDA on a
    device error.  Clears the flag. */
 int bfgt_plan_check(bfgt_plan plan);
+
+/* No counterpart in the reference.  Sets the poll limit of the bounded
+   device-side waits of this plan's tensor-core kernels (default 2^26 polls,
+   restored by passing 0xFFFFFFFF).  A wait that reaches the limit makes the
+   kernel stop issuing tensor-core work, drain what is in flight, free its
+   tensor memory and return; bfgt_plan_check then reports BFGT_ERR_TIMEOUT and
+   that execute's result is invalid.  A limit of 0 makes every such wait give
+   up at once (used to test the error path).  No effect on FP64 plans. */
+int bfgt_plan_set_wait_limit(bfgt_plan plan, unsigned int polls);
 
 int bfgt_plan_destroy(bfgt_plan plan);
 

@@ -83,3 +83,30 @@ def test_split_deterministic(trees):
     a, _ = run_split(t, 1e-4, 1e-6)
     b, _ = run_split(t, 1e-4, 1e-6)
     np.testing.assert_array_equal(a, b)
+
+
+def test_bounded_wait_expiry_reports_timeout_and_context_survives(trees):
+    """A wait limit of 0 makes every tensor-core pipeline wait give up at once:
+    the kernels stop issuing, drain, free tensor memory and return; check()
+    reports BFGT_ERR_TIMEOUT.  The next execute with the default limit on the
+    same plan and context is correct."""
+    import torch
+    t = trees["ad16_leg_per"]
+    delta, eps = 1e-4, 1e-6
+    plan = hb.Plan(t, delta, eps, precision=hb.BFGT_PREC_SPLIT)
+    f = torch.from_numpy(t.fvals.reshape(-1)).cuda()
+    p = torch.zeros_like(f)
+    plan.set_wait_limit(0)
+    plan.execute(f, p)
+    with pytest.raises(hb.BfgtError) as e:
+        plan.check()
+    assert e.value.code == 7
+    plan.set_wait_limit(None)
+    p.zero_()
+    plan.execute(f, p)
+    plan.check()
+    got = p.cpu().numpy()
+    plan.close()
+    ref = oracle.boxfgt(t, t.fvals, delta, eps)
+    lv = t.leaves()
+    assert rel_l2(got.reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv]) < SPLIT_TOL

@@ -61,13 +61,6 @@ struct FormTcArgs {
   uint32_t wait_iters;
 };
 
-// 16-byte copy of a global tile into shared memory
-__device__ __forceinline__ void copy_tile(unsigned char *dst, const uint16_t *src, int bytes) {
-  const uint4 *s = reinterpret_cast<const uint4 *>(src);
-  uint4 *d = reinterpret_cast<uint4 *>(dst);
-  for (int i = threadIdx.x; i < bytes / 16; i += blockDim.x) d[i] = s[i];
-}
-
 template <int NT>
 __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -289,96 +282,96 @@ struct EvalTcArgs {
   uint32_t wait_iters;
 };
 
-__global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
+// Steps of a chunk per tensor-core group in the eval kernel: the group's B
+// operand is the step tiles side by side, N = 16 x steps <= 128.
+constexpr int kEvalBatch = 8;
+constexpr int kEvalThreads = 256;
+
+// Cutoff expansions -> leaf values (steps 4+5).  One CTA of 8 warps per chunk,
+// two CTAs per SM.  H(k1,m2) = sum_m1 E(m1,k1) phase_ox(m1) L(m1,m2) is formed
+// in FP64 once per chunk and split into the A operand (rows (slot,k1), K =
+// re/im x m2).  The steps are then taken kEvalBatch at a time: their Ey tiles
+// are copied side by side into one B operand (cp.async, issued while the
+// previous group is read out), 18 MMAs with N = 16 x steps produce the values
+// of every leaf of the group, and the readout adds 2 (D0 + D1) into pot.
+// Warps w and w+4 share TMEM lanes 32 (w%4).. and split the group's steps.
+__global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(EvalTcArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);  // [0] MMA group done, [1] drain
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 64);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int4 ch = a.chunks[blockIdx.x];
-  const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, NB = a.NB, KE = a.KE, KH = a.KH;
+  const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, KE = a.KE, KH = a.KH;
   const int ncol = ch.y - ch.x;
-  const int abytes = 3 * kRows * KE * 2, bbytes = 3 * NB * KE * 2;
+  const int abytes = 3 * kRows * KE * 2, bbytes = 3 * (16 * kEvalBatch) * KE * 2;
   unsigned char *sA = smem + 128;
-  unsigned char *sB = sA + ((abytes + 127) / 128) * 128;  // two buffers
-  double2 *sL = reinterpret_cast<double2 *>(sB + ((2 * bbytes + 127) / 128) * 128);  // [m1][m2]
-  double2 *sE = sL + (size_t)npw * hh;                                                    // [m1][k1]
-  double2 *sph = sE + (size_t)npw * n;                                                    // [slot][m1]
-  (void)lane;
+  unsigned char *sB = sA + ((abytes + 127) / 128) * 128;
+  double2 *sL = reinterpret_cast<double2 *>(sB + ((bbytes + 127) / 128) * 128);  // [m1][m2]
+  double2 *sE = sL + (size_t)npw * hh;                                             // [m1][k1]
+  double2 *sph = sE + (size_t)npw * n;                                             // [slot][m1]
 
-  if (warp == 0) tc::tmem_alloc(tmem_slot, 64);
+  if (warp == 0) tc::tmem_alloc(tmem_slot, 256);
   if (tid == 0) {
     tc::mbar_init(&mbar[0], 1);
     tc::mbar_init(&mbar[1], 1);
-    tc::mbar_init(&mbar[2], 1);
     tc::fence_mbar_init();
+  }
+  const int sb = a.step_begin[blockIdx.x], se = a.step_begin[blockIdx.x + 1], nsteps = se - sb;
+  const int stride = 1 + cpc;
+  const uint16_t *eyb = a.EyB + a.eyb_off[ch.w];
+  const int nbatch = (nsteps + kEvalBatch - 1) / kEvalBatch;
+  // Ey tiles of steps [s0, s0+S) -> B rows 16 s .. 16 s + 15 (K-major core layout, N = 16 S)
+  auto load_batch = [&](int s0, int S) {
+    const int N = 16 * S, KG = KE / 8, U = 3 * KG * 16;
+    for (int u = tid; u < U * S; u += kEvalThreads) {
+      const int st = u / U, rem = u - st * U;
+      const int c = rem / (KG * 16), kg = (rem >> 4) % KG, w = rem & 15;
+      const int oy = a.steps[(size_t)(sb + s0 + st) * stride];
+      const unsigned char *src =
+          reinterpret_cast<const unsigned char *>(eyb + (size_t)oy * a.eyb_tile) + c * (16 * KE * 2) + kg * 256 + w * 16;
+      tc::cp_async16(sB + c * (N * KE * 2) + (kg * (N / 8) + 2 * st) * 128 + w * 16, src);
+    }
+    tc::cp_async_commit();
+  };
+  if (nbatch > 0) load_batch(0, min(kEvalBatch, nsteps));
+  // E(m1,k1) of this level and the x phases of the chunk's columns (FP64)
+  for (int i = tid; i < npw * n; i += kEvalThreads) {
+    const int m = i % npw, k = i / npw;
+    sE[m * n + k] = a.E[(size_t)n * npw * ch.w + i];
+  }
+  for (int i = tid; i < ncol * npw; i += kEvalThreads) {
+    const int slot = i / npw, m = i - slot * npw;
+    sph[i] = a.PH[a.ph_off[ch.w] + (size_t)a.columns[ch.x + slot].z * npw + m];
   }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t idesc = tc::idesc_bf16_f32(kRows, NB);
-  const int sb = a.step_begin[blockIdx.x], se = a.step_begin[blockIdx.x + 1], nsteps = se - sb;
-  const int stride = 1 + cpc;
-  const uint16_t *eyb = a.EyB + a.eyb_off[ch.w];
-  // E(m1,k1) of this level and the x phases of the chunk's columns (FP64)
-  for (int i = tid; i < npw * n; i += kThreads) {
-    const int m = i % npw, k = i / npw;
-    sE[m * n + k] = a.E[(size_t)n * npw * ch.w + i];
-  }
-  for (int i = tid; i < ncol * npw; i += kThreads) {
-    const int slot = i / npw, m = i - slot * npw;
-    sph[i] = a.PH[a.ph_off[ch.w] + (size_t)a.columns[ch.x + slot].z * npw + m];
-  }
   bool ok = true;
-  const int r = tid, rslot = r / n, rk1 = r - rslot * n;
-  const uint32_t lanebase = (uint32_t)(32 * warp) << 16;
-
-  // wait for the MMAs of global step g (density ind, step s), add 2 Re(...) into pot
-  auto readout = [&](int ind, int s, int g) {
-    const int b = g & 1;
-    const int *st = a.steps + (size_t)(sb + s) * stride;
-    const int box = st[1 + rslot];
-    double *pb = a.pot + (size_t)(box < 0 ? 0 : box) * nd * npb + ind + (size_t)nd * rk1;
-    double pv[16];
-#pragma unroll
-    for (int k2 = 0; k2 < 16; k2++) pv[k2] = (box >= 0 && k2 < n) ? pb[(size_t)nd * n * k2] : 0.0;
-    if (ok && !tc::mbar_wait(&mbar[b], (g >> 1) & 1, a.wait_iters)) {
-      ok = false;
-      atomicExch(a.err, 1);
-    }
-    tc::fence_after_sync();
-    float v0[16], v1[16];
-    tc::tmem_ld16(tmem + lanebase + (uint32_t)(b * 2 * NB), v0);
-    tc::tmem_ld16(tmem + lanebase + (uint32_t)(b * 2 * NB + NB), v1);
-    tc::tmem_ld_wait();
-    if (ok && box >= 0) {
-#pragma unroll
-      for (int k2 = 0; k2 < 16; k2++)
-        if (k2 < n) pb[(size_t)nd * n * k2] = pv[k2] + 2.0 * ((double)v0[k2] + (double)v1[k2]);
-    }
-    tc::fence_before_sync();
-  };
+  int g = 0;  // MMA groups issued so far (mbarrier phase)
 
   for (int ind = 0; ind < nd; ind++) {
     const double2 *Lg = a.L + ((size_t)ch.z * nd + ind) * a.nexp;
-    for (int e = tid; e < a.nexp; e += kThreads) {
+    for (int e = tid; e < a.nexp; e += kEvalThreads) {
       const int m2 = e / npw, m1 = e - m2 * npw;
       sL[m1 * hh + m2] = Lg[e];
     }
     __syncthreads();
-    // H(k1,m2) = sum_m1 E(m1,k1) phase_ox(m1) L(m1,m2) for row r = (slot, k1), sliced into the A operand
+    // H for row r = (slot, k1), four m2 at a time; the two thread halves take alternate blocks
     {
+      const int r = tid & (kRows - 1), half = tid >> 7, rslot = r / n, rk1 = r - rslot * n;
       const bool live = rslot < ncol;
-      for (int mb = 0; mb < KH; mb += 8) {
-        double2 acc[8];
+      for (int blk = half; blk < KH / 4; blk += 2) {
+        const int mb = 4 * blk;
+        double2 acc[4];
 #pragma unroll
-        for (int j = 0; j < 8; j++) acc[j] = make_double2(0, 0);
-        if (live) {
+        for (int j = 0; j < 4; j++) acc[j] = make_double2(0, 0);
+        if (live && mb < hh) {
 #pragma unroll 2
           for (int m1 = 0; m1 < npw; m1++) {
             const double2 e = zmul(sE[m1 * n + rk1], sph[rslot * npw + m1]);
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
+            for (int j = 0; j < 4; j++) {
               const double2 l = (mb + j < hh) ? sL[m1 * hh + mb + j] : make_double2(0, 0);
               acc[j].x = fma(e.x, l.x, acc[j].x);
               acc[j].x = fma(-e.y, l.y, acc[j].x);
@@ -387,68 +380,43 @@ __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
             }
           }
         }
-        uint32_t re0[4], re1[4], re2[4], im0[4], im1[4], im2[4];
+        uint32_t re[3][2], im[3][2];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const bool v0 = mb + 2 * j < hh, v1 = mb + 2 * j + 1 < hh;
-          tc::split3_bf16x2(v0 ? acc[2 * j].x : 0.0, v1 ? acc[2 * j + 1].x : 0.0, re0[j], re1[j], re2[j]);
-          tc::split3_bf16x2(v0 ? acc[2 * j].y : 0.0, v1 ? acc[2 * j + 1].y : 0.0, im0[j], im1[j], im2[j]);
+        for (int j = 0; j < 2; j++) {
+          tc::split3_bf16x2(acc[2 * j].x, acc[2 * j + 1].x, re[0][j], re[1][j], re[2][j]);
+          tc::split3_bf16x2(acc[2 * j].y, acc[2 * j + 1].y, im[0][j], im[1][j], im[2][j]);
         }
         const uint32_t ore = tc::kmajor_off(r, mb, kRows), oim = tc::kmajor_off(r, KH + mb, kRows);
-        *reinterpret_cast<uint4 *>(sA + ore) = *reinterpret_cast<uint4 *>(re0);
-        *reinterpret_cast<uint4 *>(sA + kRows * KE * 2 + ore) = *reinterpret_cast<uint4 *>(re1);
-        *reinterpret_cast<uint4 *>(sA + 2 * kRows * KE * 2 + ore) = *reinterpret_cast<uint4 *>(re2);
-        *reinterpret_cast<uint4 *>(sA + oim) = *reinterpret_cast<uint4 *>(im0);
-        *reinterpret_cast<uint4 *>(sA + kRows * KE * 2 + oim) = *reinterpret_cast<uint4 *>(im1);
-        *reinterpret_cast<uint4 *>(sA + 2 * kRows * KE * 2 + oim) = *reinterpret_cast<uint4 *>(im2);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          *reinterpret_cast<uint2 *>(sA + c * kRows * KE * 2 + ore) = make_uint2(re[c][0], re[c][1]);
+          *reinterpret_cast<uint2 *>(sA + c * kRows * KE * 2 + oim) = make_uint2(im[c][0], im[c][1]);
+        }
       }
-      for (int k = 2 * KH; k < KE; k += 8) {  // zero K padding
+      for (int k = 2 * KH + 4 * half; k < KE; k += 8) {  // zero K padding
         const uint32_t o = tc::kmajor_off(r, k, kRows);
-        const uint4 z = make_uint4(0, 0, 0, 0);
-        *reinterpret_cast<uint4 *>(sA + o) = z;
-        *reinterpret_cast<uint4 *>(sA + kRows * KE * 2 + o) = z;
-        *reinterpret_cast<uint4 *>(sA + 2 * kRows * KE * 2 + o) = z;
+#pragma unroll
+        for (int c = 0; c < 3; c++) *reinterpret_cast<uint2 *>(sA + c * kRows * KE * 2 + o) = make_uint2(0, 0);
       }
     }
-    const int bpieces = bbytes / 16;
-    constexpr int kMaxPieces = 4;
-    uint4 bnext[kMaxPieces];
-    auto load_tile = [&](int s2) {
-      const int *st2 = a.steps + (size_t)(sb + s2) * stride;
-      const uint4 *src = reinterpret_cast<const uint4 *>(eyb + (size_t)st2[0] * a.eyb_tile);
-#pragma unroll
-      for (int q = 0; q < kMaxPieces; q++) {
-        const int i = tid + kThreads * q;
-        if (i < bpieces) bnext[q] = src[i];
-      }
-    };
-    if (nsteps > 0) load_tile(0);
-    for (int s = 0; s < nsteps; s++) {
-      const int g = ind * nsteps + s, b = g & 1;
-      unsigned char *Bb = sB + b * bbytes;
-      uint4 bcur[kMaxPieces];
-#pragma unroll
-      for (int q = 0; q < kMaxPieces; q++) bcur[q] = bnext[q];
-      if (s + 1 < nsteps) load_tile(s + 1);
-#pragma unroll
-      for (int q = 0; q < kMaxPieces; q++) {
-        const int i = tid + kThreads * q;
-        if (i < bpieces) reinterpret_cast<uint4 *>(Bb)[i] = bcur[q];
-      }
+    for (int j = 0; j < nbatch; j++, g++) {
+      const int s0 = j * kEvalBatch, S = min(kEvalBatch, nsteps - s0), N = 16 * S;
+      tc::cp_async_wait_all();
       tc::fence_async_smem();
       tc::fence_before_sync();
       __syncthreads();
       if (tid == 0 && ok) {
         tc::fence_after_sync();
-        const uint32_t aA = tc::smem_u32(sA), aB = tc::smem_u32(Bb);
-        const uint32_t lboA = (kRows / 8) * 128, lboB = (NB / 8) * 128;
-        const uint32_t d0 = tmem + (uint32_t)(b * 2 * NB), d1 = d0 + (uint32_t)NB;
+        const uint32_t aA = tc::smem_u32(sA), aB = tc::smem_u32(sB);
+        const uint32_t lboA = (kRows / 8) * 128, lboB = (uint32_t)(N / 8) * 128;
+        const uint32_t idesc = tc::idesc_bf16_f32(kRows, N);
+        const uint32_t d0 = tmem, d1 = tmem + 128;
         for (int kk = 0; kk < KE / 16; kk++) {
           uint64_t ad[3], bd[3];
 #pragma unroll
           for (int c = 0; c < 3; c++) {
             ad[c] = tc::smem_desc(aA + c * kRows * KE * 2 + kk * 2 * lboA, lboA, 128);
-            bd[c] = tc::smem_desc(aB + c * NB * KE * 2 + kk * 2 * lboB, lboB, 128);
+            bd[c] = tc::smem_desc(aB + c * N * KE * 2 + kk * 2 * lboB, lboB, 128);
           }
           const uint32_t acc = kk > 0 ? 1u : 0u;
           tc::mma_bf16(d0, ad[0], bd[0], idesc, acc);
@@ -458,18 +426,56 @@ __global__ void __launch_bounds__(kThreads) k_eval_tc(EvalTcArgs a) {
           tc::mma_bf16(d1, ad[1], bd[1], idesc, 1u);
           tc::mma_bf16(d1, ad[2], bd[0], idesc, 1u);
         }
-        tc::commit(&mbar[b]);
+        tc::commit(&mbar[0]);
       }
-      if (s >= 1) readout(ind, s - 1, g - 1);
+      if (ok && !tc::mbar_wait(&mbar[0], g & 1, a.wait_iters)) {
+        ok = false;
+        atomicExch(a.err, 1);
+      }
+      tc::fence_after_sync();
+      // the B buffer is free again: fetch the next group's tiles during the readout
+      if (j + 1 < nbatch) load_batch(s0 + kEvalBatch, min(kEvalBatch, nsteps - s0 - kEvalBatch));
+      else if (ind + 1 < nd) load_batch(0, min(kEvalBatch, nsteps));
+      // readout: warp w covers TMEM lanes 32 (w%4)..; warps 0-3 take even steps, 4-7 odd steps
+      {
+        const int q = warp & 3, r = 32 * q + lane, rslot = r / n, rk1 = r - rslot * n;
+        const uint32_t lb = (uint32_t)(32 * q) << 16;
+        double pv[16];
+        double *pb = nullptr;
+        auto load_pot = [&](int st) {
+          const int box = st < S ? a.steps[(size_t)(sb + s0 + st) * stride + 1 + rslot] : -1;
+          pb = box >= 0 ? a.pot + (size_t)box * nd * npb + ind + (size_t)nd * rk1 : nullptr;
+#pragma unroll
+          for (int k2 = 0; k2 < 16; k2++) pv[k2] = (pb && k2 < n) ? pb[(size_t)nd * n * k2] : 0.0;
+        };
+        load_pot(warp >> 2);
+        for (int st = warp >> 2; st < S; st += 2) {
+          double pc[16];
+#pragma unroll
+          for (int k2 = 0; k2 < 16; k2++) pc[k2] = pv[k2];
+          double *pbc = pb;
+          if (st + 2 < S) load_pot(st + 2);
+          float v0[16], v1[16];
+          tc::tmem_ld16(tmem + lb + (uint32_t)(16 * st), v0);
+          tc::tmem_ld16(tmem + lb + 128u + (uint32_t)(16 * st), v1);
+          tc::tmem_ld_wait();
+          if (ok && pbc) {
+#pragma unroll
+            for (int k2 = 0; k2 < 16; k2++)
+              if (k2 < n) pbc[(size_t)nd * n * k2] = pc[k2] + 2.0 * ((double)v0[k2] + (double)v1[k2]);
+          }
+        }
+      }
+      tc::fence_before_sync();
+      __syncthreads();
     }
-    if (nsteps > 0) readout(ind, nsteps - 1, ind * nsteps + nsteps - 1);
-    __syncthreads();
   }
-  if (tid == 0) tc::commit(&mbar[2]);
-  if (!tc::mbar_wait(&mbar[2], 0, kWaitIters)) atomicExch(a.err, 2);
+  tc::cp_async_wait_all();
+  if (tid == 0) tc::commit(&mbar[1]);
+  if (!tc::mbar_wait(&mbar[1], 0, kWaitIters)) atomicExch(a.err, 2);
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 64);
+  if (warp == 0) tc::tmem_dealloc(tmem, 256);
 }
 
 // ---- host-side table preparation -----------------------------------------
@@ -647,8 +653,8 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     const int ybytes = kRows * hh * 16;
     const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 127) / 128) * 128;
     sp.smem_form = 128 + ubytes + sizeof(double2) * (size_t)n * npw;
-    const int eab = 3 * kRows * sp.KE * 2, ebb = 3 * sp.NB * sp.KE * 2;
-    sp.smem_eval = 128 + ((eab + 127) / 128) * 128 + ((2 * ebb + 127) / 128) * 128 +
+    const int eab = 3 * kRows * sp.KE * 2, ebb = 3 * (16 * kEvalBatch) * sp.KE * 2;
+    sp.smem_eval = 128 + ((eab + 127) / 128) * 128 + ((ebb + 127) / 128) * 128 +
                    sizeof(double2) * ((size_t)npw * hh + (size_t)npw * n + (size_t)sp.cpc * npw);
   }
   const int ntiles = ((npw + 1) / 2) * ((hh + 3) / 4);
@@ -694,7 +700,7 @@ void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
   EvalTcArgs a{d_pot, sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, dp.E,
                dp.PH, dp.ph_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
                sp.wait_iters};
-  k_eval_tc<<<sp.nchunks, kThreads, sp.smem_eval, s>>>(a);
+  k_eval_tc<<<sp.nchunks, kEvalThreads, sp.smem_eval, s>>>(a);
 }
 
 unsigned int split_default_wait_iters() { return kWaitIters; }

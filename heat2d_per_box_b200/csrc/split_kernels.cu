@@ -295,6 +295,7 @@ constexpr int kEvalThreads = 256;
 // previous group is read out), 18 MMAs with N = 16 x steps produce the values
 // of every leaf of the group, and the readout adds 2 (D0 + D1) into pot.
 // Warps w and w+4 share TMEM lanes 32 (w%4).. and split the group's steps.
+template <int NNT>
 __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(EvalTcArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);  // [0] MMA group done, [1] drain
@@ -343,6 +344,17 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(EvalTcArgs a) {
     const int slot = i / npw, m = i - slot * npw;
     sph[i] = a.PH[a.ph_off[ch.w] + (size_t)a.columns[ch.x + slot].z * npw + m];
   }
+  // A columns that H never writes: m2 in [hh, KH) of both parts, and K in [2 KH, KE)
+  {
+    const int padr = KH - hh, padk = KE - 2 * KH, per = 2 * padr + padk;
+    for (int i = tid; i < kRows * per; i += kEvalThreads) {
+      const int r = i / per, e = i - r * per;
+      const int k = e < padr ? hh + e : (e < 2 * padr ? KH + hh + (e - padr) : 2 * KH + (e - 2 * padr));
+      const uint32_t o = tc::kmajor_off(r, k, kRows);
+#pragma unroll
+      for (int c = 0; c < 3; c++) *reinterpret_cast<uint16_t *>(sA + c * kRows * KE * 2 + o) = 0;
+    }
+  }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
@@ -357,46 +369,69 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(EvalTcArgs a) {
       sL[m1 * hh + m2] = Lg[e];
     }
     __syncthreads();
-    // H for row r = (slot, k1), four m2 at a time; the two thread halves take alternate blocks
+    // H(r, m2) for rows r = (slot, k1) on the FP64 tensor cores: the real GEMM
+    // [Hr Hi] = [Er Ei] [[Lr Li], [-Li Lr]] with K = (m1, re/im) and N = (m2,
+    // re/im) interleaved, E(m1,k1) phase_ox(m1) formed on the fly.  Warp w owns
+    // rows 16w..16w+15 (two 8-row tiles) and all NNT column tiles.
     {
-      const int r = tid & (kRows - 1), half = tid >> 7, rslot = r / n, rk1 = r - rslot * n;
-      const bool live = rslot < ncol;
-      for (int blk = half; blk < KH / 4; blk += 2) {
-        const int mb = 4 * blk;
-        double2 acc[4];
+      const int g8 = lane >> 2, t4 = lane & 3;
+      int rs[2], rk[2];
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[j] = make_double2(0, 0);
-        if (live && mb < hh) {
-#pragma unroll 2
-          for (int m1 = 0; m1 < npw; m1++) {
-            const double2 e = zmul(sE[m1 * n + rk1], sph[rslot * npw + m1]);
+      for (int mt = 0; mt < 2; mt++) {
+        const int r = 16 * warp + 8 * mt + g8;
+        rs[mt] = r / n;
+        rk[mt] = r - rs[mt] * n;
+      }
+      double c[2][NNT][2];
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-              const double2 l = (mb + j < hh) ? sL[m1 * hh + mb + j] : make_double2(0, 0);
-              acc[j].x = fma(e.x, l.x, acc[j].x);
-              acc[j].x = fma(-e.y, l.y, acc[j].x);
-              acc[j].y = fma(e.x, l.y, acc[j].y);
-              acc[j].y = fma(e.y, l.x, acc[j].y);
-            }
+      for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int i = 0; i < NNT; i++) c[mt][i][0] = c[mt][i][1] = 0.0;
+      const int p = t4 & 1, q = g8 & 1;
+      for (int j = 0; j < (npw + 1) / 2; j++) {
+        const int m1 = 2 * j + (t4 >> 1);
+        const bool mok = m1 < npw;
+        double av[2];
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++) {
+          double v = 0.0;
+          if (mok && rs[mt] < ncol) {
+            const double2 e = zmul(sE[m1 * n + rk[mt]], sph[rs[mt] * npw + m1]);
+            v = p ? e.y : e.x;
           }
+          av[mt] = v;
         }
-        uint32_t re[3][2], im[3][2];
 #pragma unroll
-        for (int j = 0; j < 2; j++) {
-          tc::split3_bf16x2(acc[2 * j].x, acc[2 * j + 1].x, re[0][j], re[1][j], re[2][j]);
-          tc::split3_bf16x2(acc[2 * j].y, acc[2 * j + 1].y, im[0][j], im[1][j], im[2][j]);
-        }
-        const uint32_t ore = tc::kmajor_off(r, mb, kRows), oim = tc::kmajor_off(r, KH + mb, kRows);
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          *reinterpret_cast<uint2 *>(sA + c * kRows * KE * 2 + ore) = make_uint2(re[c][0], re[c][1]);
-          *reinterpret_cast<uint2 *>(sA + c * kRows * KE * 2 + oim) = make_uint2(im[c][0], im[c][1]);
+        for (int i = 0; i < NNT; i++) {
+          const int m2 = 4 * i + (g8 >> 1);
+          double bv = 0.0;
+          if (mok && m2 < hh) {
+            const double2 l = sL[m1 * hh + m2];
+            bv = p == 0 ? (q == 0 ? l.x : l.y) : (q == 0 ? -l.y : l.x);
+          }
+          tc::dmma_8x8x4(c[0][i], av[0], bv);
+          tc::dmma_8x8x4(c[1][i], av[1], bv);
         }
       }
-      for (int k = 2 * KH + 4 * half; k < KE; k += 8) {  // zero K padding
-        const uint32_t o = tc::kmajor_off(r, k, kRows);
+      // lane holds (Hr, Hi) of row 16w + 8mt + g8, m2 = 4i + t4: split into the A operand
 #pragma unroll
-        for (int c = 0; c < 3; c++) *reinterpret_cast<uint2 *>(sA + c * kRows * KE * 2 + o) = make_uint2(0, 0);
+      for (int mt = 0; mt < 2; mt++) {
+        const int r = 16 * warp + 8 * mt + g8;
+#pragma unroll
+        for (int i = 0; i < NNT; i++) {
+          const int m2 = 4 * i + t4;
+          if (m2 >= hh) continue;
+          uint16_t s0, s1, s2;
+          const uint32_t ore = tc::kmajor_off(r, m2, kRows), oim = tc::kmajor_off(r, KH + m2, kRows);
+          tc::split3_bf16x1(c[mt][i][0], s0, s1, s2);
+          *reinterpret_cast<uint16_t *>(sA + ore) = s0;
+          *reinterpret_cast<uint16_t *>(sA + kRows * KE * 2 + ore) = s1;
+          *reinterpret_cast<uint16_t *>(sA + 2 * kRows * KE * 2 + ore) = s2;
+          tc::split3_bf16x1(c[mt][i][1], s0, s1, s2);
+          *reinterpret_cast<uint16_t *>(sA + oim) = s0;
+          *reinterpret_cast<uint16_t *>(sA + kRows * KE * 2 + oim) = s1;
+          *reinterpret_cast<uint16_t *>(sA + 2 * kRows * KE * 2 + oim) = s2;
+        }
       }
     }
     for (int j = 0; j < nbatch; j++, g++) {
@@ -669,7 +704,14 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   }
   cudaFuncSetAttribute(k_form_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
   cudaFuncSetAttribute(k_form_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  cudaFuncSetAttribute(k_eval_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_eval_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_eval_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_eval_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_eval_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_eval_tc<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_eval_tc<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_eval_tc<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_eval_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
   sp.wait_iters = kWaitIters;
   // tensor-core FLOP issued per transform (every slice product counted)
   const double nsteps_total = (double)(steps.size() / (1 + sp.cpc));
@@ -700,7 +742,12 @@ void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
   EvalTcArgs a{d_pot, sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, dp.E,
                dp.PH, dp.ph_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
                sp.wait_iters};
-  k_eval_tc<<<sp.nchunks, kEvalThreads, sp.smem_eval, s>>>(a);
+  switch ((dp.hh + 3) / 4) {
+#define EVAL_NNT(X) \
+  case X: k_eval_tc<X><<<sp.nchunks, kEvalThreads, sp.smem_eval, s>>>(a); break;
+    EVAL_NNT(1) EVAL_NNT(2) EVAL_NNT(3) EVAL_NNT(4) EVAL_NNT(5) EVAL_NNT(6) EVAL_NNT(7) EVAL_NNT(8)
+#undef EVAL_NNT
+  }
 }
 
 unsigned int split_default_wait_iters() { return kWaitIters; }

@@ -102,6 +102,26 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint3
   return false;
 }
 
+// FP64 tensor-core MMA, D(8x8) += A(8x4) B(4x8): lane (g = lane/4, t = lane%4)
+// holds A[g][t], B[t][g] and D[g][2t], D[g][2t+1]
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// FP64 value -> three BF16 slices through FP32 (see split3_bf16x2)
+__device__ __forceinline__ void split3_bf16x1(double v, uint16_t &s0, uint16_t &s1, uint16_t &s2) {
+  const float a = __double2float_rn(v);
+  const __nv_bfloat16 h = __float2bfloat16_rn(a);
+  const float r = a - __bfloat162float(h);
+  const __nv_bfloat16 m = __float2bfloat16_rn(r);
+  const __nv_bfloat16 l = __float2bfloat16_rn(r - __bfloat162float(m));
+  s0 = __bfloat16_as_ushort(h);
+  s1 = __bfloat16_as_ushort(m);
+  s2 = __bfloat16_as_ushort(l);
+}
+
 // 16-byte global -> shared copy that bypasses registers (completion: cp_async_wait_all)
 __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");

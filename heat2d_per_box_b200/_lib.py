@@ -76,6 +76,10 @@ def lib():
     L.bfgt_plan_info.argtypes = [C.c_void_p, _i32p]
     L.bfgt_plan_work.restype = C.c_int
     L.bfgt_plan_work.argtypes = [C.c_void_p, _f64p]
+    L.bfgt_plan_execute_adjoint.restype = C.c_int
+    L.bfgt_plan_execute_adjoint.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.bfgt_plan_execute_adjoint_host.restype = C.c_int
+    L.bfgt_plan_execute_adjoint_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.bfgt_plan_execute_noalloc.restype = C.c_int
     L.bfgt_plan_execute_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.bfgt_noalloc_scratch_bytes.restype = C.c_int

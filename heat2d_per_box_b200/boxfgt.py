@@ -100,6 +100,19 @@ class Plan:
         _lib.check(self._L.bfgt_plan_execute_host(self._h, fv.ctypes.data, pot.ctypes.data, s))
         return pot
 
+    def execute_adjoint(self, d_potbar, d_fbar, stream=None):
+        """fbar += K^T potbar on leaf boxes (the transpose of execute: pot += K fvals)."""
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_plan_execute_adjoint(self._h, self._ptr(d_potbar), self._ptr(d_fbar), s))
+
+    def execute_adjoint_host(self, potbar, fbar, stream=None):
+        pb = np.ascontiguousarray(potbar, np.float64)
+        if not (isinstance(fbar, np.ndarray) and fbar.dtype == np.float64 and fbar.flags.c_contiguous):
+            raise TypeError("fbar must be a C-contiguous float64 array")
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_plan_execute_adjoint_host(self._h, pb.ctypes.data, fbar.ctypes.data, s))
+        return fbar
+
     def graph_capture(self, d_fvals, d_pot, stream=None):
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         _lib.check(self._L.bfgt_plan_graph_capture(self._h, self._ptr(d_fvals), self._ptr(d_pot), s))

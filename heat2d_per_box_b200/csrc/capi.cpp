@@ -113,13 +113,14 @@ int bfgt_plan_execute(bfgt_plan plan, const double *d_fvals, double *d_pot, void
   return BFGT_OK;
 }
 
-int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, void *stream) {
-  g_err.clear();
-  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
-  if (!fvals || !pot) return fail(BFGT_ERR_ARG, "fvals/pot are NULL");
-  bfgt::DevicePlan &dp = plan->dp;
+}  // extern "C"
+
+namespace {
+
+// Host-array form of one transform on dp: uploads the leaf runs of the input
+// and of the accumulator, runs, and copies the accumulator's leaf runs back.
+int execute_host_on(bfgt_plan plan, bfgt::DevicePlan &dp, const double *in, double *acc, cudaStream_t s) {
   const size_t elems = (size_t)dp.nd * dp.n * dp.n * dp.nboxes;
-  cudaStream_t s = (cudaStream_t)stream;
   if (dp.stage_elems < elems) {
     if (dp.d_stage_f) cudaFree(dp.d_stage_f);
     if (dp.d_stage_p) cudaFree(dp.d_stage_p);
@@ -132,12 +133,12 @@ int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, voi
     }
     dp.stage_elems = elems;
   }
-  // only the leaf boxes are read (fvals) and accumulated into (pot)
+  // only the leaf boxes are read (input) and accumulated into
   const size_t per = (size_t)dp.nd * dp.n * dp.n;
   for (const auto &r : plan->leaf_runs) {
     const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
-    if (cudaMemcpyAsync(dp.d_stage_f + o, fvals + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(dp.d_stage_p + o, pot + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    if (cudaMemcpyAsync(dp.d_stage_f + o, in + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dp.d_stage_p + o, acc + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess)
       return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
   }
   std::string msg;
@@ -145,11 +146,69 @@ int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, voi
   if (rc != BFGT_OK) return fail(rc, msg);
   for (const auto &r : plan->leaf_runs) {
     const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
-    if (cudaMemcpyAsync(pot + o, dp.d_stage_p + o, c, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    if (cudaMemcpyAsync(acc + o, dp.d_stage_p + o, c, cudaMemcpyDeviceToHost, s) != cudaSuccess)
       return fail(BFGT_ERR_CUDA, "device-to-host copy failed");
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(BFGT_ERR_CUDA, std::string("transform failed: ") + cudaGetErrorString(cudaGetLastError()));
   return BFGT_OK;
+}
+
+// Builds the plan's transposed twin on first use (host tables, then upload).
+int ensure_adjoint(bfgt_plan plan) {
+  if (plan->adj_dp) return BFGT_OK;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev != plan->dp.device) {
+    cudaGetLastError();
+    return fail(BFGT_ERR_ARG, "the current device is not the plan's device");
+  }
+  std::unique_ptr<bfgt::HostPlan> h(new bfgt::HostPlan());
+  try {
+    bfgt::build_adjoint_host_plan(*h, plan->hp);
+  } catch (const std::exception &e) {
+    return fail(BFGT_ERR_TREE, e.what());
+  }
+  std::unique_ptr<bfgt::DevicePlan> d(new bfgt::DevicePlan());
+  std::string msg;
+  int rc = bfgt::device_plan_create(*d, *h, msg);
+  if (rc != BFGT_OK) {
+    bfgt::device_plan_destroy(*d);
+    return fail(rc, msg);
+  }
+  plan->adj_hp = std::move(h);
+  plan->adj_dp = std::move(d);
+  return BFGT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, void *stream) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (!fvals || !pot) return fail(BFGT_ERR_ARG, "fvals/pot are NULL");
+  return execute_host_on(plan, plan->dp, fvals, pot, (cudaStream_t)stream);
+}
+
+int bfgt_plan_execute_adjoint(bfgt_plan plan, const double *d_potbar, double *d_fbar, void *stream) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (!d_potbar || !d_fbar) return fail(BFGT_ERR_ARG, "potbar/fbar device pointers are NULL");
+  int rc = ensure_adjoint(plan);
+  if (rc != BFGT_OK) return rc;
+  std::string msg;
+  rc = bfgt::device_plan_execute(*plan->adj_dp, d_potbar, d_fbar, (cudaStream_t)stream, msg);
+  if (rc != BFGT_OK) return fail(rc, msg);
+  return BFGT_OK;
+}
+
+int bfgt_plan_execute_adjoint_host(bfgt_plan plan, const double *potbar, double *fbar, void *stream) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (!potbar || !fbar) return fail(BFGT_ERR_ARG, "potbar/fbar are NULL");
+  int rc = ensure_adjoint(plan);
+  if (rc != BFGT_OK) return rc;
+  return execute_host_on(plan, *plan->adj_dp, potbar, fbar, (cudaStream_t)stream);
 }
 
 int bfgt_plan_graph_capture(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream) {
@@ -257,6 +316,7 @@ int bfgt_plan_check(bfgt_plan plan) {
   if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(BFGT_ERR_CUDA, std::string("device error: ") + cudaGetErrorString(cudaGetLastError()));
   int rc = bfgt::split_check(plan->dp);
+  if (rc == BFGT_OK && plan->adj_dp) rc = bfgt::split_check(*plan->adj_dp);
   if (rc == BFGT_ERR_TIMEOUT) return fail(rc, "a bounded device-side wait gave up (tensor-core pipeline)");
   if (rc != BFGT_OK) return fail(rc, "error flag read-out failed");
   return BFGT_OK;
@@ -266,6 +326,7 @@ int bfgt_plan_set_wait_limit(bfgt_plan plan, unsigned int polls) {
   g_err.clear();
   if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
   plan->dp.split.wait_iters = polls == 0xFFFFFFFFu ? bfgt::split_default_wait_iters() : polls;
+  if (plan->adj_dp) plan->adj_dp->split.wait_iters = plan->dp.split.wait_iters;
   return BFGT_OK;
 }
 
@@ -273,6 +334,7 @@ int bfgt_plan_destroy(bfgt_plan plan) {
   g_err.clear();
   if (!plan) return BFGT_OK;
   bfgt::device_plan_destroy(plan->dp);
+  if (plan->adj_dp) bfgt::device_plan_destroy(*plan->adj_dp);
   delete plan;
   return BFGT_OK;
 }

@@ -43,6 +43,7 @@ struct DevicePlan {
   int *cut_chunk_begin = nullptr, *cut_pw_begin = nullptr, *cut_pw_src = nullptr, *cut_pw_ind = nullptr;
   double2 *W = nullptr;         // cutoff shifts (nexp, 9)
   double *pw_weight = nullptr;  // (hh)
+  double *kscale = nullptr;     // (hh) translation factor per k2, or null
   double2 *Mpart = nullptr;     // (nchunks, nd, nexp) partial expansions per chunk
   double2 *M = nullptr;         // (ncut, nd, nexp) cutoff-box expansions
   double2 *L = nullptr;         // (ncut, nd, nexp) cutoff-box local expansions
@@ -53,7 +54,7 @@ struct DevicePlan {
   bool multi_group = false;
   SplitPlan split;
   // near field
-  int *nf_target = nullptr, *nf_level = nullptr, *nf_begin = nullptr, *nf_src = nullptr;
+  int *nf_target = nullptr, *nf_begin = nullptr, *nf_src = nullptr;
   int2 *nf_ixy = nullptr;
   double *tab_loc = nullptr;
   int *ind_loc = nullptr;

@@ -73,9 +73,12 @@ struct FormArgs {
 // across its columns; warps are then summed in a fixed order.
 // L(icut) = M(icut) + sum over its plane-wave list of M(src) * W(shift)
 // (mp -> loc at the cutoff level, boxfgt.f:805-822), one thread per element.
+// kscale (hh entries, may be null) multiplies element (k1,k2) by kscale[k2];
+// the transposed transform uses it for the half-spectrum weight.
 __global__ void k_translate(const double2 *__restrict__ M, const int *__restrict__ pw_begin,
                             const int *__restrict__ pw_src, const int *__restrict__ pw_ind,
-                            const double2 *__restrict__ W, double2 *__restrict__ L, int ncut, int nd, int nexp) {
+                            const double2 *__restrict__ W, const double *__restrict__ kscale,
+                            double2 *__restrict__ L, int ncut, int nd, int npw, int nexp) {
   const size_t per = (size_t)nd * nexp;
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= per * ncut) return;
@@ -89,9 +92,13 @@ __global__ void k_translate(const double2 *__restrict__ M, const int *__restrict
     s.x += m.x * w.x - m.y * w.y;
     s.y += m.x * w.y + m.y * w.x;
   }
+  if (kscale) {
+    const double f = kscale[e / npw];
+    s.x *= f;
+    s.y *= f;
+  }
   L[idx] = s;
 }
-
 
 template <int TM, int TN, int NT>
 __global__ void __launch_bounds__(kWarps * 32, 3) k_form_fp64(FormArgs a) {
@@ -401,15 +408,17 @@ void set_smem_attrs(int bytes) {
 struct NearArgs {
   const double *fvals;
   double *pot;
-  const int *target, *level, *begin, *src;
-  const int2 *ixy;
+  const int *target, *begin, *src;
+  const int2 *ixy;  // per entry: table slots (level * 13 + offset + 6) in x and y
   const double *tab_loc;
   const int *ind_loc;
   int ntarget, nd, n;
 };
 
 // One warp per near-field target leaf; pot(k1,k2) += sum over its list1
-// entries of Ty^T (Tx^T F) on the banded 1D tables of the target's level.
+// entries of Ty^T (Tx^T F) on the banded 1D tables of each entry's slots
+// (the forward pass uses the target's level, the transposed pass the level
+// of the forward target).
 __global__ void __launch_bounds__(kWarps * 32) k_near_fp64(NearArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -418,21 +427,20 @@ __global__ void __launch_bounds__(kWarps * 32) k_near_fp64(NearArgs a) {
   const int n = a.n, npb = n * n, nd = a.nd;
   double *wb = reinterpret_cast<double *>(smem_raw) + (size_t)warp * 3 * npb;
   double *sF = wb, *sff = wb + npb, *sP = wb + 2 * npb;
-  const int tb = a.target[t], lev = a.level[t];
-  const size_t tsz = (size_t)npb * 13, isz = (size_t)2 * (n + 1) * 13;
-  const double *tl = a.tab_loc + tsz * lev;
-  const int *il = a.ind_loc + isz * lev;
+  const int tb = a.target[t];
+  const double *tl = a.tab_loc;
+  const int *il = a.ind_loc;
   for (int ind = 0; ind < nd; ind++) {
     for (int o = lane; o < npb; o += 32) sP[o] = 0;
     for (int e = a.begin[t]; e < a.begin[t + 1]; e++) {
       const int sb = a.src[e];
       const int ix = a.ixy[e].x, iy = a.ixy[e].y;
-      const int *bx = il + (size_t)2 * (n + 1) * (ix + 6);
-      const int *by = il + (size_t)2 * (n + 1) * (iy + 6);
+      const int *bx = il + (size_t)2 * (n + 1) * ix;
+      const int *by = il + (size_t)2 * (n + 1) * iy;
       const int kx0 = bx[2 * n], kx1 = bx[2 * n + 1], ky0 = by[2 * n], ky1 = by[2 * n + 1];
       if (kx1 - kx0 + 1 == 0 || ky1 - ky0 + 1 == 0) continue;
-      const double *tx = tl + (size_t)npb * (ix + 6);
-      const double *ty = tl + (size_t)npb * (iy + 6);
+      const double *tx = tl + (size_t)npb * ix;
+      const double *ty = tl + (size_t)npb * iy;
       const double *fv = a.fvals + (size_t)sb * nd * npb;
       __syncwarp();
       for (int o = lane; o < npb; o += 32) sF[o] = fv[ind + (size_t)nd * o];
@@ -591,6 +599,7 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     chk(upload(dp.cut_pw_src, hp.cut_pw_src, msg));
     chk(upload(dp.cut_pw_ind, hp.cut_pw_ind, msg));
     chk(upload(dp.pw_weight, hp.pw_weight, msg));
+    chk(upload(dp.kscale, hp.kscale, msg));
     const size_t ex = (size_t)dp.nd * dp.nexp * sizeof(double2);
     chk(alloc_bytes((void **)&dp.Mpart, ex * dp.nchunks, msg));
     chk(alloc_bytes((void **)&dp.M, ex * dp.ncut, msg));
@@ -620,9 +629,9 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   dp.nnf_entries = (int)hp.nf_src.size();
   if (dp.nnf > 0) {
     std::vector<int2> ixy(hp.nf_src.size());
-    for (size_t i = 0; i < ixy.size(); i++) ixy[i] = make_int2(hp.nf_ix[i], hp.nf_iy[i]);
+    for (size_t i = 0; i < ixy.size(); i++)
+      ixy[i] = make_int2(hp.nf_elev[i] * 13 + hp.nf_ix[i] + 6, hp.nf_elev[i] * 13 + hp.nf_iy[i] + 6);
     chk(upload(dp.nf_target, hp.nf_target, msg));
-    chk(upload(dp.nf_level, hp.nf_level, msg));
     chk(upload(dp.nf_begin, hp.nf_begin, msg));
     chk(upload(dp.nf_src, hp.nf_src, msg));
     chk(upload(dp.nf_ixy, ixy, msg));
@@ -654,7 +663,7 @@ void device_plan_destroy(DevicePlan &dp) {
   if (dp.graph) cudaGraphDestroy(dp.graph);
   split_plan_destroy(dp);
   void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.columns, dp.cut_chunk_begin, dp.cut_pw_begin,
-                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.Mpart, dp.M, dp.L, dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups, dp.nf_target, dp.nf_level,
+                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.kscale, dp.Mpart, dp.M, dp.L, dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups, dp.nf_target,
                   dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.d_stage_f, dp.d_stage_p};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -715,7 +724,7 @@ int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cu
     {
       const size_t tot = (size_t)dp.ncut * dp.nd * dp.nexp;
       k_translate<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(dp.M, dp.cut_pw_begin, dp.cut_pw_src, dp.cut_pw_ind,
-                                                                 dp.W, dp.L, dp.ncut, dp.nd, dp.nexp);
+                                                                 dp.W, dp.kscale, dp.L, dp.ncut, dp.nd, dp.npw, dp.nexp);
     }
     if (ev) cudaEventRecord(ev[3], s);
     if (dp.precision == BFGT_PREC_SPLIT) {
@@ -730,8 +739,8 @@ int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cu
     for (int i = 1; i <= 4; i++) cudaEventRecord(ev[i], s);
   }
   if (dp.nnf > 0) {
-    NearArgs na{d_fvals, d_pot, dp.nf_target, dp.nf_level, dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc,
-                dp.ind_loc, dp.nnf, dp.nd, dp.n};
+    NearArgs na{d_fvals, d_pot, dp.nf_target, dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.nnf,
+                dp.nd, dp.n};
     k_near_fp64<<<(dp.nnf + kWarps - 1) / kWarps, nthreads, dp.smem_near, s>>>(na);
   }
   if (ev) cudaEventRecord(ev[5], s);

@@ -696,6 +696,29 @@ void leaf_nodes(int ipoly, int n, std::vector<double> &x, std::vector<double> &u
   else chebexps2(n, x, u, v, w);
 }
 
+namespace {
+
+// FLOP of the near-field pass: a banded x then y contraction per pair entry
+double near_flops(const HostPlan &hp) {
+  const int n = hp.norder;
+  const double nn = n;
+  double f = 0;
+  for (size_t e = 0; e < hp.nf_src.size(); e++) {
+    const int *il = &hp.ind_loc[(size_t)2 * (n + 1) * 13 * hp.nf_elev[e]];
+    auto band = [&](int k) {
+      const int *p = il + (size_t)2 * (n + 1) * (k + 6);
+      int nk = p[2 * n + 1] - p[2 * n] + 1;
+      return nk < 0 ? 0 : nk;
+    };
+    const double nx = band(hp.nf_ix[e]), ny = band(hp.nf_iy[e]);
+    if (nx == 0 || ny == 0) continue;
+    f += hp.nd * 2.0 * (nx * nn * nn + nx * ny * nn);
+  }
+  return f;
+}
+
+}  // namespace
+
 void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, double eps, int ipoly, int iperiod,
                      int norder, int precision) {
   if (nd < 1) throw std::runtime_error("nd must be >= 1");
@@ -1110,6 +1133,9 @@ void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, doub
   hp.nf_src.clear();
   hp.nf_ix.clear();
   hp.nf_iy.clear();
+  hp.nf_elev.clear();
+  hp.kscale.clear();
+  hp.adjoint = false;
   if (!(npwlevel == 0 && iperiod_i == 0)) {
     auto loctab_ind = [&](int ip, double tx, double ty, double sx, double sy, double sbs, int *ixy) {
       double bs = sbs / 4.0;
@@ -1138,6 +1164,7 @@ void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, doub
             hp.nf_src.push_back(jb - 1);
             hp.nf_ix.push_back(v[0]);
             hp.nf_iy.push_back(v[1]);
+            hp.nf_elev.push_back(l);
           };
           if (iperiod_i == 1 && jlev == 1) {
             loctab_ind(0, t.cen(1, b), t.cen(2, b), t.cen(1, jb), t.cen(2, jb), bs, ixy);
@@ -1193,20 +1220,7 @@ void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, doub
     hp.bytes_form = nl * nn * nn * 8;    // leaf values read
     hp.bytes_eval = nl * nn * nn * 16;   // pot read + write
     fl += hp.flops_form + hp.flops_eval + hp.flops_translate;
-    for (size_t tg = 0; tg < hp.nf_target.size(); tg++) {
-      const int *il = &hp.ind_loc[(size_t)2 * (n + 1) * 13 * hp.nf_level[tg]];
-      auto band = [&](int k) {
-        const int *p = il + (size_t)2 * (n + 1) * (k + 6);
-        int nk = p[2 * n + 1] - p[2 * n] + 1;
-        return nk < 0 ? 0 : nk;
-      };
-      for (int e = hp.nf_begin[tg]; e < hp.nf_begin[tg + 1]; e++) {
-        // banded x then y contraction of one near-field pair
-        double nx = band(hp.nf_ix[e]), ny = band(hp.nf_iy[e]);
-        if (nx == 0 || ny == 0) continue;
-        hp.flops_near += nd * 2.0 * (nx * nn * nn + nx * ny * nn);
-      }
-    }
+    hp.flops_near = near_flops(hp);
     fl += hp.flops_near;
     hp.bytes_near = (double)hp.nf_target.size() * nd * nn * nn * 16 + (double)hp.nf_src.size() * nd * nn * nn * 8;
     hp.flops = fl;
@@ -1217,6 +1231,103 @@ void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, doub
     hp.points = leafpts * nd;
     hp.bytes = hp.points * 24.0;
   }
+}
+
+void build_adjoint_host_plan(HostPlan &a, const HostPlan &f) {
+  a = f;
+  a.adjoint = true;
+  const int n = f.norder, npw = f.npw;
+  // plane waves.  Per leaf the forward map is
+  //   M = sum T(m1,k1) T(m2,k2) conj(ph(k1) ph(k2)) F(m1,m2),  L = Tr(M),
+  //   pot += 2 Re sum w(k2) E(k1,x1) E(k2,x2) ph(k1) ph(k2) L(k1,k2).
+  // Its transpose (real inner products) is
+  //   L' = 2 w(k2) sum conj(E(k1,x1)) conj(E(k2,x2)) conj(ph ph) P(x1,x2),
+  //   M' = Tr^H(L') = Tr(L') (listpw is symmetric and W(-d) = conj(W(d))),
+  //   G += Re sum conj(T(m1,k1)) conj(T(m2,k2)) ph ph M'(k1,k2),
+  // i.e. the forward kernels with T <- conj(E)^T, E <- conj(T)^T, weight 1
+  // in the evaluation, and the factor w(k2) (= 2 w / 2) applied by the
+  // translation, which commutes with it (elementwise in k2).
+  if (!f.direct_only) {
+    const size_t per = (size_t)n * npw;
+    for (int l = f.nlevstart; l <= f.nlevels; l++) {
+      const cplx *T = &f.tab_poly2pw[per * l];
+      const cplx *E = &f.tab_pw2pot[per * l];
+      cplx *Ta = &a.tab_poly2pw[per * l];
+      cplx *Ea = &a.tab_pw2pot[per * l];
+      for (int k = 0; k < npw; k++)
+        for (int m = 0; m < n; m++) {
+          const cplx e = E[k + (size_t)npw * m], t = T[m + (size_t)n * k];
+          Ta[m + (size_t)n * k] = cplx{e.re, -e.im};
+          Ea[k + (size_t)npw * m] = cplx{t.re, -t.im};
+        }
+    }
+    a.kscale = f.pw_weight;
+    a.pw_weight.assign(f.hh, 1.0);
+  }
+  // near field: each 1D table A(j,k) (source node j -> target node k, used on
+  // the band ind_loc of column k) becomes its transpose with the band of the
+  // transposed nonzero pattern; entries outside the forward band are zero, so
+  // the transpose is exact for the banded operator the forward pass applies
+  const size_t ntl = (size_t)n * n, nil = (size_t)2 * (n + 1);
+  const size_t nslot = (size_t)13 * (f.nlevels + 1);
+  for (size_t sl = 0; sl < nslot; sl++) {
+    const double *tb = &f.tab_loc[ntl * sl];
+    const int *ib = &f.ind_loc[nil * sl];
+    double *ta = &a.tab_loc[ntl * sl];
+    int *ia = &a.ind_loc[nil * sl];
+    std::fill(ta, ta + ntl, 0.0);
+    std::vector<int> lo(n + 1, n + 1), hi(n + 1, 0);
+    const int k0 = ib[2 * n], k1 = ib[2 * n + 1];
+    for (int k = k0; k >= 1 && k <= k1; k++)
+      for (int j = ib[2 * (k - 1)]; j >= 1 && j <= ib[2 * (k - 1) + 1]; j++) {
+        ta[(k - 1) + (size_t)n * (j - 1)] = tb[(j - 1) + (size_t)n * (k - 1)];
+        lo[j] = std::min(lo[j], k);
+        hi[j] = std::max(hi[j], k);
+      }
+    int j0 = 0, j1 = -1;
+    for (int j = 1; j <= n; j++) {
+      if (hi[j] > 0) {
+        ia[2 * (j - 1)] = lo[j];
+        ia[2 * (j - 1) + 1] = hi[j];
+        if (j0 == 0) j0 = j;
+        j1 = j;
+      } else {
+        ia[2 * (j - 1)] = 0;
+        ia[2 * (j - 1) + 1] = -1;
+      }
+    }
+    ia[2 * n] = j0;
+    ia[2 * n + 1] = j1;
+  }
+  // transposed pair lists: grouped by the forward source, in forward order
+  const size_t ne = f.nf_src.size();
+  std::vector<int> tgt_of(ne);
+  for (size_t tg = 0; tg < f.nf_target.size(); tg++)
+    for (int e = f.nf_begin[tg]; e < f.nf_begin[tg + 1]; e++) tgt_of[e] = f.nf_target[tg];
+  std::vector<size_t> ord(ne);
+  for (size_t e = 0; e < ne; e++) ord[e] = e;
+  std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return f.nf_src[x] < f.nf_src[y]; });
+  a.nf_target.clear();
+  a.nf_level.clear();
+  a.nf_begin.assign(1, 0);
+  a.nf_src.resize(ne);
+  a.nf_ix.resize(ne);
+  a.nf_iy.resize(ne);
+  a.nf_elev.resize(ne);
+  for (size_t i = 0; i < ne; i++) {
+    const size_t e = ord[i];
+    if (a.nf_target.empty() || a.nf_target.back() != f.nf_src[e]) {
+      if (!a.nf_target.empty()) a.nf_begin.push_back((int)i);
+      a.nf_target.push_back(f.nf_src[e]);
+      a.nf_level.push_back(-1);  // entries carry their own table level
+    }
+    a.nf_src[i] = tgt_of[e];
+    a.nf_ix[i] = f.nf_ix[e];
+    a.nf_iy[i] = f.nf_iy[e];
+    a.nf_elev[i] = f.nf_elev[e];
+  }
+  if (!a.nf_target.empty()) a.nf_begin.push_back((int)ne);
+  a.flops_near = near_flops(a);
 }
 
 }  // namespace bfgt

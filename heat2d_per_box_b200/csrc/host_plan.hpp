@@ -95,6 +95,10 @@ struct HostPlan {
   // near field: per target leaf, entries (source box, ix, iy)
   std::vector<int> nf_target, nf_level, nf_begin;  // nf_begin has ntarget+1 entries
   std::vector<int> nf_src, nf_ix, nf_iy;
+  std::vector<int> nf_elev;  // per entry: level of the 1D tables it uses (its target's level)
+  // per-k2 factor the cutoff translation applies to L (hh entries; empty = 1)
+  std::vector<double> kscale;
+  bool adjoint = false;  // this plan applies the transpose of the transform
   // work accounting
   double flops = 0, bytes = 0, tc_flops = 0, points = 0;
   double flops_form = 0, flops_eval = 0, flops_near = 0, flops_translate = 0;
@@ -106,6 +110,14 @@ struct HostPlan {
 // Throws std::runtime_error with a message on invalid input.
 void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, double eps, int ipoly, int iperiod,
                      int norder, int precision);
+
+// Host half of the transpose of the transform fwd describes (f -> pot
+// becomes pot_bar -> f_bar, both on leaf boxes).  Same tree lists, leaf
+// offsets, phases and cutoff shifts; the plane-wave tables are swapped and
+// conjugated (values->PW becomes conj(E)^T, PW->values conj(T)^T), the
+// half-spectrum weight moves into the cutoff translation, and the near-field
+// tables, band patterns and pair lists are transposed.
+void build_adjoint_host_plan(HostPlan &adj, const HostPlan &fwd);
 
 // A generated tree in the reference layout (caller-side test/benchmark input).
 struct TreeData {

@@ -3,6 +3,7 @@
 #include "device_plan.hpp"
 #include "host_plan.hpp"
 
+#include <memory>
 #include <utility>
 #include <vector>
 
@@ -15,4 +16,7 @@ struct bfgt_plan_s {
   // merged, so a range may include some non-leaf boxes, which the transform
   // neither reads nor writes)
   std::vector<std::pair<int, int>> leaf_runs;
+  // the transposed transform (bfgt_plan_execute_adjoint), built on first use
+  std::unique_ptr<bfgt::HostPlan> adj_hp;
+  std::unique_ptr<bfgt::DevicePlan> adj_dp;
 };

@@ -89,6 +89,21 @@ int bfgt_plan_execute(bfgt_plan plan, const double *d_fvals, double *d_pot, void
    result into the host pot (the reference-facing form of a planned call). */
 int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, void *stream);
 
+/* No counterpart in the reference (boxfgt has no adjoint; this is the
+   differentiation entry point).  Applies the transpose of this plan's discrete
+   transform on device arrays: fbar(nd,norder**2,nboxes) += K^T potbar on leaf
+   boxes, where pot += K fvals is what bfgt_plan_execute computes, so that
+   sum(potbar * K f) = sum(f * K^T potbar) over leaf values.  For
+   J = 0.5*|K f - g|^2 the gradient dJ/dfvals is K^T (K f - g).  Same precision
+   mode as the plan.  The first call builds the transposed tables (host
+   precomputation and device allocation, synchronous); later calls only queue
+   kernels on stream. */
+int bfgt_plan_execute_adjoint(bfgt_plan plan, const double *d_potbar, double *d_fbar, void *stream);
+
+/* The same on host arrays (leaf boxes copied in and out, as in
+   bfgt_plan_execute_host). */
+int bfgt_plan_execute_adjoint_host(bfgt_plan plan, const double *potbar, double *fbar, void *stream);
+
 /* No counterpart in the reference (the Fortran boxfgt allocates its own
    workspace on every call).  Runs the same transform as bfgt_plan_execute
    without allocating anything: the plane-wave scratch (partial expansions of

@@ -92,6 +92,18 @@ def lib():
     L.bfgt_plan_set_wait_limit.argtypes = [C.c_void_p, C.c_uint]
     L.bfgt_plan_destroy.restype = C.c_int
     L.bfgt_plan_destroy.argtypes = [C.c_void_p]
+    for name, args in (("bfgt_batch_create", [C.POINTER(C.c_void_p), C.c_int, C.c_void_p]),
+                       ("bfgt_batch_layout", [C.c_void_p, C.c_void_p]),
+                       ("bfgt_batch_execute", [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+                       ("bfgt_batch_graph_capture", [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+                       ("bfgt_batch_graph_launch", [C.c_void_p, C.c_void_p]),
+                       ("bfgt_batch_stage_ms", [C.c_void_p, _f64p]),
+                       ("bfgt_batch_info", [C.c_void_p, _i32p]),
+                       ("bfgt_batch_check", [C.c_void_p]),
+                       ("bfgt_batch_destroy", [C.c_void_p])):
+        f = getattr(L, name)
+        f.restype = C.c_int
+        f.argtypes = args
     L.bfgt_host_plan_dump.restype = C.c_int
     L.bfgt_host_plan_dump.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                       C.c_int, _i32p, _i32p, _f64p, _f64p] + [C.c_void_p] * 4 + [C.c_int] + \

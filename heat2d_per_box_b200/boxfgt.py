@@ -165,6 +165,63 @@ class Plan:
             pass
 
 
+class Batch:
+    """Transforms of several plans run together (bfgt_batch_* in bfgt.h).
+
+    The leaf arrays of the plans are packed one after another: plan i's
+    fvals/pot occupy elements offsets[i]:offsets[i+1] of the batch arrays.
+    The plans must stay open while the batch exists.
+    """
+
+    def __init__(self, plans):
+        self._L = _lib.lib()
+        self.plans = list(plans)
+        arr = (C.c_void_p * len(self.plans))(*[p._h.value for p in self.plans])
+        h = C.c_void_p()
+        _lib.check(self._L.bfgt_batch_create(C.byref(h), len(self.plans), C.cast(arr, C.c_void_p)))
+        self._h = h
+        off = np.zeros(len(self.plans) + 1, np.int64)
+        _lib.check(self._L.bfgt_batch_layout(self._h, off.ctypes.data))
+        self.offsets = off
+
+    def execute(self, d_fvals, d_pot, stream=None):
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_batch_execute(self._h, Plan._ptr(d_fvals), Plan._ptr(d_pot), s))
+
+    def graph_capture(self, d_fvals, d_pot, stream=None):
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_batch_graph_capture(self._h, Plan._ptr(d_fvals), Plan._ptr(d_pot), s))
+
+    def graph_launch(self, stream=None):
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_batch_graph_launch(self._h, s))
+
+    def stage_ms(self):
+        out = np.zeros(8)
+        _lib.check(self._L.bfgt_batch_stage_ms(self._h, out))
+        return out
+
+    def info(self):
+        out = np.zeros(8, np.int32)
+        _lib.check(self._L.bfgt_batch_info(self._h, out))
+        keys = ["plans", "launches", "form_items", "eval_items", "translate_blocks", "near_blocks"]
+        return {k: int(out[i]) for i, k in enumerate(keys)}
+
+    def check(self):
+        _lib.check(self._L.bfgt_batch_check(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.bfgt_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def host_plan_dump(tree, delta, eps, nd=1, mnlist1_cap=64):
     """Host half of a plan (no device needed): lists, band patterns, near-field tables, PW nodes."""
     L = _lib.lib()

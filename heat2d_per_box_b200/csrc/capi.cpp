@@ -10,6 +10,7 @@
 #include <string>
 
 #include "../../include/bfgt.h"
+#include "batch.hpp"
 #include "device_plan.hpp"
 #include "host_plan.hpp"
 #include "split_kernels.cuh"
@@ -18,6 +19,12 @@
 
 struct bfgt_tree_s {
   std::unique_ptr<bfgt::TreeData> t;
+};
+
+struct bfgt_batch_s {
+  std::vector<bfgt_plan> plans;  // not owned; must outlive the batch
+  bfgt::DeviceBatch db;
+  int device = 0;
 };
 
 namespace {
@@ -501,6 +508,131 @@ int bfgt_tree_export(bfgt_tree tree, int *itree, int *iptr, double *centers, dou
 
 int bfgt_tree_free(bfgt_tree tree) {
   delete tree;
+  return BFGT_OK;
+}
+
+int bfgt_batch_create(bfgt_batch *batch, int nplans, const bfgt_plan *plans) {
+  g_err.clear();
+  if (!batch) return fail(BFGT_ERR_ARG, "batch pointer is NULL");
+  *batch = nullptr;
+  if (nplans <= 0 || !plans) return fail(BFGT_ERR_ARG, "a batch needs at least one plan");
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(BFGT_ERR_NODEVICE, "no current CUDA device");
+  }
+  std::unique_ptr<bfgt_batch_s> b(new bfgt_batch_s());
+  std::vector<bfgt::DevicePlan *> dps;
+  for (int i = 0; i < nplans; i++) {
+    if (!plans[i]) return fail(BFGT_ERR_ARG, "plan " + std::to_string(i) + " is NULL");
+    if (plans[i]->dp.device != dev) return fail(BFGT_ERR_ARG, "plan " + std::to_string(i) + " is on another device");
+    b->plans.push_back(plans[i]);
+    dps.push_back(&plans[i]->dp);
+  }
+  b->device = dev;
+  std::string msg;
+  int rc = bfgt::device_batch_create(b->db, dps, msg);
+  if (rc != BFGT_OK) {
+    bfgt::device_batch_destroy(b->db);
+    return fail(rc, msg);
+  }
+  *batch = b.release();
+  return BFGT_OK;
+}
+
+int bfgt_batch_layout(bfgt_batch batch, int64_t *offsets) {
+  g_err.clear();
+  if (!batch || !offsets) return fail(BFGT_ERR_ARG, "NULL argument");
+  for (size_t i = 0; i < batch->db.offs.size(); i++) offsets[i] = batch->db.offs[i];
+  return BFGT_OK;
+}
+
+int bfgt_batch_execute(bfgt_batch batch, const double *d_fvals, double *d_pot, void *stream) {
+  g_err.clear();
+  if (!batch) return fail(BFGT_ERR_ARG, "batch is NULL");
+  if (!d_fvals || !d_pot) return fail(BFGT_ERR_ARG, "fvals/pot device pointers are NULL");
+  std::string msg;
+  int rc = bfgt::device_batch_execute(batch->db, d_fvals, d_pot, (cudaStream_t)stream, msg);
+  if (rc != BFGT_OK) return fail(rc, msg);
+  return BFGT_OK;
+}
+
+int bfgt_batch_graph_capture(bfgt_batch batch, const double *d_fvals, double *d_pot, void *stream) {
+  g_err.clear();
+  if (!batch) return fail(BFGT_ERR_ARG, "batch is NULL");
+  bfgt::DeviceBatch &db = batch->db;
+  cudaStream_t cs = (cudaStream_t)stream;
+  bool own = false;
+  if (!cs) {
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return fail(BFGT_ERR_CUDA, "stream create failed");
+    own = true;
+  }
+  if (db.graph_exec) cudaGraphExecDestroy(db.graph_exec);
+  if (db.graph) cudaGraphDestroy(db.graph);
+  db.graph_exec = nullptr;
+  db.graph = nullptr;
+  const bool ev = db.events;
+  db.events = false;  // no event records inside the graph
+  std::string msg;
+  int rc = BFGT_OK;
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = BFGT_ERR_CUDA, msg = "begin capture failed";
+  if (rc == BFGT_OK) rc = bfgt::device_batch_execute(db, d_fvals, d_pot, cs, msg);
+  cudaGraph_t g = nullptr;
+  if (cudaStreamEndCapture(cs, &g) != cudaSuccess && rc == BFGT_OK) rc = BFGT_ERR_CUDA, msg = "end capture failed";
+  db.events = ev;
+  if (rc == BFGT_OK && cudaGraphInstantiate(&db.graph_exec, g, 0) != cudaSuccess) rc = BFGT_ERR_CUDA, msg = "graph instantiate failed";
+  db.graph = g;
+  if (own) cudaStreamDestroy(cs);
+  if (rc != BFGT_OK) {
+    cudaGetLastError();
+    return fail(rc, msg);
+  }
+  return BFGT_OK;
+}
+
+int bfgt_batch_graph_launch(bfgt_batch batch, void *stream) {
+  g_err.clear();
+  if (!batch || !batch->db.graph_exec) return fail(BFGT_ERR_ARG, "no captured graph on this batch");
+  if (cudaGraphLaunch(batch->db.graph_exec, (cudaStream_t)stream) != cudaSuccess) return fail(BFGT_ERR_CUDA, "graph launch failed");
+  return BFGT_OK;
+}
+
+int bfgt_batch_stage_ms(bfgt_batch batch, double *out) {
+  g_err.clear();
+  if (!batch || !out) return fail(BFGT_ERR_ARG, "NULL argument");
+  if (bfgt::device_batch_stage_ms(batch->db, out) != BFGT_OK) return fail(BFGT_ERR_CUDA, "event read-out failed");
+  return BFGT_OK;
+}
+
+int bfgt_batch_info(bfgt_batch batch, int *out) {
+  g_err.clear();
+  if (!batch || !out) return fail(BFGT_ERR_ARG, "NULL argument");
+  for (int i = 0; i < 8; i++) out[i] = 0;
+  const bfgt::DeviceBatch &db = batch->db;
+  out[0] = (int)batch->plans.size();
+  out[1] = bfgt::device_batch_launches(db);
+  for (const auto &g : db.split.form_groups) out[2] += g.count;
+  for (const auto &g : db.split.eval_groups) out[3] += g.count;
+  out[4] = db.tr_blocks;
+  out[5] = db.nf_blocks;
+  return BFGT_OK;
+}
+
+int bfgt_batch_check(bfgt_batch batch) {
+  g_err.clear();
+  if (!batch) return fail(BFGT_ERR_ARG, "batch is NULL");
+  for (bfgt_plan p : batch->plans) {
+    int rc = bfgt_plan_check(p);
+    if (rc != BFGT_OK) return rc;
+  }
+  return BFGT_OK;
+}
+
+int bfgt_batch_destroy(bfgt_batch batch) {
+  g_err.clear();
+  if (!batch) return BFGT_OK;
+  bfgt::device_batch_destroy(batch->db);
+  delete batch;
   return BFGT_OK;
 }
 

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "../../include/bfgt.h"
+#include "batch.hpp"
 #include "device_plan.hpp"
 #include "fgt_common.cuh"
 #include "split_kernels.cuh"
@@ -75,29 +76,47 @@ struct FormArgs {
 // (mp -> loc at the cutoff level, boxfgt.f:805-822), one thread per element.
 // kscale (hh entries, may be null) multiplies element (k1,k2) by kscale[k2];
 // the transposed transform uses it for the half-spectrum weight.
-__global__ void k_translate(const double2 *__restrict__ M, const int *__restrict__ pw_begin,
-                            const int *__restrict__ pw_src, const int *__restrict__ pw_ind,
-                            const double2 *__restrict__ W, const double *__restrict__ kscale,
-                            double2 *__restrict__ L, int ncut, int nd, int npw, int nexp) {
-  const size_t per = (size_t)nd * nexp;
-  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= per * ncut) return;
+struct TrArgs {
+  const double2 *M;
+  const int *pw_begin, *pw_src, *pw_ind;
+  const double2 *W;
+  const double *kscale;
+  double2 *L;
+  int ncut, nd, npw, nexp;
+};
+// a single plan (descs null, block b of `one`) or a batch (block b = block
+// work[b].y of plan work[b].x)
+struct TrLaunch {
+  TrArgs one;
+  const TrArgs *descs;
+  const int2 *work;
+};
+
+constexpr int kTrThreads = 256;
+
+__global__ void __launch_bounds__(kTrThreads) k_translate(const __grid_constant__ TrLaunch lp) {
+  const TrArgs &a = lp.descs ? lp.descs[lp.work[blockIdx.x].x] : lp.one;
+  const int blk = lp.descs ? lp.work[blockIdx.x].y : (int)blockIdx.x;
+  const int nexp = a.nexp;
+  const size_t per = (size_t)a.nd * nexp;
+  const size_t idx = (size_t)blk * blockDim.x + threadIdx.x;
+  if (idx >= per * a.ncut) return;
   const int icut = (int)(idx / per);
   const size_t r = idx - (size_t)icut * per;
   const int e = (int)(r % nexp);
-  double2 s = M[idx];
-  for (int j = pw_begin[icut]; j < pw_begin[icut + 1]; j++) {
-    const double2 m = M[(size_t)pw_src[j] * per + r];
-    const double2 w = W[(size_t)pw_ind[j] * nexp + e];
+  double2 s = a.M[idx];
+  for (int j = a.pw_begin[icut]; j < a.pw_begin[icut + 1]; j++) {
+    const double2 m = a.M[(size_t)a.pw_src[j] * per + r];
+    const double2 w = a.W[(size_t)a.pw_ind[j] * nexp + e];
     s.x += m.x * w.x - m.y * w.y;
     s.y += m.x * w.y + m.y * w.x;
   }
-  if (kscale) {
-    const double f = kscale[e / npw];
+  if (a.kscale) {
+    const double f = a.kscale[e / a.npw];
     s.x *= f;
     s.y *= f;
   }
-  L[idx] = s;
+  a.L[idx] = s;
 }
 
 template <int TM, int TN, int NT>
@@ -406,25 +425,37 @@ void set_smem_attrs(int bytes) {
 }
 
 struct NearArgs {
-  const double *fvals;
-  double *pot;
   const int *target, *begin, *src;
   const int2 *ixy;  // per entry: table slots (level * 13 + offset + 6) in x and y
   const double *tab_loc;
   const int *ind_loc;
   int ntarget, nd, n;
+  long long elem_off;  // start of this plan's leaf arrays in the (packed) fvals/pot
+};
+// a single plan (descs null, block b takes targets kWarps b..) or a batch
+// (block b takes targets work[b].y.. of plan work[b].x)
+struct NearLaunch {
+  NearArgs one;
+  const NearArgs *descs;
+  const int2 *work;
+  const double *fbase;
+  double *pbase;
 };
 
 // One warp per near-field target leaf; pot(k1,k2) += sum over its list1
 // entries of Ty^T (Tx^T F) on the banded 1D tables of each entry's slots
 // (the forward pass uses the target's level, the transposed pass the level
 // of the forward target).
-__global__ void __launch_bounds__(kWarps * 32) k_near_fp64(NearArgs a) {
+__global__ void __launch_bounds__(kWarps * 32) k_near_fp64(const __grid_constant__ NearLaunch lp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const NearArgs &a = lp.descs ? lp.descs[lp.work[blockIdx.x].x] : lp.one;
+  const int first = lp.descs ? lp.work[blockIdx.x].y : (int)blockIdx.x * kWarps;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int t = blockIdx.x * kWarps + warp;
+  const int t = first + warp;
   if (t >= a.ntarget) return;
   const int n = a.n, npb = n * n, nd = a.nd;
+  const double *fvals = lp.fbase + a.elem_off;
+  double *pot = lp.pbase + a.elem_off;
   double *wb = reinterpret_cast<double *>(smem_raw) + (size_t)warp * 3 * npb;
   double *sF = wb, *sff = wb + npb, *sP = wb + 2 * npb;
   const int tb = a.target[t];
@@ -441,7 +472,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_near_fp64(NearArgs a) {
       if (kx1 - kx0 + 1 == 0 || ky1 - ky0 + 1 == 0) continue;
       const double *tx = tl + (size_t)npb * ix;
       const double *ty = tl + (size_t)npb * iy;
-      const double *fv = a.fvals + (size_t)sb * nd * npb;
+      const double *fv = fvals + (size_t)sb * nd * npb;
       __syncwarp();
       for (int o = lane; o < npb; o += 32) sF[o] = fv[ind + (size_t)nd * o];
       __syncwarp();
@@ -465,7 +496,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_near_fp64(NearArgs a) {
       }
     }
     __syncwarp();
-    double *pb = a.pot + (size_t)tb * nd * npb;
+    double *pb = pot + (size_t)tb * nd * npb;
     for (int o = lane; o < npb; o += 32) pb[ind + (size_t)nd * o] += sP[o];
     __syncwarp();
   }
@@ -674,75 +705,103 @@ void device_plan_destroy(DevicePlan &dp) {
   dp = DevicePlan();
 }
 
-int device_plan_reserve_events(DevicePlan &dp, int n) {
-  while ((int)dp.evsets.size() < n) {
+int reserve_event_sets(std::vector<std::array<cudaEvent_t, 6>> &evsets, int n) {
+  while ((int)evsets.size() < n) {
     std::array<cudaEvent_t, 6> es;
     for (auto &e : es)
       if (cudaEventCreate(&e) != cudaSuccess) return BFGT_ERR_CUDA;
-    dp.evsets.push_back(es);
+    evsets.push_back(es);
   }
   return BFGT_OK;
 }
 
-int device_plan_stage_ms(DevicePlan &dp, double *out) {
+int read_stage_ms(std::vector<std::array<cudaEvent_t, 6>> &evsets, int &nrec, double *out) {
   for (int i = 0; i < 8; i++) out[i] = 0;
-  if (dp.nrec == 0) return BFGT_OK;
-  const int nr = std::min<int>(dp.nrec, (int)dp.evsets.size());
-  if (cudaEventSynchronize(dp.evsets[nr - 1][5]) != cudaSuccess) return BFGT_ERR_CUDA;
+  if (nrec == 0) return BFGT_OK;
+  const int nr = std::min<int>(nrec, (int)evsets.size());
+  if (cudaEventSynchronize(evsets[nr - 1][5]) != cudaSuccess) return BFGT_ERR_CUDA;
   for (int r = 0; r < nr; r++) {
     float ms;
     for (int i = 0; i < 5; i++)
-      if (cudaEventElapsedTime(&ms, dp.evsets[r][i], dp.evsets[r][i + 1]) == cudaSuccess) out[i] += ms;
-    if (cudaEventElapsedTime(&ms, dp.evsets[r][0], dp.evsets[r][5]) == cudaSuccess) out[5] += ms;
+      if (cudaEventElapsedTime(&ms, evsets[r][i], evsets[r][i + 1]) == cudaSuccess) out[i] += ms;
+    if (cudaEventElapsedTime(&ms, evsets[r][0], evsets[r][5]) == cudaSuccess) out[5] += ms;
   }
   out[6] = nr;
-  dp.nrec = 0;
+  nrec = 0;
   cudaGetLastError();
   return BFGT_OK;
 }
 
-int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cudaStream_t s, std::string &msg) {
-  const int nthreads = kWarps * 32;
-  cudaEvent_t *ev = nullptr;
-  if (dp.events) {
-    if (dp.nrec >= (int)dp.evsets.size() && dp.evsets.size() < 65536) device_plan_reserve_events(dp, dp.nrec + 1);
-    ev = dp.evsets[dp.nrec % dp.evsets.size()].data();
-    dp.nrec++;
+int device_plan_reserve_events(DevicePlan &dp, int n) { return reserve_event_sets(dp.evsets, n); }
+
+int device_plan_stage_ms(DevicePlan &dp, double *out) { return read_stage_ms(dp.evsets, dp.nrec, out); }
+
+namespace {
+
+TrArgs tr_args(const DevicePlan &dp) {
+  return TrArgs{dp.M, dp.cut_pw_begin, dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.kscale, dp.L, dp.ncut, dp.nd, dp.npw,
+                dp.nexp};
+}
+
+NearArgs near_args(const DevicePlan &dp, long long elem_off) {
+  return NearArgs{dp.nf_target, dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.nnf, dp.nd, dp.n,
+                  elem_off};
+}
+
+bool has_pw(const DevicePlan &dp) { return !dp.direct_only && dp.nchunks > 0; }
+
+// steps 1+2 (leaf values -> cutoff expansions, merge fused) of one plan
+void plan_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
+  if (dp.precision == BFGT_PREC_SPLIT) {
+    split_form(dp, d_fvals, s);
+  } else {
+    FormArgs fa{d_fvals, dp.leaves, dp.columns, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, reduce_args(dp),
+                dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
+    launch_form_fp64(TileChoice{dp.form_tile[0], dp.form_tile[1], dp.form_tile[2]}, dp.nchunks, dp.smem_form, s, fa);
   }
+}
+
+// steps 4+5 (cutoff expansions -> leaf values, split fused) of one plan
+void plan_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
+  if (dp.precision == BFGT_PREC_SPLIT) {
+    split_eval(dp, d_pot, s);
+  } else {
+    EvalArgs ea{d_pot, dp.leaves, dp.columns, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n,
+                dp.npw, dp.hh, dp.nexp};
+    launch_eval_fp64(TileChoice{dp.eval_tile[0], dp.eval_tile[1], dp.eval_tile[2]}, dp.nchunks, dp.smem_eval, s, ea);
+  }
+}
+
+cudaEvent_t *next_events(std::vector<std::array<cudaEvent_t, 6>> &evsets, int &nrec, bool on) {
+  if (!on) return nullptr;
+  if (nrec >= (int)evsets.size() && evsets.size() < 65536) reserve_event_sets(evsets, nrec + 1);
+  cudaEvent_t *ev = evsets[nrec % evsets.size()].data();
+  nrec++;
+  return ev;
+}
+
+}  // namespace
+
+int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cudaStream_t s, std::string &msg) {
+  cudaEvent_t *ev = next_events(dp.evsets, dp.nrec, dp.events);
   if (ev) cudaEventRecord(ev[0], s);
-  if (!dp.direct_only && dp.nchunks > 0) {
-    if (dp.precision == BFGT_PREC_SPLIT) {
-      split_form(dp, d_fvals, s);
-    } else {
-      FormArgs fa{d_fvals, dp.leaves, dp.columns, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, reduce_args(dp),
-                  dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
-      launch_form_fp64(TileChoice{dp.form_tile[0], dp.form_tile[1], dp.form_tile[2]}, dp.nchunks, dp.smem_form, s, fa);
-    }
+  if (has_pw(dp)) {
+    plan_form(dp, d_fvals, s);
     // the merge to the cutoff level finishes inside the form kernels
     if (ev) cudaEventRecord(ev[1], s);
     if (ev) cudaEventRecord(ev[2], s);
-    {
-      const size_t tot = (size_t)dp.ncut * dp.nd * dp.nexp;
-      k_translate<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(dp.M, dp.cut_pw_begin, dp.cut_pw_src, dp.cut_pw_ind,
-                                                                 dp.W, dp.kscale, dp.L, dp.ncut, dp.nd, dp.npw, dp.nexp);
-    }
+    const size_t tot = (size_t)dp.ncut * dp.nd * dp.nexp;
+    k_translate<<<(unsigned)((tot + kTrThreads - 1) / kTrThreads), kTrThreads, 0, s>>>(
+        TrLaunch{tr_args(dp), nullptr, nullptr});
     if (ev) cudaEventRecord(ev[3], s);
-    if (dp.precision == BFGT_PREC_SPLIT) {
-      split_eval(dp, d_pot, s);
-    } else {
-      EvalArgs ea{d_pot, dp.leaves, dp.columns, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n,
-                  dp.npw, dp.hh, dp.nexp};
-      launch_eval_fp64(TileChoice{dp.eval_tile[0], dp.eval_tile[1], dp.eval_tile[2]}, dp.nchunks, dp.smem_eval, s, ea);
-    }
+    plan_eval(dp, d_pot, s);
     if (ev) cudaEventRecord(ev[4], s);
   } else if (ev) {
     for (int i = 1; i <= 4; i++) cudaEventRecord(ev[i], s);
   }
-  if (dp.nnf > 0) {
-    NearArgs na{d_fvals, d_pot, dp.nf_target, dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.nnf,
-                dp.nd, dp.n};
-    k_near_fp64<<<(dp.nnf + kWarps - 1) / kWarps, nthreads, dp.smem_near, s>>>(na);
-  }
+  if (dp.nnf > 0)
+    k_near_fp64<<<(dp.nnf + kWarps - 1) / kWarps, kWarps * 32, dp.smem_near, s>>>(
+        NearLaunch{near_args(dp, 0), nullptr, nullptr, d_fvals, d_pot});
   if (ev) cudaEventRecord(ev[5], s);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -750,6 +809,96 @@ int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cu
     return BFGT_ERR_CUDA;
   }
   return BFGT_OK;
+}
+
+int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, std::string &msg) {
+  device_batch_destroy(b);
+  b.plans = plans;
+  b.offs.assign(plans.size() + 1, 0);
+  for (size_t i = 0; i < plans.size(); i++)
+    b.offs[i + 1] = b.offs[i] + (long long)plans[i]->nd * plans[i]->n * plans[i]->n * plans[i]->nboxes;
+  int rc = split_batch_create(b.split, plans, b.offs, msg);
+  if (rc != BFGT_OK) return rc;
+  std::vector<TrArgs> tr;
+  std::vector<NearArgs> nf;
+  std::vector<int2> trw, nfw;
+  for (size_t i = 0; i < plans.size(); i++) {
+    const DevicePlan &dp = *plans[i];
+    tr.push_back(tr_args(dp));
+    nf.push_back(near_args(dp, b.offs[i]));
+    if (has_pw(dp)) {
+      const size_t tot = (size_t)dp.ncut * dp.nd * dp.nexp;
+      for (size_t k = 0; k < (tot + kTrThreads - 1) / kTrThreads; k++) trw.push_back(make_int2((int)i, (int)k));
+    }
+    for (int t = 0; t < dp.nnf; t += kWarps) nfw.push_back(make_int2((int)i, t));
+    b.smem_near = std::max(b.smem_near, dp.smem_near);
+  }
+  b.tr_blocks = (int)trw.size();
+  b.nf_blocks = (int)nfw.size();
+  TrArgs *dtr = nullptr;
+  NearArgs *dnf = nullptr;
+  auto chk = [&](int r) {
+    if (rc == BFGT_OK && r != BFGT_OK) rc = r;
+  };
+  chk(upload(dtr, tr, msg));
+  chk(upload(dnf, nf, msg));
+  chk(upload(b.tr_work, trw, msg));
+  chk(upload(b.nf_work, nfw, msg));
+  b.tr_descs = dtr;
+  b.nf_descs = dnf;
+  if (rc == BFGT_OK) {
+    b.events = true;
+    reserve_event_sets(b.evsets, 8);
+  }
+  return rc;
+}
+
+int device_batch_launches(const DeviceBatch &b) {
+  int n = split_batch_launches(b.split) + (b.tr_blocks > 0) + (b.nf_blocks > 0);
+  for (const DevicePlan *dp : b.plans)
+    if (dp->precision != BFGT_PREC_SPLIT && has_pw(*dp)) n += 2;
+  return n;
+}
+
+int device_batch_execute(DeviceBatch &b, const double *d_fvals, double *d_pot, cudaStream_t s, std::string &msg) {
+  cudaEvent_t *ev = next_events(b.evsets, b.nrec, b.events);
+  if (ev) cudaEventRecord(ev[0], s);
+  split_batch_form(b.split, d_fvals, s);
+  for (size_t i = 0; i < b.plans.size(); i++)
+    if (b.plans[i]->precision != BFGT_PREC_SPLIT && has_pw(*b.plans[i])) plan_form(*b.plans[i], d_fvals + b.offs[i], s);
+  if (ev) cudaEventRecord(ev[1], s);
+  if (ev) cudaEventRecord(ev[2], s);
+  if (b.tr_blocks > 0)
+    k_translate<<<b.tr_blocks, kTrThreads, 0, s>>>(TrLaunch{TrArgs{}, static_cast<const TrArgs *>(b.tr_descs), b.tr_work});
+  if (ev) cudaEventRecord(ev[3], s);
+  split_batch_eval(b.split, d_pot, s);
+  for (size_t i = 0; i < b.plans.size(); i++)
+    if (b.plans[i]->precision != BFGT_PREC_SPLIT && has_pw(*b.plans[i])) plan_eval(*b.plans[i], d_pot + b.offs[i], s);
+  if (ev) cudaEventRecord(ev[4], s);
+  if (b.nf_blocks > 0)
+    k_near_fp64<<<b.nf_blocks, kWarps * 32, b.smem_near, s>>>(
+        NearLaunch{NearArgs{}, static_cast<const NearArgs *>(b.nf_descs), b.nf_work, d_fvals, d_pot});
+  if (ev) cudaEventRecord(ev[5], s);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    msg = std::string("kernel launch failed: ") + cudaGetErrorString(e);
+    return BFGT_ERR_CUDA;
+  }
+  return BFGT_OK;
+}
+
+int device_batch_stage_ms(DeviceBatch &b, double *out) { return read_stage_ms(b.evsets, b.nrec, out); }
+
+void device_batch_destroy(DeviceBatch &b) {
+  if (b.graph_exec) cudaGraphExecDestroy(b.graph_exec);
+  if (b.graph) cudaGraphDestroy(b.graph);
+  split_batch_destroy(b.split);
+  void *ptrs[] = {b.tr_descs, b.nf_descs, b.tr_work, b.nf_work};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (auto &es : b.evsets)
+    for (cudaEvent_t e : es) cudaEventDestroy(e);
+  b = DeviceBatch();
 }
 
 }  // namespace bfgt

@@ -43,7 +43,6 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
 }
 
 struct FormTcArgs {
-  const double *fvals;
   const int4 *chunks;      // {column begin, column end, icut, level}
   const int *step_begin;   // nchunks + 1
   const int *steps;        // stride 1 + cpc: oy, then box per slot (-1: no leaf)
@@ -59,15 +58,43 @@ struct FormTcArgs {
   int *err;
   int nd, n, npw, hh, nexp, cpc, NP, KA;
   uint32_t wait_iters;
+  long long elem_off;      // start of this plan's leaf arrays in the (packed) fvals
 };
 
-template <int NT>
-__global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
+// One launch of the form kernel: a single plan (descs null, CTA b = chunk b of
+// `one`), or a batch of plans (CTA b = chunk work[b].y of plan work[b].x).
+struct FormTcLaunch {
+  FormTcArgs one;
+  const FormTcArgs *descs;
+  const int2 *work;
+  const double *fbase;
+};
+
+// Copies this CTA's plan descriptor into shared memory and returns its chunk.
+template <typename Args, typename Launch>
+__device__ __forceinline__ int load_desc(const Launch &lp, Args &dst, int *s_item) {
+  const Args *src = lp.descs ? lp.descs + lp.work[blockIdx.x].x : &lp.one;
+  for (int i = threadIdx.x; i < (int)(sizeof(Args) / 4); i += blockDim.x)
+    reinterpret_cast<int *>(&dst)[i] = reinterpret_cast<const int *>(src)[i];
+  if (threadIdx.x == 0) *s_item = lp.descs ? lp.work[blockIdx.x].y : (int)blockIdx.x;
+  __syncthreads();
+  return *s_item;
+}
+
+// kBatch: the arguments come from the per-plan descriptors (copied to shared
+// memory) instead of the launch's own parameter block.
+template <int NT, bool kBatch>
+__global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ FormTcLaunch lp) {
   extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ FormTcArgs s_desc;
+  __shared__ int s_item;
+  const int chunk = kBatch ? load_desc(lp, s_desc, &s_item) : (int)blockIdx.x;
+  const FormTcArgs &a = kBatch ? s_desc : lp.one;
+  const double *fvals = lp.fbase + a.elem_off;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);  // [0],[1] operand buffers, [2] drain
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 64);
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int4 ch = a.chunks[blockIdx.x];
+  const int4 ch = a.chunks[chunk];
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, NP = a.NP, KA = a.KA;
   const int ncol = ch.y - ch.x;
   const int abytes = 3 * kRows * KA * 2, bbytes = 3 * NP * KA * 2, bufbytes = abytes + bbytes;
@@ -96,7 +123,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
   const uint32_t tmem = *tmem_slot;
   const uint32_t tD0 = tmem, tD1 = tmem + (uint32_t)NP;
   const uint32_t idesc = tc::idesc_bf16_f32(kRows, NP);
-  const int sb = a.step_begin[blockIdx.x], se = a.step_begin[blockIdx.x + 1], nsteps = se - sb;
+  const int sb = a.step_begin[chunk], se = a.step_begin[chunk + 1], nsteps = se - sb;
   const int stride = 1 + cpc;
   const uint16_t *tyb = a.TyB + a.tyb_off[ch.w];
   bool ok = true;
@@ -113,7 +140,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
     auto load_step = [&](int s2) {
       const int *st2 = a.steps + (size_t)(sb + s2) * stride;
       const int box = st2[1 + rslot];
-      const double *fv = a.fvals + (size_t)(box < 0 ? 0 : box) * nd * npb + ind + (size_t)nd * rm1;
+      const double *fv = fvals + (size_t)(box < 0 ? 0 : box) * nd * npb + ind + (size_t)nd * rm1;
 #pragma unroll
       for (int k = 0; k < 16; k++) fnext[k] = (box >= 0 && k < n) ? fv[(size_t)nd * n * k] : 0.0;
       const uint4 *src = reinterpret_cast<const uint4 *>(tyb + (size_t)st2[0] * a.tyb_tile);
@@ -210,7 +237,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
     // x contraction (FP64): M(k1,k2) = sum_{slot,m1} T(m1,k1) conj(ph_ox(k1)) Y(slot,m1,k2)
     {
       const int ntm = (npw + 1) / 2, ntn = (hh + 3) / 4, ntiles = ntm * ntn;
-      double2 *out = a.Mpart + ((size_t)blockIdx.x * nd + ind) * a.nexp;
+      double2 *out = a.Mpart + ((size_t)chunk * nd + ind) * a.nexp;
 #pragma unroll
       for (int t = 0; t < NT; t++) {
         const int tile = tid + kThreads * t;
@@ -261,11 +288,10 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(FormTcArgs a) {
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tmem, 128);
-  finish_cutoff_box(a.red, blockIdx.x, nd, a.nexp, reinterpret_cast<int *>(smem + 68));
+  finish_cutoff_box(a.red, chunk, nd, a.nexp, reinterpret_cast<int *>(smem + 68));
 }
 
 struct EvalTcArgs {
-  double *pot;
   const int4 *chunks;
   const int *step_begin;
   const int *steps;
@@ -280,6 +306,14 @@ struct EvalTcArgs {
   int *err;
   int nd, n, npw, hh, nexp, cpc, NB, KE, KH;
   uint32_t wait_iters;
+  long long elem_off;      // start of this plan's leaf arrays in the (packed) pot
+};
+
+struct EvalTcLaunch {
+  EvalTcArgs one;
+  const EvalTcArgs *descs;
+  const int2 *work;
+  double *pbase;
 };
 
 // Steps of a chunk per tensor-core group in the eval kernel: the group's B
@@ -295,13 +329,18 @@ constexpr int kEvalThreads = 256;
 // previous group is read out), 18 MMAs with N = 16 x steps produce the values
 // of every leaf of the group, and the readout adds 2 (D0 + D1) into pot.
 // Warps w and w+4 share TMEM lanes 32 (w%4).. and split the group's steps.
-template <int NNT>
-__global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(EvalTcArgs a) {
+template <int NNT, bool kBatch>
+__global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_constant__ EvalTcLaunch lp) {
   extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ EvalTcArgs s_desc;
+  __shared__ int s_item;
+  const int chunk = kBatch ? load_desc(lp, s_desc, &s_item) : (int)blockIdx.x;
+  const EvalTcArgs &a = kBatch ? s_desc : lp.one;
+  double *pot = lp.pbase + a.elem_off;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);  // [0] MMA group done, [1] drain
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 64);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int4 ch = a.chunks[blockIdx.x];
+  const int4 ch = a.chunks[chunk];
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, KE = a.KE, KH = a.KH;
   const int ncol = ch.y - ch.x;
   const int abytes = 3 * kRows * KE * 2, bbytes = 3 * (16 * kEvalBatch) * KE * 2;
@@ -317,7 +356,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(EvalTcArgs a) {
     tc::mbar_init(&mbar[1], 1);
     tc::fence_mbar_init();
   }
-  const int sb = a.step_begin[blockIdx.x], se = a.step_begin[blockIdx.x + 1], nsteps = se - sb;
+  const int sb = a.step_begin[chunk], se = a.step_begin[chunk + 1], nsteps = se - sb;
   const int stride = 1 + cpc;
   const uint16_t *eyb = a.EyB + a.eyb_off[ch.w];
   const int nbatch = (nsteps + kEvalBatch - 1) / kEvalBatch;
@@ -479,7 +518,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(EvalTcArgs a) {
         double *pb = nullptr;
         auto load_pot = [&](int st) {
           const int box = st < S ? a.steps[(size_t)(sb + s0 + st) * stride + 1 + rslot] : -1;
-          pb = box >= 0 ? a.pot + (size_t)box * nd * npb + ind + (size_t)nd * rk1 : nullptr;
+          pb = box >= 0 ? pot + (size_t)box * nd * npb + ind + (size_t)nd * rk1 : nullptr;
 #pragma unroll
           for (int k2 = 0; k2 < 16; k2++) pv[k2] = (pb && k2 < n) ? pb[(size_t)nd * n * k2] : 0.0;
         };
@@ -511,6 +550,18 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(EvalTcArgs a) {
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tmem, 256);
+}
+
+// Opts every kernel variant into the full dynamic shared memory (per device;
+// cheap to repeat).
+void set_split_smem_attrs() {
+#define SMEM_ATTR(K) cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  SMEM_ATTR((k_form_tc<1, false>)) SMEM_ATTR((k_form_tc<1, true>))
+  SMEM_ATTR((k_form_tc<2, false>)) SMEM_ATTR((k_form_tc<2, true>))
+#define SMEM_EVAL(X) SMEM_ATTR((k_eval_tc<X, false>)) SMEM_ATTR((k_eval_tc<X, true>))
+  SMEM_EVAL(1) SMEM_EVAL(2) SMEM_EVAL(3) SMEM_EVAL(4) SMEM_EVAL(5) SMEM_EVAL(6) SMEM_EVAL(7) SMEM_EVAL(8)
+#undef SMEM_EVAL
+#undef SMEM_ATTR
 }
 
 // ---- host-side table preparation -----------------------------------------
@@ -702,16 +753,7 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     msg = "split precision: shared memory need exceeds 227 KB";
     return BFGT_ERR_CAPACITY;
   }
-  cudaFuncSetAttribute(k_form_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  cudaFuncSetAttribute(k_form_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  cudaFuncSetAttribute(k_eval_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  cudaFuncSetAttribute(k_eval_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  cudaFuncSetAttribute(k_eval_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  cudaFuncSetAttribute(k_eval_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  cudaFuncSetAttribute(k_eval_tc<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  cudaFuncSetAttribute(k_eval_tc<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  cudaFuncSetAttribute(k_eval_tc<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  cudaFuncSetAttribute(k_eval_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  set_split_smem_attrs();
   sp.wait_iters = kWaitIters;
   // tensor-core FLOP issued per transform (every slice product counted)
   const double nsteps_total = (double)(steps.size() / (1 + sp.cpc));
@@ -728,26 +770,136 @@ void split_plan_destroy(DevicePlan &dp) {
   sp = SplitPlan();
 }
 
-void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
-  SplitPlan &sp = dp.split;
-  FormTcArgs a{d_fvals, sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.TyB, sp.tyb_off, sp.tyb_tile, dp.T,
-               dp.PH, dp.ph_off, dp.Mpart, reduce_args(dp), sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc,
-               sp.NP, sp.KA, sp.wait_iters};
-  if (sp.nt == 1) k_form_tc<1><<<sp.nchunks, kThreads, sp.smem_form, s>>>(a);
-  else k_form_tc<2><<<sp.nchunks, kThreads, sp.smem_form, s>>>(a);
+namespace {
+
+FormTcArgs form_args(const DevicePlan &dp, long long elem_off) {
+  const SplitPlan &sp = dp.split;
+  return FormTcArgs{sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.TyB, sp.tyb_off, sp.tyb_tile, dp.T, dp.PH,
+                    dp.ph_off, dp.Mpart, reduce_args(dp), sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc,
+                    sp.NP, sp.KA, sp.wait_iters, elem_off};
 }
 
-void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
-  SplitPlan &sp = dp.split;
-  EvalTcArgs a{d_pot, sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, dp.E,
-               dp.PH, dp.ph_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
-               sp.wait_iters};
-  switch ((dp.hh + 3) / 4) {
-#define EVAL_NNT(X) \
-  case X: k_eval_tc<X><<<sp.nchunks, kEvalThreads, sp.smem_eval, s>>>(a); break;
+EvalTcArgs eval_args(const DevicePlan &dp, long long elem_off) {
+  const SplitPlan &sp = dp.split;
+  return EvalTcArgs{sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, dp.E, dp.PH,
+                    dp.ph_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
+                    sp.wait_iters, elem_off};
+}
+
+void launch_form(int nt, int grid, size_t smem, cudaStream_t s, const FormTcLaunch &lp) {
+  if (grid <= 0) return;
+  const bool b = lp.descs != nullptr;
+  if (nt == 1) {
+    if (b) k_form_tc<1, true><<<grid, kThreads, smem, s>>>(lp);
+    else k_form_tc<1, false><<<grid, kThreads, smem, s>>>(lp);
+  } else {
+    if (b) k_form_tc<2, true><<<grid, kThreads, smem, s>>>(lp);
+    else k_form_tc<2, false><<<grid, kThreads, smem, s>>>(lp);
+  }
+}
+
+void launch_eval(int nnt, int grid, size_t smem, cudaStream_t s, const EvalTcLaunch &lp) {
+  if (grid <= 0) return;
+  const bool b = lp.descs != nullptr;
+  switch (nnt) {
+#define EVAL_NNT(X)                                                         \
+  case X:                                                                   \
+    if (b) k_eval_tc<X, true><<<grid, kEvalThreads, smem, s>>>(lp);         \
+    else k_eval_tc<X, false><<<grid, kEvalThreads, smem, s>>>(lp);          \
+    break;
     EVAL_NNT(1) EVAL_NNT(2) EVAL_NNT(3) EVAL_NNT(4) EVAL_NNT(5) EVAL_NNT(6) EVAL_NNT(7) EVAL_NNT(8)
 #undef EVAL_NNT
   }
+}
+
+}  // namespace
+
+void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
+  FormTcLaunch lp{form_args(dp, 0), nullptr, nullptr, d_fvals};
+  launch_form(dp.split.nt, dp.split.nchunks, dp.split.smem_form, s, lp);
+}
+
+void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
+  EvalTcLaunch lp{eval_args(dp, 0), nullptr, nullptr, d_pot};
+  launch_eval((dp.hh + 3) / 4, dp.split.nchunks, dp.split.smem_eval, s, lp);
+}
+
+int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, const std::vector<long long> &offs,
+                       std::string &msg) {
+  split_batch_destroy(b);
+  std::vector<FormTcArgs> fd;
+  std::vector<EvalTcArgs> ed;
+  // one work item per chunk, grouped by kernel variant (tile count of the
+  // form kernel, column-tile count of the eval kernel); within a group the
+  // plans keep their order
+  std::vector<std::vector<int2>> fw(3), ew(9);
+  std::vector<size_t> fsm(3, 0), esm(9, 0);
+  for (size_t i = 0; i < plans.size(); i++) {
+    DevicePlan &dp = *plans[i];
+    fd.push_back(form_args(dp, offs[i]));
+    ed.push_back(eval_args(dp, offs[i]));
+    if (dp.precision != BFGT_PREC_SPLIT || dp.direct_only) continue;
+    const int nt = dp.split.nt, nnt = (dp.hh + 3) / 4;
+    for (int c = 0; c < dp.split.nchunks; c++) {
+      fw[nt].push_back(make_int2((int)i, c));
+      ew[nnt].push_back(make_int2((int)i, c));
+    }
+    fsm[nt] = std::max(fsm[nt], dp.split.smem_form);
+    esm[nnt] = std::max(esm[nnt], dp.split.smem_eval);
+  }
+  std::vector<int2> fall, eall;
+  for (int v = 1; v <= 2; v++)
+    if (!fw[v].empty()) {
+      b.form_groups.push_back(SplitBatch::Group{v, (int)fall.size(), (int)fw[v].size(), fsm[v]});
+      fall.insert(fall.end(), fw[v].begin(), fw[v].end());
+    }
+  for (int v = 1; v <= 8; v++)
+    if (!ew[v].empty()) {
+      b.eval_groups.push_back(SplitBatch::Group{v, (int)eall.size(), (int)ew[v].size(), esm[v]});
+      eall.insert(eall.end(), ew[v].begin(), ew[v].end());
+    }
+  int rc = BFGT_OK;
+  auto chk = [&](int x) {
+    if (rc == BFGT_OK && x != BFGT_OK) rc = x;
+  };
+  FormTcArgs *dfd = nullptr;
+  EvalTcArgs *ded = nullptr;
+  chk(upload_vec(dfd, fd, msg));
+  chk(upload_vec(ded, ed, msg));
+  chk(upload_vec(b.form_work, fall, msg));
+  chk(upload_vec(b.eval_work, eall, msg));
+  b.form_descs = dfd;
+  b.eval_descs = ded;
+  return rc;
+}
+
+void split_batch_form(const SplitBatch &b, const double *fbase, cudaStream_t s) {
+  for (const SplitBatch::Group &g : b.form_groups) {
+    FormTcLaunch lp{};
+    lp.descs = static_cast<const FormTcArgs *>(b.form_descs);
+    lp.work = b.form_work + g.begin;
+    lp.fbase = fbase;
+    launch_form(g.variant, g.count, g.smem, s, lp);
+  }
+}
+
+void split_batch_eval(const SplitBatch &b, double *pbase, cudaStream_t s) {
+  for (const SplitBatch::Group &g : b.eval_groups) {
+    EvalTcLaunch lp{};
+    lp.descs = static_cast<const EvalTcArgs *>(b.eval_descs);
+    lp.work = b.eval_work + g.begin;
+    lp.pbase = pbase;
+    launch_eval(g.variant, g.count, g.smem, s, lp);
+  }
+}
+
+int split_batch_launches(const SplitBatch &b) { return (int)(b.form_groups.size() + b.eval_groups.size()); }
+
+void split_batch_destroy(SplitBatch &b) {
+  void *ptrs[] = {b.form_descs, b.eval_descs, b.form_work, b.eval_work};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  b = SplitBatch();
 }
 
 unsigned int split_default_wait_iters() { return kWaitIters; }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "device_plan.hpp"
 #include "fgt_common.cuh"
@@ -18,6 +19,25 @@ void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s);
 // cutoff expansions -> leaf values, accumulated into pot (same as k_eval_fp64)
 void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s);
 void split_plan_destroy(DevicePlan &dp);
+
+// Work lists of a batch of plans whose form and eval stages run as one launch
+// per kernel variant (all chunks of all split plans in the batch).
+struct SplitBatch {
+  struct Group {
+    int variant, begin, count;
+    size_t smem;
+  };
+  void *form_descs = nullptr, *eval_descs = nullptr;  // per-plan kernel arguments (device)
+  int2 *form_work = nullptr, *eval_work = nullptr;     // {plan, chunk}, grouped by variant
+  std::vector<Group> form_groups, eval_groups;
+};
+// offs[i]: element offset of plan i's arrays in the packed fvals/pot
+int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, const std::vector<long long> &offs,
+                       std::string &msg);
+void split_batch_form(const SplitBatch &b, const double *fbase, cudaStream_t s);
+void split_batch_eval(const SplitBatch &b, double *pbase, cudaStream_t s);
+int split_batch_launches(const SplitBatch &b);
+void split_batch_destroy(SplitBatch &b);
 // Reads and clears the device error flag of the tensor-core kernels (waits
 // for the device); BFGT_ERR_TIMEOUT if a bounded wait gave up.
 int split_check(DevicePlan &dp);

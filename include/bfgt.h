@@ -171,6 +171,38 @@ int bfgt_plan_set_wait_limit(bfgt_plan plan, unsigned int polls);
 
 int bfgt_plan_destroy(bfgt_plan plan);
 
+/* ---- batches of plans --------------------------------------------------- */
+/* No counterpart in the reference: its solvers call boxfgt once per density,
+   species and time node with its own delta (hpots/hpots2dadap.f:329-346,
+   4018-4102).  A batch runs the transforms of several plans (independent
+   trees, deltas, eps, orders, nd) together: the split-precision form and eval
+   stages of all plans go through one launch per kernel variant driven by a
+   device-side list of (plan, chunk) work items, and the cutoff translations
+   and the near field of all plans through one launch each; FP64 plans run
+   their form and eval stages as launches of their own.  The plans must stay
+   alive (and on the current device) while the batch exists.  The leaf arrays
+   are packed: plan i's fvals(nd_i,norder_i**2,nboxes_i) and pot start at
+   element offsets[i] of the batch arrays (bfgt_batch_layout). */
+typedef struct bfgt_batch_s *bfgt_batch;
+int bfgt_batch_create(bfgt_batch *batch, int nplans, const bfgt_plan *plans);
+/* offsets: nplans + 1 element offsets (the last is the packed length). */
+int bfgt_batch_layout(bfgt_batch batch, int64_t *offsets);
+/* pot += K_i fvals for every plan i, on the packed device arrays; asynchronous. */
+int bfgt_batch_execute(bfgt_batch batch, const double *d_fvals, double *d_pot, void *stream);
+/* Capture bfgt_batch_execute for these buffers into a CUDA graph / replay it. */
+int bfgt_batch_graph_capture(bfgt_batch batch, const double *d_fvals, double *d_pot, void *stream);
+int bfgt_batch_graph_launch(bfgt_batch batch, void *stream);
+/* Stage milliseconds summed over the executes since the last call, as
+   bfgt_plan_stage_ms. */
+int bfgt_batch_stage_ms(bfgt_batch batch, double *out);
+/* out[0]=plans, out[1]=kernel launches per execute, out[2]/out[3]=form/eval
+   work items (chunks), out[4]=translation blocks, out[5]=near-field blocks.
+   out must hold 8. */
+int bfgt_batch_info(bfgt_batch batch, int *out);
+/* bfgt_plan_check on every plan of the batch. */
+int bfgt_batch_check(bfgt_batch batch);
+int bfgt_batch_destroy(bfgt_batch batch);
+
 /* ---- host-side plan introspection (no device needed) ------------------- */
 /* Builds only the host half of a plan (tables and lists) and copies out the
    interaction lists and near-field band patterns so that they can be compared

@@ -165,6 +165,111 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def make_uneven_trees(seed, ntrees=64, lo=1000, hi=50000):
+    """Uneven-trees workload: order-8 periodic trees whose leaf counts follow
+    targets drawn log-uniform in [lo, hi], each a sum of 5-30 Gaussians (widths
+    log-uniform in [2e-3, 5e-2], N(0,1) amplitudes); delta log-uniform in
+    [1e-5, 1e-1] per tree.  A tree is refined uniformly to level L or L+1
+    (4^L <= target) and then adaptively by the Legendre-tail criterion with a
+    tolerance of 1e-6, 1e-9 or 1e-12 (at most 4 more levels): of these six
+    trees the one whose leaf count is nearest the target (in log) is kept."""
+    import heat2d_per_box_b200 as hb
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(ntrees):
+        ng = int(rng.integers(5, 31))
+        c = rng.uniform(-0.5, 0.5, (ng, 2))
+        w = np.exp(rng.uniform(np.log(2e-3), np.log(5e-2), ng))
+        a = rng.standard_normal(ng)
+        target = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        L = max(1, int(np.floor(np.log(target) / np.log(4))))
+        t, best = None, np.inf
+        for minlev in (L, L + 1):
+            for tail in (1e-6, 1e-9, 1e-12):
+                cand = hb.build_adaptive(hb.gauss_params(c, w, a), norder=8, ipoly=0, iperiod=1, eps=tail,
+                                         minlev=minlev, maxlev=minlev + 4)
+                d = abs(np.log(len(cand.leaves()) / target))
+                if d < best:
+                    t, best = cand, d
+        delta = float(np.exp(rng.uniform(np.log(1e-5), np.log(1e-1))))
+        out.append((t, delta))
+    return out
+
+
+def run_uneven(args, rank, world):
+    """64 uneven trees x nd=8 densities, one batch (split precision), captured
+    as one CUDA graph; also the same plans executed one after another."""
+    import torch
+    import heat2d_per_box_b200 as hb
+    torch.cuda.set_device(0)
+    nd, eps = 8, 1e-6
+    trees = make_uneven_trees(6)
+    plans = [hb.Plan(t, d, eps, nd=nd, precision=hb.BFGT_PREC_SPLIT) for t, d in trees]
+    batch = hb.Batch(plans)
+    off = batch.offsets
+    rng = np.random.default_rng(7)
+    fv = []
+    for t, _ in trees:
+        f = np.repeat(t.fvals[:, :, None], nd, axis=2) * rng.uniform(0.5, 2.0, nd)[None, None, :]
+        f[t.nchild() > 0] = 0.0
+        fv.append(f.reshape(-1))
+    F = torch.from_numpy(np.concatenate(fv)).cuda()
+    P = torch.zeros_like(F)
+    npts = sum(len(t.leaves()) * t.npbox * nd for t, _ in trees)
+    stream = torch.cuda.current_stream()
+    batch.graph_capture(F, P, stream)
+    for _ in range(args.warmup):
+        batch.graph_launch(stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.graph_launch(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    batch.check()
+    # the same transforms as separate plan executes (4 launches per tree)
+    fs = [F[off[i]:off[i + 1]] for i in range(len(plans))]
+    ps = [P[off[i]:off[i + 1]] for i in range(len(plans))]
+    for _ in range(args.warmup):
+        for pl, f, p in zip(plans, fs, ps):
+            pl.execute(f, p, stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        for pl, f, p in zip(plans, fs, ps):
+            pl.execute(f, p, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_seq = e0.elapsed_time(e1) / args.steps
+    # per-stage device time of the batched execute (events, outside the graph)
+    batch.stage_ms()
+    for _ in range(max(3, min(args.steps, 10))):
+        batch.execute(F, P, stream)
+    st = batch.stage_ms()
+    nst = max(st[6], 1)
+    stage = {k: round(st[i] / nst, 4) for i, k in enumerate(["form", "reduce", "translate", "eval", "near"])}
+    info = batch.info()
+    leaves = [len(t.leaves()) for t, _ in trees]
+    regimes = [pl.info()["regime"] for pl in plans]
+    line = {"metric": METRIC, "value": npts / (ms * 1e-3), "unit": "leaf points/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f16-split/f32acc/f64", "data": "synthetic",
+            "config": {"workload": "64 uneven periodic order-8 trees, nd=8, delta log-U[1e-5,1e-1] per tree, "
+                                   "eps=1e-6, one batch captured as one CUDA graph",
+                       "trees": len(trees), "leaves_total": int(sum(leaves)), "leaves_min": int(min(leaves)),
+                       "leaves_max": int(max(leaves)), "points_x_nd": int(npts),
+                       "regimes": {str(r): int(regimes.count(r)) for r in sorted(set(regimes))},
+                       "launches_per_step": info["launches"], "form_items": info["form_items"]},
+            "stage_ms": stage, "unbatched_value": npts / (ms_seq * 1e-3), "unbatched_ms_per_step": ms_seq,
+            "batched_over_unbatched": ms_seq / ms}
+    batch.close()
+    for pl in plans:
+        pl.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -176,6 +281,9 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "split"])
     ap.add_argument("--small", action="store_true", help="level-6 base tree (for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="adaptive16", choices=["adaptive16", "uneven64"],
+                    help="adaptive16: one adaptive order-16 tree (default); uneven64: 64 uneven order-8 trees, "
+                         "nd=8, batched in one graph")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -185,6 +293,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "uneven64":
+        run_uneven(args, rank, world)
         return
 
     import torch

@@ -20,9 +20,18 @@ def _iref(v):
     return C.byref(C.c_int(int(v)))
 
 
+def _arr(a):
+    if a is None:
+        return None
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+        raise TypeError("grad/hess must be C-contiguous float64 numpy arrays")
+    return a.ctypes.data
+
+
 def boxfgt(nd, ndim, delta, eps, ipoly, iperiod, norder, npbox, nboxes, nlevels, ltree, itree, iptr, centers, boxsize,
            fvals, ifpgh, pot, grad, hess, ifnewtree, ntarg, targs, ifpghtarg, pote, grade, hesse, timeinfo):
-    """Drop-in for `call boxfgt(...)`: pot(nd,npbox,nboxes) += G_delta * fvals on leaves.
+    """Drop-in for `call boxfgt(...)`: pot(nd,npbox,nboxes) += G_delta * fvals on leaves
+    (and grad(nd,2,npbox,nboxes), hess(nd,3,npbox,nboxes) for ifpgh = 2, 3).
 
     Raises BfgtError when the library records an error (the Fortran routine
     itself has no error argument; the C ABI keeps its message in
@@ -39,7 +48,8 @@ def boxfgt(nd, ndim, delta, eps, ipoly, iperiod, norder, npbox, nboxes, nlevels,
     dl, ep = C.c_double(float(delta)), C.c_double(float(eps))
     L.boxfgt_(_iref(nd), _iref(ndim), C.byref(dl), C.byref(ep), _iref(ipoly), C.byref(ip), _iref(norder), _iref(npbox),
               C.byref(nb), C.byref(nl), C.byref(lt), itree.reshape(-1), iptr, centers.reshape(-1), boxsize,
-              fvals.reshape(-1), _iref(ifpgh), pot.reshape(-1), None, None, _iref(ifnewtree), _iref(ntarg), None,
+              fvals.reshape(-1), _iref(ifpgh), pot.reshape(-1), _arr(grad), _arr(hess), _iref(ifnewtree), _iref(ntarg),
+              None,
               _iref(ifpghtarg), None, None, None, timeinfo)
     err = _lib.last_error()
     if err:
@@ -99,6 +109,24 @@ class Plan:
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         _lib.check(self._L.bfgt_plan_execute_host(self._h, fv.ctypes.data, pot.ctypes.data, s))
         return pot
+
+    def execute_pgh(self, ifpgh, d_fvals, d_pot, d_grad=None, d_hess=None, stream=None):
+        """pot += K f; grad(nd,2,npbox,nboxes) and hess(nd,3,npbox,nboxes) (xx, xy, yy)
+        += its derivatives for ifpgh = 2, 3 (device arrays)."""
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_plan_execute_pgh(self._h, int(ifpgh), self._ptr(d_fvals), self._ptr(d_pot),
+                                                 self._ptr(d_grad), self._ptr(d_hess), s))
+
+    def execute_pgh_host(self, ifpgh, fvals, pot, grad=None, hess=None, stream=None):
+        fv = np.ascontiguousarray(fvals, np.float64)
+        for nm, a in (("pot", pot), ("grad", grad), ("hess", hess)):
+            if a is not None and not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+                raise TypeError(f"{nm} must be a C-contiguous float64 array")
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_plan_execute_pgh_host(self._h, int(ifpgh), fv.ctypes.data, pot.ctypes.data,
+                                                      None if grad is None else grad.ctypes.data,
+                                                      None if hess is None else hess.ctypes.data, s))
+        return pot, grad, hess
 
     def execute_adjoint(self, d_potbar, d_fbar, stream=None):
         """fbar += K^T potbar on leaf boxes (the transpose of execute: pot += K fvals)."""

@@ -125,8 +125,10 @@ int bfgt_plan_execute(bfgt_plan plan, const double *d_fvals, double *d_pot, void
 namespace {
 
 // Host-array form of one transform on dp: uploads the leaf runs of the input
-// and of the accumulator, runs, and copies the accumulator's leaf runs back.
-int execute_host_on(bfgt_plan plan, bfgt::DevicePlan &dp, const double *in, double *acc, cudaStream_t s) {
+// and of the accumulators, runs, and copies the accumulators' leaf runs back.
+// With ifpgh >= 2 grad(nd,2,..) and, for 3, hess(nd,3,..) are accumulated too.
+int execute_host_on(bfgt_plan plan, bfgt::DevicePlan &dp, const double *in, double *acc, cudaStream_t s,
+                    int ifpgh = 1, double *grad = nullptr, double *hess = nullptr) {
   const size_t elems = (size_t)dp.nd * dp.n * dp.n * dp.nboxes;
   if (dp.stage_elems < elems) {
     if (dp.d_stage_f) cudaFree(dp.d_stage_f);
@@ -140,23 +142,55 @@ int execute_host_on(bfgt_plan plan, bfgt::DevicePlan &dp, const double *in, doub
     }
     dp.stage_elems = elems;
   }
+  if (ifpgh >= 2 && dp.stage_gh_elems < elems) {
+    if (dp.d_stage_gh) cudaFree(dp.d_stage_gh);
+    dp.d_stage_gh = nullptr;
+    dp.stage_gh_elems = 0;
+    if (cudaMalloc(&dp.d_stage_gh, 5 * elems * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(BFGT_ERR_OOM, "cannot allocate device staging buffers (grad/hess)");
+    }
+    dp.stage_gh_elems = elems;
+  }
+  double *dg = ifpgh >= 2 ? dp.d_stage_gh : nullptr;
+  double *dh = ifpgh == 3 ? dp.d_stage_gh + 2 * elems : nullptr;
   // only the leaf boxes are read (input) and accumulated into
   const size_t per = (size_t)dp.nd * dp.n * dp.n;
+  struct Acc {
+    double *h, *d;
+    size_t k;  // components per point
+  };
+  std::vector<Acc> accs = {{acc, dp.d_stage_p, 1}};
+  if (dg) accs.push_back({grad, dg, 2});
+  if (dh) accs.push_back({hess, dh, 3});
   for (const auto &r : plan->leaf_runs) {
     const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
-    if (cudaMemcpyAsync(dp.d_stage_f + o, in + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(dp.d_stage_p + o, acc + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    if (cudaMemcpyAsync(dp.d_stage_f + o, in + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess)
       return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
+    for (const Acc &a : accs)
+      if (cudaMemcpyAsync(a.d + a.k * o, a.h + a.k * o, a.k * c, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
   }
   std::string msg;
-  int rc = bfgt::device_plan_execute(dp, dp.d_stage_f, dp.d_stage_p, s, msg);
+  int rc = ifpgh >= 2 ? bfgt::device_plan_execute_pgh(dp, ifpgh, dp.d_stage_f, dp.d_stage_p, dg, dh, s, msg)
+                      : bfgt::device_plan_execute(dp, dp.d_stage_f, dp.d_stage_p, s, msg);
   if (rc != BFGT_OK) return fail(rc, msg);
   for (const auto &r : plan->leaf_runs) {
     const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
-    if (cudaMemcpyAsync(acc + o, dp.d_stage_p + o, c, cudaMemcpyDeviceToHost, s) != cudaSuccess)
-      return fail(BFGT_ERR_CUDA, "device-to-host copy failed");
+    for (const Acc &a : accs)
+      if (cudaMemcpyAsync(a.h + a.k * o, a.d + a.k * o, a.k * c, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return fail(BFGT_ERR_CUDA, "device-to-host copy failed");
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(BFGT_ERR_CUDA, std::string("transform failed: ") + cudaGetErrorString(cudaGetLastError()));
+  return BFGT_OK;
+}
+
+// Uploads the derivative tables on first use.
+int ensure_pgh(bfgt_plan plan) {
+  if (plan->dp.pgh_ready) return BFGT_OK;
+  std::string msg;
+  int rc = bfgt::device_plan_prepare_pgh(plan->dp, plan->hp, msg);
+  if (rc != BFGT_OK) return fail(rc, msg);
   return BFGT_OK;
 }
 
@@ -195,6 +229,37 @@ int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, voi
   if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
   if (!fvals || !pot) return fail(BFGT_ERR_ARG, "fvals/pot are NULL");
   return execute_host_on(plan, plan->dp, fvals, pot, (cudaStream_t)stream);
+}
+
+int bfgt_plan_execute_pgh(bfgt_plan plan, int ifpgh, const double *d_fvals, double *d_pot, double *d_grad,
+                          double *d_hess, void *stream) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (ifpgh < 1 || ifpgh > 3) return fail(BFGT_ERR_ARG, "ifpgh must be 1, 2 or 3");
+  if (!d_fvals || !d_pot || (ifpgh >= 2 && !d_grad) || (ifpgh == 3 && !d_hess))
+    return fail(BFGT_ERR_ARG, "a device array that ifpgh asks for is NULL");
+  if (ifpgh >= 2) {
+    int rc = ensure_pgh(plan);
+    if (rc != BFGT_OK) return rc;
+  }
+  std::string msg;
+  int rc = bfgt::device_plan_execute_pgh(plan->dp, ifpgh, d_fvals, d_pot, d_grad, d_hess, (cudaStream_t)stream, msg);
+  if (rc != BFGT_OK) return fail(rc, msg);
+  return BFGT_OK;
+}
+
+int bfgt_plan_execute_pgh_host(bfgt_plan plan, int ifpgh, const double *fvals, double *pot, double *grad,
+                               double *hess, void *stream) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (ifpgh < 1 || ifpgh > 3) return fail(BFGT_ERR_ARG, "ifpgh must be 1, 2 or 3");
+  if (!fvals || !pot || (ifpgh >= 2 && !grad) || (ifpgh == 3 && !hess))
+    return fail(BFGT_ERR_ARG, "an array that ifpgh asks for is NULL");
+  if (ifpgh >= 2) {
+    int rc = ensure_pgh(plan);
+    if (rc != BFGT_OK) return rc;
+  }
+  return execute_host_on(plan, plan->dp, fvals, pot, (cudaStream_t)stream, ifpgh, grad, hess);
 }
 
 int bfgt_plan_execute_adjoint(bfgt_plan plan, const double *d_potbar, double *d_fbar, void *stream) {
@@ -346,16 +411,21 @@ int bfgt_plan_destroy(bfgt_plan plan) {
   return BFGT_OK;
 }
 
-int bfgt_boxfgt(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
+}  // extern "C"
+
+namespace {
+
+int boxfgt_impl(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
                 int ltree, int *itree, const int *iptr, const double *centers, const double *boxsize,
-                const double *fvals, double *pot, double *timeinfo, int precision) {
+                const double *fvals, int ifpgh, double *pot, double *grad, double *hess, double *timeinfo,
+                int precision) {
   double t0 = now_s();
   bfgt_plan plan = nullptr;
   int rc = bfgt_plan_create(&plan, nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree, iptr,
                             centers, boxsize, precision);
   if (rc != BFGT_OK) return rc;
   double t1 = now_s();
-  rc = bfgt_plan_execute_host(plan, fvals, pot, nullptr);
+  rc = bfgt_plan_execute_pgh_host(plan, ifpgh, fvals, pot, grad, hess, nullptr);
   if (rc == BFGT_OK) rc = bfgt_plan_check(plan);
   if (rc == BFGT_OK && timeinfo) {
     double st[8];
@@ -375,13 +445,22 @@ int bfgt_boxfgt(int nd, double delta, double eps, int ipoly, int iperiod, int no
   return rc;
 }
 
+}  // namespace
+
+extern "C" {
+
+int bfgt_boxfgt(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
+                int ltree, int *itree, const int *iptr, const double *centers, const double *boxsize,
+                const double *fvals, double *pot, double *timeinfo, int precision) {
+  return boxfgt_impl(nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree, iptr, centers, boxsize,
+                     fvals, 1, pot, nullptr, nullptr, timeinfo, precision);
+}
+
 void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *eps, const int *ipoly, int *iperiod,
              const int *norder, const int *npbox, int *nboxes, int *nlevels, int *ltree, int *itree, int *iptr,
              double *centers, double *boxsize, const double *fvals, const int *ifpgh, double *pot, double *grad,
              double *hess, const int *ifnewtree, const int *ntarg, const double *targs, const int *ifpghtarg,
              double *pote, double *grade, double *hesse, double *timeinfo) {
-  (void)grad;
-  (void)hess;
   (void)targs;
   (void)pote;
   (void)grade;
@@ -396,8 +475,12 @@ void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *
     fail(BFGT_ERR_ARG, "boxfgt_: only ndim=2 is supported");
     return;
   }
-  if (*ifpgh != 1 || *ifpghtarg > 0 || *ifnewtree != 0) {
-    fail(BFGT_ERR_ARG, "boxfgt_: only ifpgh=1, ifpghtarg=0, ifnewtree=0 are supported");
+  if (*ifpgh < 1 || *ifpgh > 3 || *ifpghtarg > 0 || *ifnewtree != 0) {
+    fail(BFGT_ERR_ARG, "boxfgt_: only ifpgh=1,2,3 with ifpghtarg=0, ifnewtree=0 are supported");
+    return;
+  }
+  if ((*ifpgh >= 2 && !grad) || (*ifpgh == 3 && !hess)) {
+    fail(BFGT_ERR_ARG, "boxfgt_: grad/hess arrays are NULL");
     return;
   }
   if (*npbox != (*norder) * (*norder)) {
@@ -405,8 +488,8 @@ void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *
     return;
   }
   double ti[20];
-  bfgt_boxfgt(*nd, *delta, *eps, *ipoly, *iperiod, *norder, *nboxes, *nlevels, *ltree, itree, iptr, centers, boxsize,
-              fvals, pot, timeinfo ? timeinfo : ti, BFGT_PREC_FP64);
+  boxfgt_impl(*nd, *delta, *eps, *ipoly, *iperiod, *norder, *nboxes, *nlevels, *ltree, itree, iptr, centers, boxsize,
+              fvals, *ifpgh, pot, grad, hess, timeinfo ? timeinfo : ti, BFGT_PREC_FP64);
 }
 
 int bfgt_host_plan_dump(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes,

@@ -44,6 +44,13 @@ struct DevicePlan {
   double2 *W = nullptr;         // cutoff shifts (nexp, 9)
   double *pw_weight = nullptr;  // (hh)
   double *kscale = nullptr;     // (hh) translation factor per k2, or null
+  // gradient / hessian outputs (built on first use): per-element derivative
+  // factors (5, nexp) for x, y, xx, xy, yy; scratch for the derivative local
+  // expansions (ncut, 3 nd, nexp); the near tables with their first and
+  // second derivatives appended
+  double2 *dfac = nullptr, *Ld = nullptr;
+  double *tab3_loc = nullptr;
+  bool pgh_ready = false;
   double2 *Mpart = nullptr;     // (nchunks, nd, nexp) partial expansions per chunk
   double2 *M = nullptr;         // (ncut, nd, nexp) cutoff-box expansions
   double2 *L = nullptr;         // (ncut, nd, nexp) cutoff-box local expansions
@@ -62,6 +69,8 @@ struct DevicePlan {
   double *h_stage_f = nullptr, *h_stage_p = nullptr;  // pinned
   double *d_stage_f = nullptr, *d_stage_p = nullptr;
   size_t stage_elems = 0;
+  double *d_stage_gh = nullptr;  // grad (2 x) and hess (3 x) staging, 5 * stage_gh_elems
+  size_t stage_gh_elems = 0;
   // timing: one set of stage events per execute since the last read-out
   std::vector<std::array<cudaEvent_t, 6>> evsets;
   int nrec = 0;
@@ -78,6 +87,12 @@ int build_reduce_groups(DevicePlan &dp, const std::vector<int> &cut_of_chunk, st
 // Allocates and uploads; returns a BFGT_* status and fills msg on failure.
 int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);
 void device_plan_destroy(DevicePlan &dp);
+// Uploads the derivative tables used by device_plan_execute_pgh.
+int device_plan_prepare_pgh(DevicePlan &dp, const HostPlan &hp, std::string &msg);
+// pot += K f and, for ifpgh >= 2, grad(nd,2,npbox,nboxes) += grad K f, for
+// ifpgh = 3 also hess(nd,3,npbox,nboxes) (xx, xy, yy).
+int device_plan_execute_pgh(DevicePlan &dp, int ifpgh, const double *d_fvals, double *d_pot, double *d_grad,
+                            double *d_hess, cudaStream_t stream, std::string &msg);
 // Queues the transform on stream; returns BFGT_* status.
 int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cudaStream_t stream,
                         std::string &msg);

@@ -119,6 +119,24 @@ __global__ void __launch_bounds__(kTrThreads) k_translate(const __grid_constant_
   a.L[idx] = s;
 }
 
+// Ld(icut, c*nd + ind, e) = L(icut, ind, e) * fac(c, e) for nc components:
+// the local expansions of derivatives of the potential (fac = (i ts/sqrt(delta0))
+// to the derivative orders in x (first index of e) and y (second)).
+__global__ void k_deriv_expand(const double2 *__restrict__ L, const double2 *__restrict__ fac,
+                               double2 *__restrict__ Ld, int ncut, int nd, int nc, int nexp) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)ncut * nd * nc * nexp;
+  if (idx >= tot) return;
+  const int e = (int)(idx % nexp);
+  const size_t r = idx / nexp;
+  const int q = (int)(r % ((size_t)nd * nc));
+  const size_t icut = r / ((size_t)nd * nc);
+  const int c = q / nd, ind = q - c * nd;
+  const double2 l = L[(icut * nd + ind) * nexp + e];
+  const double2 f = fac[(size_t)c * nexp + e];
+  Ld[idx] = make_double2(l.x * f.x - l.y * f.y, l.x * f.y + l.y * f.x);
+}
+
 template <int TM, int TN, int NT>
 __global__ void __launch_bounds__(kWarps * 32, 3) k_form_fp64(FormArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -431,6 +449,11 @@ struct NearArgs {
   const int *ind_loc;
   int ntarget, nd, n;
   long long elem_off;  // start of this plan's leaf arrays in the (packed) fvals/pot
+  // output out(nd, ncomp, npbox, nboxes) += component (out_off / nd) of the
+  // transform (out_nd = nd * ncomp); the x and y tables are read at slot +
+  // xoff / yoff (0: values, one table set further: first derivatives, two:
+  // second derivatives), the band pattern always at the slot itself
+  int out_nd, out_off, xoff, yoff;
 };
 // a single plan (descs null, block b takes targets kWarps b..) or a batch
 // (block b takes targets work[b].y.. of plan work[b].x)
@@ -470,8 +493,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_near_fp64(const __grid_constant
       const int *by = il + (size_t)2 * (n + 1) * iy;
       const int kx0 = bx[2 * n], kx1 = bx[2 * n + 1], ky0 = by[2 * n], ky1 = by[2 * n + 1];
       if (kx1 - kx0 + 1 == 0 || ky1 - ky0 + 1 == 0) continue;
-      const double *tx = tl + (size_t)npb * ix;
-      const double *ty = tl + (size_t)npb * iy;
+      const double *tx = tl + (size_t)npb * (ix + a.xoff);
+      const double *ty = tl + (size_t)npb * (iy + a.yoff);
       const double *fv = fvals + (size_t)sb * nd * npb;
       __syncwarp();
       for (int o = lane; o < npb; o += 32) sF[o] = fv[ind + (size_t)nd * o];
@@ -496,8 +519,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_near_fp64(const __grid_constant
       }
     }
     __syncwarp();
-    double *pb = pot + (size_t)tb * nd * npb;
-    for (int o = lane; o < npb; o += 32) pb[ind + (size_t)nd * o] += sP[o];
+    double *pb = pot + (size_t)tb * a.out_nd * npb + a.out_off;
+    for (int o = lane; o < npb; o += 32) pb[ind + (size_t)a.out_nd * o] += sP[o];
     __syncwarp();
   }
 }
@@ -694,8 +717,8 @@ void device_plan_destroy(DevicePlan &dp) {
   if (dp.graph) cudaGraphDestroy(dp.graph);
   split_plan_destroy(dp);
   void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.columns, dp.cut_chunk_begin, dp.cut_pw_begin,
-                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.kscale, dp.Mpart, dp.M, dp.L, dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups, dp.nf_target,
-                  dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.d_stage_f, dp.d_stage_p};
+                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.kscale, dp.dfac, dp.Ld, dp.tab3_loc, dp.Mpart, dp.M, dp.L, dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups, dp.nf_target,
+                  dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.d_stage_f, dp.d_stage_p, dp.d_stage_gh};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (dp.h_stage_f) cudaFreeHost(dp.h_stage_f);
@@ -745,7 +768,7 @@ TrArgs tr_args(const DevicePlan &dp) {
 
 NearArgs near_args(const DevicePlan &dp, long long elem_off) {
   return NearArgs{dp.nf_target, dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.nnf, dp.nd, dp.n,
-                  elem_off};
+                  elem_off, dp.nd, 0, 0, 0};
 }
 
 bool has_pw(const DevicePlan &dp) { return !dp.direct_only && dp.nchunks > 0; }
@@ -803,6 +826,97 @@ int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cu
     k_near_fp64<<<(dp.nnf + kWarps - 1) / kWarps, kWarps * 32, dp.smem_near, s>>>(
         NearLaunch{near_args(dp, 0), nullptr, nullptr, d_fvals, d_pot});
   if (ev) cudaEventRecord(ev[5], s);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    msg = std::string("kernel launch failed: ") + cudaGetErrorString(e);
+    return BFGT_ERR_CUDA;
+  }
+  return BFGT_OK;
+}
+
+int device_plan_prepare_pgh(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
+  if (dp.pgh_ready) return BFGT_OK;
+  int rc = BFGT_OK;
+  auto chk = [&](int r) {
+    if (rc == BFGT_OK && r != BFGT_OK) rc = r;
+  };
+  if (has_pw(dp)) {
+    // derivative factor of PW index m (1-based), as mk_pw2pgh_tables builds
+    // tab_pw2der = tab_pw2pot * ts * dfac for m > npw/2 and its conjugate
+    // mirror below (bfgt_volrouts.f:339-401; dfac = i / sqrt(delta0))
+    const int npw = hp.npw, hh = hp.hh, npw2 = npw / 2;
+    const double s0 = 1.0 / std::sqrt(hp.delta0);
+    std::vector<double2> f(npw);
+    for (int m = 1; m <= npw; m++) {
+      if (m > npw2) f[m - 1] = make_double2(0.0, hp.ts[m - 1] * s0);
+      else f[m - 1] = make_double2(0.0, -hp.ts[npw - m] * s0);
+    }
+    auto mul = [](double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };
+    std::vector<double2> fac((size_t)5 * hp.nexp);
+    for (int k2 = 0; k2 < hh; k2++)
+      for (int k1 = 0; k1 < npw; k1++) {
+        const size_t e = (size_t)k1 + (size_t)npw * k2;
+        const double2 fx = f[k1], fy = f[k2];
+        fac[e] = fx;                                  // d/dx
+        fac[hp.nexp + e] = fy;                        // d/dy
+        fac[2 * (size_t)hp.nexp + e] = mul(fx, fx);   // d2/dx2
+        fac[3 * (size_t)hp.nexp + e] = mul(fx, fy);   // d2/dxdy
+        fac[4 * (size_t)hp.nexp + e] = mul(fy, fy);   // d2/dy2
+      }
+    chk(upload(dp.dfac, fac, msg));
+    chk(alloc_bytes((void **)&dp.Ld, sizeof(double2) * (size_t)dp.ncut * dp.nd * 3 * dp.nexp, msg));
+  }
+  if (dp.nnf > 0) {
+    std::vector<double> t3(hp.tab_loc);
+    t3.insert(t3.end(), hp.tabx_loc.begin(), hp.tabx_loc.end());
+    t3.insert(t3.end(), hp.tabxx_loc.begin(), hp.tabxx_loc.end());
+    chk(upload(dp.tab3_loc, t3, msg));
+  }
+  if (rc == BFGT_OK) dp.pgh_ready = true;
+  return rc;
+}
+
+int device_plan_execute_pgh(DevicePlan &dp, int ifpgh, const double *d_fvals, double *d_pot, double *d_grad,
+                            double *d_hess, cudaStream_t s, std::string &msg) {
+  int rc = device_plan_execute(dp, d_fvals, d_pot, s, msg);
+  if (rc != BFGT_OK || ifpgh < 2) return rc;
+  if (!dp.pgh_ready) {
+    msg = "derivative tables are not prepared";
+    return BFGT_ERR_ARG;
+  }
+  struct Part {
+    int nc, c0;
+    double *out;
+  };
+  const Part parts[2] = {{2, 0, d_grad}, {3, 2, d_hess}};
+  for (int p = 0; p < (ifpgh == 3 ? 2 : 1); p++) {
+    const Part &pt = parts[p];
+    if (has_pw(dp)) {
+      const size_t tot = (size_t)dp.ncut * dp.nd * pt.nc * dp.nexp;
+      k_deriv_expand<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(dp.L, dp.dfac + (size_t)pt.c0 * dp.nexp, dp.Ld,
+                                                                    dp.ncut, dp.nd, pt.nc, dp.nexp);
+      DevicePlan view = dp;
+      view.events = false;
+      view.nd = dp.nd * pt.nc;
+      view.L = dp.Ld;
+      plan_eval(view, pt.out, s);
+    }
+    if (dp.nnf > 0) {
+      // derivative orders of the components: grad x, y; hess xx, xy, yy
+      static const int ox[5] = {1, 0, 2, 1, 0}, oy[5] = {0, 1, 0, 1, 2};
+      const int nslot = 13 * (dp.nlevels + 1);
+      for (int c = 0; c < pt.nc; c++) {
+        NearArgs na = near_args(dp, 0);
+        na.tab_loc = dp.tab3_loc;
+        na.out_nd = dp.nd * pt.nc;
+        na.out_off = c * dp.nd;
+        na.xoff = ox[pt.c0 + c] * nslot;
+        na.yoff = oy[pt.c0 + c] * nslot;
+        k_near_fp64<<<(dp.nnf + kWarps - 1) / kWarps, kWarps * 32, dp.smem_near, s>>>(
+            NearLaunch{na, nullptr, nullptr, d_fvals, pt.out});
+      }
+    }
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     msg = std::string("kernel launch failed: ") + cudaGetErrorString(e);

@@ -582,12 +582,13 @@ void sparse_pattern(double eps, int n, const double *a, int *indc) {
 }
 
 // tab_loc(n,n,-6:6) and ind_loc(2,n+1,-6:6) of one target level (mrefinelev = 0)
-void mk_loctab_level(const LocTabCtx &c, double eps, double delta, double boxdim, double *tab_loc, int *ind_loc) {
+void mk_loctab_level(const LocTabCtx &c, double eps, double delta, double boxdim, double *tab_loc, double *tabx_out,
+                     double *tabxx_out, int *ind_loc) {
   const int n = c.n, nl = 6;
   auto T = [&](double *base, int m, int j, int k) -> double & {
     return base[(m - 1) + (size_t)n * ((j - 1) + (size_t)n * (k + nl))];
   };
-  std::vector<double> tabx_loc((size_t)n * n * 13), tabxx_loc((size_t)n * n * 13);
+  std::vector<double> tabx_loc((size_t)n * n * 13, 0.0), tabxx_loc((size_t)n * n * 13, 0.0);
   std::vector<double> tab(n * n), tabx(n * n), tabxx(n * n);
   std::vector<int> ind(2 * (n + 1)), indx(2 * (n + 1)), indxx(2 * (n + 1));
   auto merge = [&](int k) {
@@ -641,6 +642,8 @@ void mk_loctab_level(const LocTabCtx &c, double eps, double delta, double boxdim
       merge(kk);
     }
   }
+  std::copy(tabx_loc.begin(), tabx_loc.end(), tabx_out);
+  std::copy(tabxx_loc.begin(), tabxx_loc.end(), tabxx_out);
 }
 
 // ---- tree lists ------------------------------------------------------------
@@ -955,10 +958,13 @@ void build_host_plan(HostPlan &hp, const TreeView &t, int nd, double delta, doub
     }
     const size_t ntl = (size_t)n * n * 13, nil = (size_t)2 * (n + 1) * 13;
     hp.tab_loc.assign(ntl * (nlevels + 1), 0.0);
+    hp.tabx_loc.assign(ntl * (nlevels + 1), 0.0);
+    hp.tabxx_loc.assign(ntl * (nlevels + 1), 0.0);
     hp.ind_loc.assign(nil * (nlevels + 1), 0);
 #pragma omp parallel for schedule(dynamic)
     for (int l = 0; l <= nlevels; l++)
-      mk_loctab_level(c, eps, delta, t.boxsize[l], &hp.tab_loc[ntl * l], &hp.ind_loc[nil * l]);
+      mk_loctab_level(c, eps, delta, t.boxsize[l], &hp.tab_loc[ntl * l], &hp.tabx_loc[ntl * l],
+                      &hp.tabxx_loc[ntl * l], &hp.ind_loc[nil * l]);
   }
 
   hp.direct_only = (npwlevel >= nlevels && npwlevel > 0);

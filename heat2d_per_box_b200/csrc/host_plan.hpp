@@ -76,6 +76,10 @@ struct HostPlan {
   std::vector<cplx> tab_poly2pw;  // (n, npw, 0:nlevels), Fortran order
   std::vector<cplx> tab_pw2pot;   // (npw, n, 0:nlevels)
   std::vector<double> tab_loc;    // (n, n, -6:6, 0:nlevels)
+  // first and second derivatives of tab_loc in the target coordinate
+  // (tabx_loc, tabxx_loc of mk_loctab_all, bfgt_volrouts.f:407-660); ind_loc
+  // is the merged band pattern of all three
+  std::vector<double> tabx_loc, tabxx_loc;
   std::vector<int> ind_loc;       // (2, n+1, -6:6, 0:nlevels)
   std::vector<cplx> wshift;       // (nexp, 9) cutoff-level mp->loc shifts
   // lists (1-based box ids as in the reference)

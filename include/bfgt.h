@@ -45,9 +45,10 @@ extern "C" {
 #define BFGT_PREC_SPLIT 1       /* tensor-core split-FP16 slices, FP32 accum.,
                                    FP64 phases and FP64 cross-leaf accumulation */
 
-/* Replaces bfgt/boxfgt.f:5-286 (boxfgt).  Supported: ndim=2, ifpgh=1,
-   ifnewtree=0, ifpghtarg=0 (the configuration every solver in the reference
-   uses, hpots/hpots2dadap.f:79-106).  pot is accumulated into, on leaf boxes
+/* Replaces bfgt/boxfgt.f:5-286 (boxfgt).  Supported: ndim=2, ifpgh=1, 2, 3,
+   ifnewtree=0, ifpghtarg=0 (ifpgh=1 is what every solver in the reference
+   uses, hpots/hpots2dadap.f:79-106).  pot (and grad(nd,2,npbox,nboxes),
+   hess(nd,3,npbox,nboxes) as ifpgh asks) are accumulated into, on leaf boxes
    only; the colleague arrays itree(iptr(6)), itree(iptr(7)) are recomputed as
    the reference does (boxfgt.f:516-528); timeinfo(1:20) is zeroed and filled
    with per-stage seconds. */
@@ -88,6 +89,22 @@ int bfgt_plan_execute(bfgt_plan plan, const double *d_fvals, double *d_pot, void
 /* Same transform on host arrays: uploads the leaf values, runs, and adds the
    result into the host pot (the reference-facing form of a planned call). */
 int bfgt_plan_execute_host(bfgt_plan plan, const double *fvals, double *pot, void *stream);
+
+/* Replaces the ifpgh = 2, 3 branches of bfgt/boxfgt.f steps 5 and 6
+   (gnd_pw2pgh -> g2d_pw2pg / g2d_pw2pgh, bfgt_pwrouts.f:309-375, 608-784;
+   gnd_tens_prod_to_pghloc -> g2d_tens_prod_to_pgloc / _pghloc,
+   bfgt_local.f:379-552) on device arrays: pot += K fvals, and for ifpgh >= 2
+   grad(nd,2,norder**2,nboxes) += its gradient (x, y), for ifpgh = 3 also
+   hess(nd,3,norder**2,nboxes) += its hessian (xx, xy, yy), on leaf boxes.
+   ifpgh = 1 is bfgt_plan_execute (grad and hess may then be NULL).  The first
+   call with ifpgh >= 2 uploads the derivative tables (synchronous); later
+   calls only queue kernels on stream. */
+int bfgt_plan_execute_pgh(bfgt_plan plan, int ifpgh, const double *d_fvals, double *d_pot, double *d_grad,
+                          double *d_hess, void *stream);
+
+/* The same on host arrays (leaf boxes copied in and out). */
+int bfgt_plan_execute_pgh_host(bfgt_plan plan, int ifpgh, const double *fvals, double *pot, double *grad,
+                               double *hess, void *stream);
 
 /* No counterpart in the reference (boxfgt has no adjoint; this is the
    differentiation entry point).  Applies the transpose of this plan's discrete

@@ -2,20 +2,22 @@
  * CPU oracle for the 2D periodic/free-space box fast Gauss transform.
  *
  * TEST INFRASTRUCTURE ONLY.  This file is a line-by-line C restatement of the
- * reference Fortran (Jsu1029/heat2d_per_box) for ndim=2, ifpgh=1, ifnewtree=0,
- * ifpghtarg=0.  It is linked only by the tests, by __graft_entry__.smoke() as
+ * reference Fortran (Jsu1029/heat2d_per_box) for ndim=2, ifpgh=1, 2, 3,
+ * ifnewtree=0, ifpghtarg=0.  It is linked only by the tests, by __graft_entry__.smoke() as
  * the checker, and by bench.py's CPU-baseline leg.  The product library never
  * links or calls it.
  *
  * Followed files (paths inside the reference project):
  *   bfgt/boxfgt.f        boxfgt 5-286, bfgtmain 291-1591, gnd_mpalloc 1598-1702
  *   bfgt/bfgt_pwrouts.f  g2d_tens_prod_to_pw 98-147, g2d_pw2pot 549-602,
+ *                        g2d_pw2pg 608-684, g2d_pw2pgh 688-784,
  *                        g2d_mk_pw_translation_matrices 1415-1471,
  *                        g2d_mk_merge_split_pw_matrices 1645-1703,
  *                        gnd_shiftpw 1798-1844, gnd_find_pwshift_ind 1848-1892,
  *                        gnd_shiftpw_loc 1905-1941, gnd_find_msshift_ind 1946-1976,
  *                        gnd_copy_pwexp 1987-2015, gnd_pwzero 2021-2046
- *   bfgt/bfgt_local.f    g2d_tens_prod_to_potloc 315-375, gnd_find_loctab_ind 1729-1765
+ *   bfgt/bfgt_local.f    g2d_tens_prod_to_potloc 315-375, g2d_tens_prod_to_pgloc 379-447,
+ *                        g2d_tens_prod_to_pghloc 451-552, gnd_find_loctab_ind 1729-1765
  *   bfgt/bfgt_volrouts.f mk_leg2pw_tables 58-143, mk_cheb2pw_tables 151-275,
  *                        mk_pw2pgh_tables 339-401, mk_loctab_all 407-660,
  *                        mk_loctab 920-1060, mk_legetab_recur 1095-1187,
@@ -500,6 +502,30 @@ static void mk_pw2pot_table(int n, int npw, const double *ts, const double *xs, 
     for (int j1 = npw2 + 1; j1 <= npw; j1++) {
       ZT(tab, npw, j1, i) = zexpi(ts[j1 - 1] * x);
       ZT(tab, npw, npw - j1 + 1, i) = zconj(ZT(tab, npw, j1, i));
+    }
+  }
+}
+
+/* tab_pw2der = tab_pw2pot * ts * i/sqrt(delta) and tab_pw2dxx = tab_pw2der *
+   ts * i/sqrt(delta), with the conjugate symmetry of mk_pw2pgh_tables
+   (bfgt_volrouts.f:339-401; dfac = i*dsq*2/boxdim) */
+static void mk_pw2der_tables(int n, int npw, const double *ts, const double *xs, double delta, double boxdim,
+                             zc *tab, zc *tabx, zc *tabxx) {
+  double dsq = boxdim / 2 / sqrt(delta);
+  zc dfac = zmk(0, dsq * 2 / boxdim);
+  int npw2 = npw / 2;
+  for (int i = 1; i <= n; i++) {
+    double x = xs[i - 1] * dsq;
+    for (int j1 = npw2 + 1; j1 <= npw; j1++) {
+      zc t = zexpi(ts[j1 - 1] * x);
+      zc tx = zmul(zscal(t, ts[j1 - 1]), dfac);
+      zc txx = zmul(zscal(tx, ts[j1 - 1]), dfac);
+      ZT(tab, npw, j1, i) = t;
+      ZT(tabx, npw, j1, i) = tx;
+      ZT(tabxx, npw, j1, i) = txx;
+      ZT(tab, npw, npw - j1 + 1, i) = zconj(t);
+      ZT(tabx, npw, npw - j1 + 1, i) = zconj(tx);
+      ZT(tabxx, npw, npw - j1 + 1, i) = zconj(txx);
     }
   }
 }
@@ -1112,6 +1138,61 @@ static void g2d_pw2pot(int nd, int n, int npw, const zc *pwexp, const zc *tab, d
   }
 }
 
+/* g2d_pw2pg (ifpgh = 2, bfgt_pwrouts.f:608-684) and g2d_pw2pgh (ifpgh = 3,
+   bfgt_pwrouts.f:688-784): pot, grad(nd,2,n,n) and hess(nd,3,n,n) += 2 Re(...),
+   hess ordered xx, xy, yy */
+static void g2d_pw2pgh(int nd, int n, int npw, const zc *pwexp, const zc *tab, const zc *tabx, const zc *tabxx,
+                       int ifpgh, double *pot, double *grad, double *hess, zc *ff) {
+  int hh = (npw + 1) / 2;
+  int npw2 = npw / 2;
+  zc *ffx = ff + (size_t)n * hh, *ffxx = ffx + (size_t)n * hh;
+  for (int ind = 1; ind <= nd; ind++) {
+    for (int m2 = 1; m2 <= hh; m2++)
+      for (int k1 = 1; k1 <= n; k1++) {
+        zc cd = zmk(0, 0), cdx = zmk(0, 0), cdxx = zmk(0, 0);
+        for (int m1 = 1; m1 <= npw; m1++) {
+          zc pw = pwexp[(m1 - 1) + (size_t)npw * ((m2 - 1) + (size_t)hh * (ind - 1))];
+          cd = zadd(cd, zmul(ZT(tab, npw, m1, k1), pw));
+          cdx = zadd(cdx, zmul(ZT(tabx, npw, m1, k1), pw));
+          if (ifpgh == 3) cdxx = zadd(cdxx, zmul(ZT(tabxx, npw, m1, k1), pw));
+        }
+        ff[(m2 - 1) + (size_t)hh * (k1 - 1)] = cd;
+        ffx[(m2 - 1) + (size_t)hh * (k1 - 1)] = cdx;
+        ffxx[(m2 - 1) + (size_t)hh * (k1 - 1)] = cdxx;
+      }
+    for (int k2 = 1; k2 <= n; k2++)
+      for (int k1 = 1; k1 <= n; k1++) {
+        zc cd = zmk(0, 0), cdx = zmk(0, 0), cdy = zmk(0, 0), cdxx = zmk(0, 0), cdxy = zmk(0, 0), cdyy = zmk(0, 0);
+        for (int m2 = 1; m2 <= hh; m2++) {
+          if (m2 > npw2 && m2 != hh) continue;
+          const double w = (m2 > npw2) ? 0.5 : 1.0; /* zero frequency of odd npw */
+          zc f = ff[(m2 - 1) + (size_t)hh * (k1 - 1)], fx = ffx[(m2 - 1) + (size_t)hh * (k1 - 1)];
+          zc fxx = ffxx[(m2 - 1) + (size_t)hh * (k1 - 1)];
+          zc t = ZT(tab, npw, m2, k2), tx = ZT(tabx, npw, m2, k2), txx = ZT(tabxx, npw, m2, k2);
+          cd = zadd(cd, zscal(zmul(t, f), w));
+          cdy = zadd(cdy, zscal(zmul(tx, f), w));
+          cdx = zadd(cdx, zscal(zmul(t, fx), w));
+          if (ifpgh == 3) {
+            cdyy = zadd(cdyy, zscal(zmul(txx, f), w));
+            cdxy = zadd(cdxy, zscal(zmul(tx, fx), w));
+            cdxx = zadd(cdxx, zscal(zmul(t, fxx), w));
+          }
+        }
+        size_t o = (ind - 1) + (size_t)nd * ((k1 - 1) + (size_t)n * (k2 - 1));
+        size_t og = (ind - 1) + (size_t)nd * 2 * ((k1 - 1) + (size_t)n * (k2 - 1));
+        pot[o] = pot[o] + cd.re * 2;
+        grad[og] = grad[og] + cdx.re * 2;
+        grad[og + nd] = grad[og + nd] + cdy.re * 2;
+        if (ifpgh == 3) {
+          size_t oh = (ind - 1) + (size_t)nd * 3 * ((k1 - 1) + (size_t)n * (k2 - 1));
+          hess[oh] = hess[oh] + cdxx.re * 2;
+          hess[oh + nd] = hess[oh + nd] + cdxy.re * 2;
+          hess[oh + 2 * (size_t)nd] = hess[oh + 2 * (size_t)nd] + cdyy.re * 2;
+        }
+      }
+  }
+}
+
 static void gnd_shiftpw(int nd, size_t nexp, const zc *p1, zc *p2, const zc *w) {
   for (int ind = 0; ind < nd; ind++)
     for (size_t j = 0; j < nexp; j++) p2[j + nexp * ind] = zadd(p2[j + nexp * ind], zmul(p1[j + nexp * ind], w[j]));
@@ -1188,6 +1269,61 @@ static void g2d_tens_prod_to_potloc(int nd, int n, const double *fvals, double *
   }
 }
 
+/* g2d_tens_prod_to_pgloc / g2d_tens_prod_to_pghloc (bfgt_local.f:379-552):
+   pot, grad(nd,2,n,n) and, for ifpgh = 3, hess(nd,3,n,n) on the band pattern
+   of the value tables (ind_loc is the merged pattern of all three) */
+static void g2d_tens_prod_to_pghloc(int nd, int n, const double *fvals, int ifpgh, double *pot, double *grad,
+                                    double *hess, int ntab, const double *tab_loc, const double *tabx_loc,
+                                    const double *tabxx_loc, const int *ind_loc, const int *ixy, double *ff) {
+  int ix = ixy[0], iy = ixy[1];
+  int nx = ILOC(ind_loc, n, ntab, 2, n + 1, ix) - ILOC(ind_loc, n, ntab, 1, n + 1, ix) + 1;
+  int ny = ILOC(ind_loc, n, ntab, 2, n + 1, iy) - ILOC(ind_loc, n, ntab, 1, n + 1, iy) + 1;
+  if (nx == 0 || ny == 0) return;
+  double *ffx = ff + (size_t)n * n, *ffxx = ffx + (size_t)n * n;
+  for (int ind = 1; ind <= nd; ind++) {
+    for (int j2 = 1; j2 <= n; j2++)
+      for (int k1 = ILOC(ind_loc, n, ntab, 1, n + 1, ix); k1 <= ILOC(ind_loc, n, ntab, 2, n + 1, ix); k1++) {
+        double cd = 0, cdx = 0, cdxx = 0;
+        for (int j1 = ILOC(ind_loc, n, ntab, 1, k1, ix); j1 <= ILOC(ind_loc, n, ntab, 2, k1, ix); j1++) {
+          double f = fvals[(ind - 1) + (size_t)nd * ((j1 - 1) + (size_t)n * (j2 - 1))];
+          cd = cd + TLOC(tab_loc, n, ntab, j1, k1, ix) * f;
+          cdx = cdx + TLOC(tabx_loc, n, ntab, j1, k1, ix) * f;
+          if (ifpgh == 3) cdxx = cdxx + TLOC(tabxx_loc, n, ntab, j1, k1, ix) * f;
+        }
+        ff[(k1 - 1) + (size_t)n * (j2 - 1)] = cd;
+        ffx[(k1 - 1) + (size_t)n * (j2 - 1)] = cdx;
+        ffxx[(k1 - 1) + (size_t)n * (j2 - 1)] = cdxx;
+      }
+    for (int k2 = ILOC(ind_loc, n, ntab, 1, n + 1, iy); k2 <= ILOC(ind_loc, n, ntab, 2, n + 1, iy); k2++)
+      for (int k1 = ILOC(ind_loc, n, ntab, 1, n + 1, ix); k1 <= ILOC(ind_loc, n, ntab, 2, n + 1, ix); k1++) {
+        double cd = 0, cdx = 0, cdy = 0, cdxx = 0, cdxy = 0, cdyy = 0;
+        for (int j2 = ILOC(ind_loc, n, ntab, 1, k2, iy); j2 <= ILOC(ind_loc, n, ntab, 2, k2, iy); j2++) {
+          size_t q = (k1 - 1) + (size_t)n * (j2 - 1);
+          double t = TLOC(tab_loc, n, ntab, j2, k2, iy), tx = TLOC(tabx_loc, n, ntab, j2, k2, iy);
+          cd = cd + t * ff[q];
+          cdy = cdy + tx * ff[q];
+          cdx = cdx + t * ffx[q];
+          if (ifpgh == 3) {
+            cdyy = cdyy + TLOC(tabxx_loc, n, ntab, j2, k2, iy) * ff[q];
+            cdxy = cdxy + tx * ffx[q];
+            cdxx = cdxx + t * ffxx[q];
+          }
+        }
+        size_t o = (ind - 1) + (size_t)nd * ((k1 - 1) + (size_t)n * (k2 - 1));
+        size_t og = (ind - 1) + (size_t)nd * 2 * ((k1 - 1) + (size_t)n * (k2 - 1));
+        pot[o] = pot[o] + cd;
+        grad[og] = grad[og] + cdx;
+        grad[og + nd] = grad[og + nd] + cdy;
+        if (ifpgh == 3) {
+          size_t oh = (ind - 1) + (size_t)nd * 3 * ((k1 - 1) + (size_t)n * (k2 - 1));
+          hess[oh] = hess[oh] + cdxx;
+          hess[oh + nd] = hess[oh + nd] + cdxy;
+          hess[oh + 2 * (size_t)nd] = hess[oh + 2 * (size_t)nd] + cdyy;
+        }
+      }
+  }
+}
+
 /* ------------------------------------------------------------------------- */
 /* Driver (bfgt/boxfgt.f)                                                    */
 /* ------------------------------------------------------------------------- */
@@ -1220,7 +1356,7 @@ typedef struct {
 static void boxfgt_core(int nd, double delta, double eps, int ipoly, int *iperiod_p, int norder, int npbox,
                         int nboxes, int nlevels, int *itree, const int *iptr, const double *centers,
                         const double *boxsize, const double *fvals, double *pot, double *timeinfo,
-                        oracle_info *info) {
+                        oracle_info *info, int ifpgh, double *grad, double *hess) {
   int iperiod = *iperiod_p;
   double pi = 4.0 * atan(1.0);
   (void)pi;
@@ -1320,6 +1456,7 @@ static void boxfgt_core(int nd, double delta, double eps, int ipoly, int *iperio
   zc *rmlexp = NULL;
   int *nlistpw = NULL, *listpw = NULL;
   zc *tab_poly2pw = NULL, *tab_pw2pot = NULL, *wpwmsshift = NULL, *wpwshift = NULL;
+  zc *tab_pw2p = NULL, *tab_pw2der = NULL, *tab_pw2dxx = NULL; /* ifpgh >= 2 (mk_pw2pgh_tables) */
   int nmaxms = 0;
   if (!direct_only) {
     /* gnd_mpalloc (boxfgt.f:1598-1702), in complex units */
@@ -1346,6 +1483,14 @@ static void boxfgt_core(int nd, double delta, double eps, int ipoly, int *iperio
       if (ipoly == 0) mk_leg2pw_tables(norder, npw, ws, ts, delta0, boxsize[ilev], tab_poly2pw + (size_t)norder * npw * ilev);
       else mk_cheb2pw_tables(norder, npw, ws, ts, delta0, boxsize[ilev], tab_poly2pw + (size_t)norder * npw * ilev);
       mk_pw2pot_table(norder, npw, ts, xq, delta0, boxsize[ilev], tab_pw2pot + (size_t)norder * npw * ilev);
+    }
+    if (ifpgh >= 2) {
+      tab_pw2p = malloc(sizeof(zc) * (size_t)norder * npw * (nlevels + 1));
+      tab_pw2der = malloc(sizeof(zc) * (size_t)norder * npw * (nlevels + 1));
+      tab_pw2dxx = malloc(sizeof(zc) * (size_t)norder * npw * (nlevels + 1));
+      for (int ilev = nlevstart; ilev <= nlevels; ilev++)
+        mk_pw2der_tables(norder, npw, ts, xq, delta0, boxsize[ilev], tab_pw2p + (size_t)norder * npw * ilev,
+                         tab_pw2der + (size_t)norder * npw * ilev, tab_pw2dxx + (size_t)norder * npw * ilev);
     }
     nmaxms = nlevels - (npwlevel > 0 ? npwlevel : 0);
     wpwmsshift = malloc(sizeof(zc) * nexp * 4 * (nmaxms > 0 ? nmaxms : 1));
@@ -1386,7 +1531,7 @@ static void boxfgt_core(int nd, double delta, double eps, int ipoly, int *iperio
     if (info->ws) memcpy(info->ws, ws, sizeof(double) * npw);
   }
 
-  size_t ffsz = (size_t)norder * (hh > norder ? hh : norder) + (size_t)norder * norder;
+  size_t ffsz = 3 * ((size_t)norder * (hh > norder ? hh : norder) + (size_t)norder * norder);
   if (!direct_only) {
     /* STEP 1: leaf values -> mp PW (boxfgt.f:728-744) */
     t1 = wtime();
@@ -1474,9 +1619,16 @@ static void boxfgt_core(int nd, double delta, double eps, int ipoly, int *iperio
         zc *ff = malloc(sizeof(zc) * ffsz);
 #pragma omp for schedule(dynamic)
         for (int ibox = b0; ibox <= b1; ibox++) {
-          if (ifpwexp[ibox - 1] == 1 && IT(itree, iptr, 4, ibox) == 0)
-            g2d_pw2pot(nd, norder, npw, rmlexp + iaddr[2 * (ibox - 1) + 1], tab_pw2pot + (size_t)norder * npw * ilev,
-                       pot + (size_t)nd * npbox * (ibox - 1), ff);
+          if (ifpwexp[ibox - 1] == 1 && IT(itree, iptr, 4, ibox) == 0) {
+            if (ifpgh == 1)
+              g2d_pw2pot(nd, norder, npw, rmlexp + iaddr[2 * (ibox - 1) + 1],
+                         tab_pw2pot + (size_t)norder * npw * ilev, pot + (size_t)nd * npbox * (ibox - 1), ff);
+            else
+              g2d_pw2pgh(nd, norder, npw, rmlexp + iaddr[2 * (ibox - 1) + 1], tab_pw2p + (size_t)norder * npw * ilev,
+                         tab_pw2der + (size_t)norder * npw * ilev, tab_pw2dxx + (size_t)norder * npw * ilev, ifpgh,
+                         pot + (size_t)nd * npbox * (ibox - 1), grad + (size_t)nd * 2 * npbox * (ibox - 1),
+                         hess ? hess + (size_t)nd * 3 * npbox * (ibox - 1) : NULL, ff);
+          }
         }
         free(ff);
       }
@@ -1491,10 +1643,11 @@ static void boxfgt_core(int nd, double delta, double eps, int ipoly, int *iperio
     for (int ilev = 0; ilev <= nlevend; ilev++) {
       int b0 = LADDR(itree, 1, ilev), b1 = LADDR(itree, 2, ilev);
       const double *tl = tab_loc + ntabl * ilev;
+      const double *tlx = tabx_loc + ntabl * ilev, *tlxx = tabxx_loc + ntabl * ilev;
       const int *il = ind_loc + nindl * ilev;
 #pragma omp parallel
       {
-        double *ff = malloc(sizeof(double) * norder * norder);
+        double *ff = malloc(sizeof(double) * 3 * norder * norder);
 #pragma omp for schedule(dynamic)
         for (int ibox = b0; ibox <= b1; ibox++) {
           int nl1 = nlist1[ibox - 1];
@@ -1505,9 +1658,17 @@ static void boxfgt_core(int nd, double delta, double eps, int ipoly, int *iperio
             int ixyz[2];
             const double *fj = fvals + (size_t)nd * npbox * (jbox - 1);
             double *pi_ = pot + (size_t)nd * npbox * (ibox - 1);
+            double *gi_ = ifpgh >= 2 ? grad + (size_t)nd * 2 * npbox * (ibox - 1) : NULL;
+            double *hi_ = ifpgh == 3 ? hess + (size_t)nd * 3 * npbox * (ibox - 1) : NULL;
+#define NEAR_PAIR()                                                                                 \
+  do {                                                                                              \
+    if (ifpgh == 1) g2d_tens_prod_to_potloc(nd, norder, fj, pi_, nloctab, tl, il, ixyz, ff);        \
+    else g2d_tens_prod_to_pghloc(nd, norder, fj, ifpgh, pi_, gi_, hi_, nloctab, tl, tlx, tlxx, il,  \
+                                 ixyz, ff);                                                         \
+  } while (0)
             if (iperiod == 1 && jlev == 1) {
               gnd_find_loctab_ind(0, &CEN(centers, 1, ibox), &CEN(centers, 1, jbox), bs, bs0, mrefinelev, ixyz);
-              g2d_tens_prod_to_potloc(nd, norder, fj, pi_, nloctab, tl, il, ixyz, ff);
+              NEAR_PAIR();
               int nimage = 0, iimage[2];
               double dxyz[2], ctmp[2][3];
               double bsh = bs * 0.25;
@@ -1532,12 +1693,12 @@ static void boxfgt_core(int nd, double delta, double eps, int ipoly, int *iperio
                 for (int k = 1; k <= (1 << nimage) - 1; k++) {
                   double cc[2] = {ctmp[0][k - 1], ctmp[1][k - 1]};
                   gnd_find_loctab_ind(0, &CEN(centers, 1, ibox), cc, bs, bs0, mrefinelev, ixyz);
-                  g2d_tens_prod_to_potloc(nd, norder, fj, pi_, nloctab, tl, il, ixyz, ff);
+                  NEAR_PAIR();
                 }
               }
             } else {
               gnd_find_loctab_ind(iperiod, &CEN(centers, 1, ibox), &CEN(centers, 1, jbox), bs, bs0, mrefinelev, ixyz);
-              g2d_tens_prod_to_potloc(nd, norder, fj, pi_, nloctab, tl, il, ixyz, ff);
+              NEAR_PAIR();
             }
           }
         }
@@ -1552,7 +1713,8 @@ static void boxfgt_core(int nd, double delta, double eps, int ipoly, int *iperio
   free(xq); free(umat); free(vmat); free(wts); free(ifpwexp); free(list1); free(nlist1);
   free(tab_loc); free(tabx_loc); free(tabxx_loc); free(ind_loc);
   free(iaddr); free(rmlexp); free(nlistpw); free(listpw); free(tab_poly2pw); free(tab_pw2pot);
-  free(wpwmsshift); free(wpwshift);
+  free(wpwmsshift); free(wpwshift); free(tab_pw2p); free(tab_pw2der); free(tab_pw2dxx);
+#undef NEAR_PAIR
 }
 
 /* ------------------------------------------------------------------------- */
@@ -1568,7 +1730,18 @@ void oracle_boxfgt(int nd, double delta, double eps, int ipoly, int iperiod, int
   int ip = iperiod;
   double tinfo[20];
   boxfgt_core(nd, delta, eps, ipoly, &ip, norder, norder * norder, nboxes, nlevels, itree, iptr, centers, boxsize,
-              fvals, pot, timeinfo ? timeinfo : tinfo, info);
+              fvals, pot, timeinfo ? timeinfo : tinfo, info, 1, NULL, NULL);
+}
+
+/* The same with ifpgh = 1, 2 or 3: grad(nd,2,npbox,nboxes) and, for ifpgh = 3,
+   hess(nd,3,npbox,nboxes) (xx, xy, yy) are accumulated into as pot is. */
+void oracle_boxfgt_pgh(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
+                       int *itree, const int *iptr, const double *centers, const double *boxsize,
+                       const double *fvals, int ifpgh, double *pot, double *grad, double *hess) {
+  int ip = iperiod;
+  double tinfo[20];
+  boxfgt_core(nd, delta, eps, ipoly, &ip, norder, norder * norder, nboxes, nlevels, itree, iptr, centers, boxsize,
+              fvals, pot, tinfo, NULL, ifpgh, grad, hess);
 }
 
 void oracle_set_threads(int n) {

@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as the
 checker and by bench.py's CPU-baseline leg.  It restates the reference's
-boxfgt (bfgt/boxfgt.f:5-1591, ndim=2, ifpgh=1) in C.
+boxfgt (bfgt/boxfgt.f:5-1591, ndim=2, ifpgh=1, 2, 3) in C.
 """
 from __future__ import annotations
 
@@ -39,6 +39,10 @@ def lib():
         L.oracle_boxfgt.restype = None
         L.oracle_boxfgt.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                     _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, C.c_void_p, C.c_void_p]
+        L.oracle_boxfgt_pgh.restype = None
+        L.oracle_boxfgt_pgh.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int, _f64p, C.c_void_p,
+                                        C.c_void_p]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_max_threads.restype = C.c_int
         L.oracle_nodes.argtypes = [C.c_int, C.c_int, _f64p, _f64p, _f64p, _f64p]
@@ -117,6 +121,29 @@ def boxfgt(tree, fvals, delta, eps, nd=1, pot=None, itree=None, timeinfo=None, w
                     a["list1"].reshape(tree.nboxes, 64), a["nlistpw"], a["listpw"].reshape(tree.nboxes, 8),
                     a["ind_loc"], a["tab_loc"], a["ts"][: info.npw].copy(), a["ws"][: info.npw].copy())
     return out, oi, it
+
+
+def boxfgt_pgh(tree, fvals, delta, eps, ifpgh, nd=1, threads=0):
+    """Runs the oracle with ifpgh = 1, 2 or 3; returns (pot, grad, hess) in the
+    reference layouts pot(nd,npbox,nboxes), grad(nd,2,npbox,nboxes),
+    hess(nd,3,npbox,nboxes) (xx, xy, yy), flattened; grad/hess are None below
+    ifpgh 2/3."""
+    L = lib()
+    if threads:
+        L.oracle_set_threads(int(threads))
+    n = tree.norder
+    m = nd * n * n * tree.nboxes
+    fv = np.ascontiguousarray(fvals, dtype=np.float64).reshape(-1)
+    pot = np.zeros(m)
+    grad = np.zeros(2 * m) if ifpgh >= 2 else None
+    hess = np.zeros(3 * m) if ifpgh == 3 else None
+    it = np.array(tree.itree, dtype=np.int32).copy()
+    L.oracle_boxfgt_pgh(int(nd), float(delta), float(eps), int(tree.ipoly), int(tree.iperiod), int(n),
+                        int(tree.nboxes), int(tree.nlevels), it, np.ascontiguousarray(tree.iptr, dtype=np.int32),
+                        np.ascontiguousarray(tree.centers, dtype=np.float64).reshape(-1),
+                        np.ascontiguousarray(tree.boxsize, dtype=np.float64), fv, int(ifpgh), pot,
+                        None if grad is None else grad.ctypes.data, None if hess is None else hess.ctypes.data)
+    return pot, grad, hess
 
 
 def nodes(ipoly, n):

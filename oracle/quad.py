@@ -30,6 +30,15 @@ def _nodes(ipoly, n):
 
 def direct_pot(tree, fvals, delta, nd=1, nq=16):
     """pot(nd, npbox, nboxes) on leaf boxes (zeros elsewhere), layout of the reference."""
+    return direct_pgh(tree, fvals, delta, nd=nd, nq=nq, ifpgh=1)[0]
+
+
+def direct_pgh(tree, fvals, delta, nd=1, nq=16, ifpgh=1):
+    """(pot, grad, hess) on leaf boxes in the reference layouts pot(nd,npbox,nboxes),
+    grad(nd,2,npbox,nboxes), hess(nd,3,npbox,nboxes) (xx, xy, yy), flattened;
+    grad/hess are None below ifpgh 2/3.  Derivatives act on the target point:
+    d/dx exp(-d^2/delta) = -2 d/delta exp(-d^2/delta), d^2/dx^2 adds
+    (4 d^2/delta^2 - 2/delta)."""
     n = tree.norder
     npb = n * n
     x, U, vand = _nodes(tree.ipoly, n)
@@ -53,7 +62,9 @@ def direct_pot(tree, fvals, delta, nd=1, nq=16):
     out = np.zeros((tree.nboxes, npb, nd))
     reach = np.sqrt(delta * 45.0)
     M = int(np.ceil((reach + L) / L)) if tree.iperiod == 1 else 0
-    acc = np.zeros((len(leaves), npb, nd))
+    comps = [(0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2)][: {1: 1, 2: 3, 3: 6}[ifpgh]]
+    orders = {1: 1, 2: 2, 3: 3}[ifpgh]
+    acc = [np.zeros((len(leaves), npb, nd)) for _ in comps]
     for B in leaves:
         D = tree.boxsize[lev[B]]
         c = tree.centers[B]
@@ -64,21 +75,33 @@ def direct_pot(tree, fvals, delta, nd=1, nq=16):
         lag = vand(t) @ U            # (nquad, n): Lagrange basis at t
         lw = lag * w[:, None]
 
-        def integ(u, cc):
+        def integ(u, cc, order):
             y = cc + t * D / 2
             tot = np.zeros((len(u), n))
             for m in range(-M, M + 1):
                 d = u[:, None] - y[None, :] - m * L
                 K = np.exp(-(d * d) / delta)
+                if order == 1:
+                    K = K * (-2 * d / delta)
+                elif order == 2:
+                    K = K * (4 * d * d / delta ** 2 - 2 / delta)
                 tot += K @ lw
             return tot
 
-        Ix = integ(ux, c[0])          # (X, n)
-        Iy = integ(uy, c[1])          # (Y, n)
-        F = fv[B].reshape(n, n, nd, order="F") if False else fv[B].reshape(n, n, nd)  # [k2][k1][ind]
+        I = {(ax, o): integ(ux if ax == 0 else uy, c[ax], o) for ax in (0, 1) for o in range(orders)}
+        F = fv[B].reshape(n, n, nd)   # [k2][k1][ind]
         for ind in range(nd):
             Fm = F[:, :, ind].T       # [i=x][j=y]
-            A = Ix @ Fm               # (X, n): sum_i Ix[x,i] F[i,j]
-            acc[:, :, ind] += np.einsum("tpj,tpj->tp", A[tix], Iy[tiy])
-    out[leaves] = acc
-    return out.reshape(-1) if nd > 1 else out[:, :, 0].reshape(-1)
+            for q, (ox, oy) in enumerate(comps):
+                A = I[(0, ox)] @ Fm   # (X, n): sum_i Ix[x,i] F[i,j]
+                acc[q][:, :, ind] += np.einsum("tpj,tpj->tp", A[tix], I[(1, oy)][tiy])
+    res = []
+    for q in range(len(comps)):
+        o = np.zeros((tree.nboxes, npb, nd))
+        o[leaves] = acc[q]
+        res.append(o)
+    # C order of the Fortran arrays: (nboxes, npbox, ncomp, nd)
+    pot = res[0].reshape(-1)
+    grad = np.stack([res[1], res[2]], axis=2).reshape(-1) if ifpgh >= 2 else None
+    hess = np.stack([res[3], res[4], res[5]], axis=2).reshape(-1) if ifpgh == 3 else None
+    return pot, grad, hess

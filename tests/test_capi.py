@@ -55,7 +55,13 @@ def test_boxfgt_rejects_unsupported_flags():
     with pytest.raises(hb.BfgtError, match="ndim=2"):
         hb.boxfgt(1, 3, 1e-3, 1e-9, 0, 1, 8, 64, t.nboxes, t.nlevels, t.ltree, t.itree.copy(), t.iptr, t.centers,
                   t.boxsize, t.fvals, 1, pot, None, None, 0, 0, None, 0, None, None, None, ti)
-    with pytest.raises(hb.BfgtError, match="ifpgh=1"):
+    with pytest.raises(hb.BfgtError, match="grad/hess"):      # ifpgh=2 needs a grad array
         hb.boxfgt(1, 2, 1e-3, 1e-9, 0, 1, 8, 64, t.nboxes, t.nlevels, t.ltree, t.itree.copy(), t.iptr, t.centers,
                   t.boxsize, t.fvals, 2, pot, None, None, 0, 0, None, 0, None, None, None, ti)
+    with pytest.raises(hb.BfgtError, match="ifpgh=1,2,3"):
+        hb.boxfgt(1, 2, 1e-3, 1e-9, 0, 1, 8, 64, t.nboxes, t.nlevels, t.ltree, t.itree.copy(), t.iptr, t.centers,
+                  t.boxsize, t.fvals, 4, pot, None, None, 0, 0, None, 0, None, None, None, ti)
+    with pytest.raises(hb.BfgtError, match="ifnewtree=0"):
+        hb.boxfgt(1, 2, 1e-3, 1e-9, 0, 1, 8, 64, t.nboxes, t.nlevels, t.ltree, t.itree.copy(), t.iptr, t.centers,
+                  t.boxsize, t.fvals, 1, pot, None, None, 1, 0, None, 0, None, None, None, ti)
     assert not pot.any()

@@ -175,3 +175,44 @@ def test_gradient_matches_central_differences(precision, tol):
     fd, an = np.array(fd), np.array(an)
     err = np.linalg.norm(fd - an) / np.linalg.norm(fd)
     assert err <= tol, err
+
+
+@pytest.mark.parametrize("precision", [hb.BFGT_PREC_FP64, hb.BFGT_PREC_SPLIT])
+def test_delta_gradient_matches_central_differences(precision, tol=1e-6):
+    """dJ/ddelta through autograd (the hessian identity of fgt_autograd) vs
+    central differences of the FP64 transform in delta, relative step 1e-6, on
+    the same order-16 tree at delta = 1e-3 (eps = 1e-9).  The identity is the
+    derivative of the exact Gaussian kernel; the differences see the discrete
+    transform, whose approximation error also moves with delta, so the two
+    agree to the transform's accuracy (about 2e-7 here), within the 1e-6 bar."""
+    import torch
+    from fgt_autograd import BoxFgtDelta, PlanCache, gauss_at_points
+
+    t = _c4_tree()
+    delta, eps = 1e-3, 1e-9
+    lv = t.leaves()
+    gpar = gauss_sum(3, 20, 1e-3, 1e-2, amp="normal", log_width=True)
+    gt = np.zeros((t.nboxes, t.npbox))
+    gt[lv] = gauss_at_points(t.grid_points(lv), gpar)
+    f0 = np.zeros((t.nboxes, t.npbox))
+    f0[lv] = t.fvals[lv]
+    dev = torch.device("cuda")
+    g = torch.from_numpy(gt.reshape(-1)).to(dev)
+    f = torch.from_numpy(f0.reshape(-1)).to(dev)
+    cache = PlanCache(t, eps, precision)
+    d = torch.tensor([delta], dtype=torch.float64, device=dev, requires_grad=True)
+    r = BoxFgtDelta.apply(f, d, cache) - g
+    J = 0.5 * torch.sum(r * r)
+    J.backward()
+    an = d.grad.item()
+    ref = PlanCache(t, eps, hb.BFGT_PREC_FP64)
+    h = 1e-6 * delta
+    with torch.no_grad():
+        rp = BoxFgtDelta.apply(f, torch.tensor([delta + h], dtype=torch.float64, device=dev), ref) - g
+        rm = BoxFgtDelta.apply(f, torch.tensor([delta - h], dtype=torch.float64, device=dev), ref) - g
+        fd = (0.5 * torch.sum((rp - rm) * (rp + rm))).item() / (2 * h)
+    for pl in list(cache.plans.values()) + list(ref.plans.values()):
+        assert pl.info()["npw"] == next(iter(ref.plans.values())).info()["npw"]
+    cache.close()
+    ref.close()
+    assert abs(fd - an) <= tol * abs(fd), (fd, an)

@@ -92,3 +92,38 @@ def test_oracle_golden_vectors():
         got = p[idx[:, 0], idx[:, 1]]
         err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
         assert err < 10 * case["eps"], (case["name"], err)
+
+
+PGH_CASES = [("uni3_leg_per", 1e-3, 1e-9), ("uni3_cheb_per", 1e-2, 1e-9), ("uni3_leg_per", 4e-4, 1e-9),
+             ("uni3_leg_free", 1e-3, 1e-9), ("ad_leg_per", 1e-4, 1e-9), ("lev1_leaf_per", 1e-3, 1e-9)]
+
+
+@pytest.mark.parametrize("name,delta,eps", PGH_CASES)
+def test_oracle_gradient_hessian_vs_quadrature(trees, name, delta, eps):
+    """ifpgh = 3 (g2d_pw2pgh, g2d_tens_prod_to_pghloc restated) against the
+    direct quadrature of the kernel's first and second derivatives.  The
+    derivatives carry the transform's error times 1/sqrt(delta) per order, so
+    the bars are 100 eps (gradient) and 1000 eps (hessian); pot must equal the
+    ifpgh = 1 result bit for bit."""
+    t = trees[name]
+    p1 = oracle.boxfgt(t, t.fvals, delta, eps)
+    p, g, h = oracle.boxfgt_pgh(t, t.fvals, delta, eps, 3)
+    np.testing.assert_array_equal(p, p1)
+    qp, qg, qh = quad.direct_pgh(t, t.fvals, delta, ifpgh=3)
+    assert rel_l2(leaf_vals(t, p), leaf_vals(t, qp)) < 10 * eps
+    assert rel_l2(leaf_vals(t, g), leaf_vals(t, qg)) < 100 * eps
+    assert rel_l2(leaf_vals(t, h), leaf_vals(t, qh)) < 1000 * eps
+    p2, g2, h2 = oracle.boxfgt_pgh(t, t.fvals, delta, eps, 2)
+    np.testing.assert_array_equal(p2, p1)
+    np.testing.assert_array_equal(g2, g)
+    assert h2 is None
+
+
+def test_oracle_gradient_multiple_densities(trees):
+    t = trees["ad_cheb_free"]
+    nd = 2
+    rng = np.random.default_rng(3)
+    fv = np.stack([t.fvals, rng.standard_normal(t.fvals.shape) * (t.nchild() == 0)[:, None]], axis=2)
+    _, g, _ = oracle.boxfgt_pgh(t, fv, 1e-3, 1e-9, 2, nd=nd)
+    _, qg, _ = quad.direct_pgh(t, fv, 1e-3, nd=nd, ifpgh=2)
+    assert rel_l2(leaf_vals(t, g), leaf_vals(t, qg)) < 1e-7

@@ -80,6 +80,8 @@ def lib():
     L.bfgt_plan_execute_pgh.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 5
     L.bfgt_plan_execute_pgh_host.restype = C.c_int
     L.bfgt_plan_execute_pgh_host.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 5
+    L.bfgt_plan_eval_targets.restype = C.c_int
+    L.bfgt_plan_eval_targets.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
     L.bfgt_plan_execute_adjoint.restype = C.c_int
     L.bfgt_plan_execute_adjoint.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.bfgt_plan_execute_adjoint_host.restype = C.c_int

@@ -24,7 +24,7 @@ def _arr(a):
     if a is None:
         return None
     if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
-        raise TypeError("grad/hess must be C-contiguous float64 numpy arrays")
+        raise TypeError("grad/hess/targs/pote/grade/hesse must be C-contiguous float64 numpy arrays")
     return a.ctypes.data
 
 
@@ -49,8 +49,7 @@ def boxfgt(nd, ndim, delta, eps, ipoly, iperiod, norder, npbox, nboxes, nlevels,
     L.boxfgt_(_iref(nd), _iref(ndim), C.byref(dl), C.byref(ep), _iref(ipoly), C.byref(ip), _iref(norder), _iref(npbox),
               C.byref(nb), C.byref(nl), C.byref(lt), itree.reshape(-1), iptr, centers.reshape(-1), boxsize,
               fvals.reshape(-1), _iref(ifpgh), pot.reshape(-1), _arr(grad), _arr(hess), _iref(ifnewtree), _iref(ntarg),
-              None,
-              _iref(ifpghtarg), None, None, None, timeinfo)
+              _arr(targs), _iref(ifpghtarg), _arr(pote), _arr(grade), _arr(hesse), timeinfo)
     err = _lib.last_error()
     if err:
         raise BfgtError(1, err)
@@ -127,6 +126,12 @@ class Plan:
                                                       None if grad is None else grad.ctypes.data,
                                                       None if hess is None else hess.ctypes.data, s))
         return pot, grad, hess
+
+    def eval_targets(self, ncomp, d_vals, ntarg, d_targs, d_out, stream=None):
+        """out(nd*ncomp, ntarg) = leaf interpolants of vals(nd*ncomp, npbox, nboxes) at targs(2, ntarg)."""
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_plan_eval_targets(self._h, int(ncomp), self._ptr(d_vals), int(ntarg),
+                                                  self._ptr(d_targs), self._ptr(d_out), s))
 
     def execute_adjoint(self, d_potbar, d_fbar, stream=None):
         """fbar += K^T potbar on leaf boxes (the transpose of execute: pot += K fvals)."""

@@ -1,6 +1,7 @@
 // C ABI of libbfgt_b200.so (declared in include/bfgt.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -8,6 +9,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/bfgt.h"
 #include "batch.hpp"
@@ -86,8 +88,9 @@ int bfgt_plan_create(bfgt_plan *plan, int nd, double delta, double eps, int ipol
   *plan = nullptr;
   if (precision != BFGT_PREC_FP64 && precision != BFGT_PREC_SPLIT) return fail(BFGT_ERR_ARG, "unknown precision mode");
   std::unique_ptr<bfgt_plan_s> p(new bfgt_plan_s());
+  bfgt::TreeView t;
   try {
-    bfgt::TreeView t = make_view(nboxes, nlevels, ltree, itree, iptr, centers, boxsize);
+    t = make_view(nboxes, nlevels, ltree, itree, iptr, centers, boxsize);
     bfgt::build_host_plan(p->hp, t, nd, delta, eps, ipoly, iperiod, norder, precision);
     constexpr int kMaxGap = 64;  // non-leaf boxes copied rather than starting a new run
     for (int b = 1; b <= nboxes; b++) {
@@ -102,6 +105,7 @@ int bfgt_plan_create(bfgt_plan *plan, int nd, double delta, double eps, int ipol
   }
   std::string msg;
   int rc = bfgt::device_plan_create(p->dp, p->hp, msg);
+  if (rc == BFGT_OK) rc = bfgt::device_plan_prepare_targets(p->dp, p->hp, t, msg);
   if (rc != BFGT_OK) {
     bfgt::device_plan_destroy(p->dp);
     return fail(rc, msg);
@@ -185,6 +189,44 @@ int execute_host_on(bfgt_plan plan, bfgt::DevicePlan &dp, const double *in, doub
   return BFGT_OK;
 }
 
+// Step 11 on the values a host execute left in dp's staging buffers (pot and,
+// as ifpghtarg asks, grad and hess): pote/grade/hesse are overwritten.
+int targets_host_on(bfgt::DevicePlan &dp, int ifpghtarg, int ntarg, const double *targs, double *pote,
+                    double *grade, double *hesse, cudaStream_t s) {
+  if (ntarg <= 0) return BFGT_OK;
+  const size_t elems = (size_t)dp.nd * dp.n * dp.n * dp.nboxes;
+  double *d_t = nullptr, *d_o = nullptr;
+  if (cudaMalloc(&d_t, sizeof(double) * 2 * (size_t)ntarg) != cudaSuccess ||
+      cudaMalloc(&d_o, sizeof(double) * 3 * (size_t)dp.nd * ntarg) != cudaSuccess) {
+    cudaGetLastError();
+    if (d_t) cudaFree(d_t);
+    return fail(BFGT_ERR_OOM, "cannot allocate target buffers");
+  }
+  int rc = BFGT_OK;
+  std::string msg;
+  struct Part {
+    int ncomp;
+    const double *vals;
+    double *out;
+  };
+  const Part parts[3] = {{1, dp.d_stage_p, pote}, {2, dp.d_stage_gh, grade}, {3, dp.d_stage_gh + 2 * elems, hesse}};
+  if (cudaMemcpyAsync(d_t, targs, sizeof(double) * 2 * (size_t)ntarg, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    rc = fail(BFGT_ERR_CUDA, "target upload failed");
+  for (int p = 0; p < ifpghtarg && rc == BFGT_OK; p++) {
+    const Part &pt = parts[p];
+    int r = bfgt::device_plan_eval_targets(dp, pt.ncomp, pt.vals, ntarg, d_t, d_o, s, msg);
+    if (r != BFGT_OK) rc = fail(r, msg);
+    else if (cudaMemcpyAsync(pt.out, d_o, sizeof(double) * pt.ncomp * dp.nd * (size_t)ntarg, cudaMemcpyDeviceToHost,
+                             s) != cudaSuccess)
+      rc = fail(BFGT_ERR_CUDA, "target download failed");
+    else if (cudaStreamSynchronize(s) != cudaSuccess)
+      rc = fail(BFGT_ERR_CUDA, std::string("target evaluation failed: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  cudaFree(d_t);
+  cudaFree(d_o);
+  return rc;
+}
+
 // Uploads the derivative tables on first use.
 int ensure_pgh(bfgt_plan plan) {
   if (plan->dp.pgh_ready) return BFGT_OK;
@@ -260,6 +302,19 @@ int bfgt_plan_execute_pgh_host(bfgt_plan plan, int ifpgh, const double *fvals, d
     if (rc != BFGT_OK) return rc;
   }
   return execute_host_on(plan, plan->dp, fvals, pot, (cudaStream_t)stream, ifpgh, grad, hess);
+}
+
+int bfgt_plan_eval_targets(bfgt_plan plan, int ncomp, const double *d_vals, int ntarg, const double *d_targs,
+                           double *d_out, void *stream) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (ncomp < 1 || ncomp > 3) return fail(BFGT_ERR_ARG, "ncomp must be 1, 2 or 3");
+  if (ntarg < 0) return fail(BFGT_ERR_ARG, "ntarg is negative");
+  if (ntarg > 0 && (!d_vals || !d_targs || !d_out)) return fail(BFGT_ERR_ARG, "vals/targs/out device pointers are NULL");
+  std::string msg;
+  int rc = bfgt::device_plan_eval_targets(plan->dp, ncomp, d_vals, ntarg, d_targs, d_out, (cudaStream_t)stream, msg);
+  if (rc != BFGT_OK) return fail(rc, msg);
+  return BFGT_OK;
 }
 
 int bfgt_plan_execute_adjoint(bfgt_plan plan, const double *d_potbar, double *d_fbar, void *stream) {
@@ -418,14 +473,32 @@ namespace {
 int boxfgt_impl(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
                 int ltree, int *itree, const int *iptr, const double *centers, const double *boxsize,
                 const double *fvals, int ifpgh, double *pot, double *grad, double *hess, double *timeinfo,
-                int precision) {
+                int precision, int ntarg = 0, const double *targs = nullptr, int ifpghtarg = 0,
+                double *pote = nullptr, double *grade = nullptr, double *hesse = nullptr) {
   double t0 = now_s();
   bfgt_plan plan = nullptr;
   int rc = bfgt_plan_create(&plan, nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree, iptr,
                             centers, boxsize, precision);
   if (rc != BFGT_OK) return rc;
   double t1 = now_s();
-  rc = bfgt_plan_execute_pgh_host(plan, ifpgh, fvals, pot, grad, hess, nullptr);
+  // as boxfgt.f:207-276: when the targets ask for more derivatives than the
+  // boxes, the transform computes them into zeroed internal arrays
+  const int ifpgh2 = std::max(ifpgh, ifpghtarg);
+  const size_t elems = (size_t)nd * norder * norder * nboxes;
+  std::vector<double> g2, h2;
+  double *gp = grad, *hp = hess;
+  if (ifpgh2 >= 2 && ifpgh < 2) {
+    g2.assign(2 * elems, 0.0);
+    gp = g2.data();
+  }
+  if (ifpgh2 == 3 && ifpgh < 3) {
+    h2.assign(3 * elems, 0.0);
+    hp = h2.data();
+  }
+  rc = bfgt_plan_execute_pgh_host(plan, ifpgh2, fvals, pot, gp, hp, nullptr);
+  double t2 = now_s();
+  if (rc == BFGT_OK && ifpghtarg > 0) rc = targets_host_on(plan->dp, ifpghtarg, ntarg, targs, pote, grade, hesse, nullptr);
+  const double t_targ = now_s() - t2;
   if (rc == BFGT_OK) rc = bfgt_plan_check(plan);
   if (rc == BFGT_OK && timeinfo) {
     double st[8];
@@ -438,6 +511,7 @@ int boxfgt_impl(int nd, double delta, double eps, int ipoly, int iperiod, int no
     timeinfo[4] = 0;                 // step 4 is fused into step 5
     timeinfo[5] = st[3] * 1e-3;      // steps 4+5: cutoff expansions -> leaf values
     timeinfo[6] = st[4] * 1e-3;      // step 6: near field
+    timeinfo[11] = ifpghtarg > 0 ? t_targ : 0;  // step 11: extra targets
   }
   std::string keep = g_err;
   bfgt_plan_destroy(plan);
@@ -461,10 +535,6 @@ void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *
              double *centers, double *boxsize, const double *fvals, const int *ifpgh, double *pot, double *grad,
              double *hess, const int *ifnewtree, const int *ntarg, const double *targs, const int *ifpghtarg,
              double *pote, double *grade, double *hesse, double *timeinfo) {
-  (void)targs;
-  (void)pote;
-  (void)grade;
-  (void)hesse;
   g_err.clear();
   if (!nd || !ndim || !delta || !eps || !ipoly || !iperiod || !norder || !npbox || !nboxes || !nlevels || !ltree ||
       !ifpgh || !ifnewtree || !ntarg || !ifpghtarg) {
@@ -475,12 +545,17 @@ void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *
     fail(BFGT_ERR_ARG, "boxfgt_: only ndim=2 is supported");
     return;
   }
-  if (*ifpgh < 1 || *ifpgh > 3 || *ifpghtarg > 0 || *ifnewtree != 0) {
-    fail(BFGT_ERR_ARG, "boxfgt_: only ifpgh=1,2,3 with ifpghtarg=0, ifnewtree=0 are supported");
+  if (*ifpgh < 1 || *ifpgh > 3 || *ifpghtarg < 0 || *ifpghtarg > 3 || *ifnewtree != 0) {
+    fail(BFGT_ERR_ARG, "boxfgt_: only ifpgh=1,2,3, ifpghtarg=0..3 with ifnewtree=0 are supported");
     return;
   }
   if ((*ifpgh >= 2 && !grad) || (*ifpgh == 3 && !hess)) {
     fail(BFGT_ERR_ARG, "boxfgt_: grad/hess arrays are NULL");
+    return;
+  }
+  if (*ifpghtarg > 0 && *ntarg > 0 &&
+      (!targs || !pote || (*ifpghtarg >= 2 && !grade) || (*ifpghtarg == 3 && !hesse))) {
+    fail(BFGT_ERR_ARG, "boxfgt_: targs/pote/grade/hesse arrays are NULL");
     return;
   }
   if (*npbox != (*norder) * (*norder)) {
@@ -489,7 +564,8 @@ void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *
   }
   double ti[20];
   boxfgt_impl(*nd, *delta, *eps, *ipoly, *iperiod, *norder, *nboxes, *nlevels, *ltree, itree, iptr, centers, boxsize,
-              fvals, *ifpgh, pot, grad, hess, timeinfo ? timeinfo : ti, BFGT_PREC_FP64);
+              fvals, *ifpgh, pot, grad, hess, timeinfo ? timeinfo : ti, BFGT_PREC_FP64, *ntarg, targs, *ifpghtarg,
+              pote, grade, hesse);
 }
 
 int bfgt_host_plan_dump(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes,

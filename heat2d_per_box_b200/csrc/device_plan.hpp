@@ -51,6 +51,13 @@ struct DevicePlan {
   double2 *dfac = nullptr, *Ld = nullptr;
   double *tab3_loc = nullptr;
   bool pgh_ready = false;
+  // extra targets (built on first use): the tree on the device (0-based box
+  // ids), the values->coefficients matrix, and scratch
+  int *t_nchild = nullptr, *t_ichild = nullptr, *t_level = nullptr, *t_has = nullptr, *t_leaf = nullptr;
+  double *t_centers = nullptr, *t_boxsize = nullptr, *t_umat = nullptr, *t_coefs = nullptr;
+  size_t t_coef_elems = 0;
+  int t_leaf_cap = 0, ipoly = 0;
+  bool targ_ready = false;
   double2 *Mpart = nullptr;     // (nchunks, nd, nexp) partial expansions per chunk
   double2 *M = nullptr;         // (ncut, nd, nexp) cutoff-box expansions
   double2 *L = nullptr;         // (ncut, nd, nexp) cutoff-box local expansions
@@ -93,6 +100,12 @@ int device_plan_prepare_pgh(DevicePlan &dp, const HostPlan &hp, std::string &msg
 // ifpgh = 3 also hess(nd,3,npbox,nboxes) (xx, xy, yy).
 int device_plan_execute_pgh(DevicePlan &dp, int ifpgh, const double *d_fvals, double *d_pot, double *d_grad,
                             double *d_hess, cudaStream_t stream, std::string &msg);
+// Uploads the tree arrays used by device_plan_eval_targets.
+int device_plan_prepare_targets(DevicePlan &dp, const HostPlan &hp, const TreeView &t, std::string &msg);
+// out(nd*ncomp, nt) = the leaf interpolant of vals(nd*ncomp, n*n, nboxes) at
+// targs(2, nt) (boxfgt.f step 11).  Grows its scratch when needed.
+int device_plan_eval_targets(DevicePlan &dp, int ncomp, const double *d_vals, int nt, const double *d_targs,
+                             double *d_out, cudaStream_t s, std::string &msg);
 // Queues the transform on stream; returns BFGT_* status.
 int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cudaStream_t stream,
                         std::string &msg);

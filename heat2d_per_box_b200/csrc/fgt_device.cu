@@ -717,7 +717,7 @@ void device_plan_destroy(DevicePlan &dp) {
   if (dp.graph) cudaGraphDestroy(dp.graph);
   split_plan_destroy(dp);
   void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.columns, dp.cut_chunk_begin, dp.cut_pw_begin,
-                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.kscale, dp.dfac, dp.Ld, dp.tab3_loc, dp.Mpart, dp.M, dp.L, dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups, dp.nf_target,
+                  dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.kscale, dp.dfac, dp.Ld, dp.tab3_loc, dp.t_nchild, dp.t_ichild, dp.t_level, dp.t_centers, dp.t_boxsize, dp.t_umat, dp.t_has, dp.t_coefs, dp.t_leaf, dp.Mpart, dp.M, dp.L, dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups, dp.nf_target,
                   dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.d_stage_f, dp.d_stage_p, dp.d_stage_gh};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -917,6 +917,186 @@ int device_plan_execute_pgh(DevicePlan &dp, int ifpgh, const double *d_fvals, do
       }
     }
   }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    msg = std::string("kernel launch failed: ") + cudaGetErrorString(e);
+    return BFGT_ERR_CUDA;
+  }
+  return BFGT_OK;
+}
+
+// ---- extra targets (boxfgt.f step 11) ---------------------------------------
+
+namespace {
+
+struct TargArgs {
+  const int *nchild, *ichild, *level;  // per box (0-based ids); ichild(4, nboxes), 0-based, -1 none
+  const double *centers, *boxsize;     // (2, nboxes), (0:nlevels)
+  const double *umat;                  // values -> coefficients (n, n), column-major
+  int n, ipoly;
+};
+
+// Leaf box of each target, by the descent of pts_tree_sort
+// (common/pts_tree_nd.f:1226-1260, find_childbox_ind 713-740): child
+// 1 + (x - cx >= 0) + 2 (y - cy >= 0) from the root until a leaf.  Marks the
+// leaves that hold targets.
+__global__ void k_target_leaf(TargArgs a, const double *__restrict__ targs, int nt, int *__restrict__ leaf_of,
+                              int *__restrict__ has_targ) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const double x = targs[2 * (size_t)t], y = targs[2 * (size_t)t + 1];
+  int b = 0;
+  while (a.nchild[b] > 0) {
+    const int k = (x - a.centers[2 * (size_t)b] >= 0 ? 1 : 0) + (y - a.centers[2 * (size_t)b + 1] >= 0 ? 2 : 0);
+    b = a.ichild[4 * (size_t)b + k];
+  }
+  leaf_of[t] = b;
+  has_targ[b] = 1;
+}
+
+// Coefficients of the leaves that hold targets: ortho_trans_2d with itype 0
+// (common/tensor_prod_routs_nd.f:103-170), one warp per box, ndc components.
+__global__ void __launch_bounds__(128) k_leaf_coefs(TargArgs a, const double *__restrict__ vals,
+                                                    double *__restrict__ coefs, const int *__restrict__ has_targ,
+                                                    int nboxes, int ndc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = blockIdx.x * 4 + warp;
+  if (b >= nboxes || !has_targ[b]) return;
+  const int n = a.n, npb = n * n;
+  double *sw = reinterpret_cast<double *>(smem_raw) + (size_t)warp * npb;
+  const double *fin = vals + (size_t)b * ndc * npb;
+  double *fout = coefs + (size_t)b * ndc * npb;
+  for (int ind = 0; ind < ndc; ind++) {
+    // work(k, j) = sum_k1 umat(k, k1) fin(k1, j)
+    for (int o = lane; o < npb; o += 32) {
+      const int k = o % n, j = o / n;
+      double dd = 0;
+      for (int k1 = 0; k1 < n; k1++) dd = fma(a.umat[k + n * k1], fin[ind + (size_t)ndc * (k1 + n * j)], dd);
+      sw[o] = dd;
+    }
+    __syncwarp();
+    // fout(k, i) = sum_i1 umat(i, i1) work(k, i1)
+    for (int o = lane; o < npb; o += 32) {
+      const int k = o % n, i = o / n;
+      double dd = 0;
+      for (int i1 = 0; i1 < n; i1++) dd = fma(a.umat[i + n * i1], sw[k + n * i1], dd);
+      fout[ind + (size_t)ndc * o] = dd;
+    }
+    __syncwarp();
+  }
+}
+
+// out(ndc, t) = sum_j py(j) sum_k coefs(k, j) px(k) at the target's local
+// coordinates (t - c) 2 / boxsize (ortho_evalt_2d, tensor_prod_routs_nd.f:
+// 2030-2066; legepols / chebpols recurrences), one thread per target.
+__global__ void __launch_bounds__(128) k_eval_targets(TargArgs a, const double *__restrict__ coefs,
+                                                      const double *__restrict__ targs, const int *__restrict__ leaf_of,
+                                                      int nt, int ndc, double *__restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const int n = a.n, npb = n * n;
+  const int b = leaf_of[t];
+  const double sc = 2.0 / a.boxsize[a.level[b]];
+  const double x = (targs[2 * (size_t)t] - a.centers[2 * (size_t)b]) * sc;
+  const double y = (targs[2 * (size_t)t + 1] - a.centers[2 * (size_t)b + 1]) * sc;
+  double px[16];
+  px[0] = 1.0;
+  px[1] = x;
+#pragma unroll
+  for (int k = 1; k < 15; k++) {
+    if (k + 1 < n) {
+      if (a.ipoly == 0) px[k + 1] = ((2 * k + 1) * x * px[k] - k * px[k - 1]) / (k + 1);
+      else px[k + 1] = 2 * x * px[k] - px[k - 1];
+    }
+  }
+  const double *c = coefs + (size_t)b * ndc * npb;
+  for (int ind = 0; ind < ndc; ind++) {
+    double pot = 0;
+    double pym = 1.0, py = 1.0;  // P_{j-1}(y), P_j(y) by the same recurrence
+#pragma unroll 1
+    for (int j = 0; j < n; j++) {
+      if (j == 1) py = y;
+      else if (j > 1) {
+        const double pn = a.ipoly == 0 ? ((2 * (j - 1) + 1) * y * py - (j - 1) * pym) / j : 2 * y * py - pym;
+        pym = py;
+        py = pn;
+      }
+      if (j == 1) pym = 1.0;
+      double pp = 0;
+      const double *cj = c + ind + (size_t)ndc * n * j;
+#pragma unroll
+      for (int k = 0; k < 16; k++)
+        if (k < n) pp = pp + cj[(size_t)ndc * k] * px[k];
+      pot = pot + pp * py;
+    }
+    out[ind + (size_t)ndc * t] = pot;
+  }
+}
+
+}  // namespace
+
+int device_plan_prepare_targets(DevicePlan &dp, const HostPlan &hp, const TreeView &t, std::string &msg) {
+  if (dp.targ_ready) return BFGT_OK;
+  const int nb = t.nboxes;
+  std::vector<int> nchild(nb), ichild(4 * (size_t)nb), level(nb);
+  std::vector<double> cen(2 * (size_t)nb), bs(t.boxsize, t.boxsize + t.nlevels + 1);
+  for (int b = 1; b <= nb; b++) {
+    nchild[b - 1] = t.nchild(b);
+    level[b - 1] = t.ilevel(b);
+    for (int j = 1; j <= 4; j++) ichild[4 * (size_t)(b - 1) + j - 1] = t.nchild(b) > 0 ? t.ichild(j, b) - 1 : -1;
+    cen[2 * (size_t)(b - 1)] = t.cen(1, b);
+    cen[2 * (size_t)(b - 1) + 1] = t.cen(2, b);
+  }
+  std::vector<double> x, u, v, w;
+  leaf_nodes(hp.ipoly, hp.norder, x, u, v, w);
+  int rc = BFGT_OK;
+  auto chk = [&](int r) {
+    if (rc == BFGT_OK && r != BFGT_OK) rc = r;
+  };
+  chk(upload(dp.t_nchild, nchild, msg));
+  chk(upload(dp.t_ichild, ichild, msg));
+  chk(upload(dp.t_level, level, msg));
+  chk(upload(dp.t_centers, cen, msg));
+  chk(upload(dp.t_boxsize, bs, msg));
+  chk(upload(dp.t_umat, u, msg));
+  chk(alloc_bytes((void **)&dp.t_has, sizeof(int) * (size_t)nb, msg));
+  if (rc == BFGT_OK) {
+    dp.targ_ready = true;
+    dp.ipoly = hp.ipoly;
+  }
+  return rc;
+}
+
+int device_plan_eval_targets(DevicePlan &dp, int ncomp, const double *d_vals, int nt, const double *d_targs,
+                             double *d_out, cudaStream_t s, std::string &msg) {
+  if (!dp.targ_ready) {
+    msg = "target tables are not prepared";
+    return BFGT_ERR_ARG;
+  }
+  if (nt <= 0) return BFGT_OK;
+  const int ndc = dp.nd * ncomp, npb = dp.n * dp.n;
+  const size_t celems = (size_t)ndc * npb * dp.nboxes;
+  if (dp.t_coef_elems < celems) {
+    if (dp.t_coefs) cudaFree(dp.t_coefs);
+    dp.t_coefs = nullptr;
+    dp.t_coef_elems = 0;
+    if (alloc_bytes((void **)&dp.t_coefs, sizeof(double) * celems, msg) != BFGT_OK) return BFGT_ERR_OOM;
+    dp.t_coef_elems = celems;
+  }
+  if (dp.t_leaf_cap < nt) {
+    if (dp.t_leaf) cudaFree(dp.t_leaf);
+    dp.t_leaf = nullptr;
+    dp.t_leaf_cap = 0;
+    if (alloc_bytes((void **)&dp.t_leaf, sizeof(int) * (size_t)nt, msg) != BFGT_OK) return BFGT_ERR_OOM;
+    dp.t_leaf_cap = nt;
+  }
+  TargArgs a{dp.t_nchild, dp.t_ichild, dp.t_level, dp.t_centers, dp.t_boxsize, dp.t_umat, dp.n, dp.ipoly};
+  cudaMemsetAsync(dp.t_has, 0, sizeof(int) * (size_t)dp.nboxes, s);
+  k_target_leaf<<<(nt + 127) / 128, 128, 0, s>>>(a, d_targs, nt, dp.t_leaf, dp.t_has);
+  k_leaf_coefs<<<(dp.nboxes + 3) / 4, 128, sizeof(double) * 4 * npb, s>>>(a, d_vals, dp.t_coefs, dp.t_has, dp.nboxes,
+                                                                           ndc);
+  k_eval_targets<<<(nt + 127) / 128, 128, 0, s>>>(a, dp.t_coefs, d_targs, dp.t_leaf, nt, ndc, d_out);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     msg = std::string("kernel launch failed: ") + cudaGetErrorString(e);

@@ -46,12 +46,15 @@ extern "C" {
                                    FP64 phases and FP64 cross-leaf accumulation */
 
 /* Replaces bfgt/boxfgt.f:5-286 (boxfgt).  Supported: ndim=2, ifpgh=1, 2, 3,
-   ifnewtree=0, ifpghtarg=0 (ifpgh=1 is what every solver in the reference
-   uses, hpots/hpots2dadap.f:79-106).  pot (and grad(nd,2,npbox,nboxes),
-   hess(nd,3,npbox,nboxes) as ifpgh asks) are accumulated into, on leaf boxes
-   only; the colleague arrays itree(iptr(6)), itree(iptr(7)) are recomputed as
-   the reference does (boxfgt.f:516-528); timeinfo(1:20) is zeroed and filled
-   with per-stage seconds. */
+   ifpghtarg=0..3, ifnewtree=0 (ifpgh=1, ifpghtarg=0 is what every solver in
+   the reference uses, hpots/hpots2dadap.f:79-106).  pot (and
+   grad(nd,2,npbox,nboxes), hess(nd,3,npbox,nboxes) as ifpgh asks) are
+   accumulated into, on leaf boxes only; with ifpghtarg >= 1 the leaf
+   interpolants of pot (and grad, hess) are evaluated at targs(2,ntarg) into
+   pote(nd,ntarg), grade(nd,2,ntarg), hesse(nd,3,ntarg), overwritten
+   (boxfgt.f:207-276, 1494-1563).  The colleague arrays itree(iptr(6)),
+   itree(iptr(7)) are recomputed as the reference does (boxfgt.f:516-528);
+   timeinfo(1:20) is zeroed and filled with per-stage seconds. */
 void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *eps, const int *ipoly,
              int *iperiod, const int *norder, const int *npbox, int *nboxes, int *nlevels, int *ltree,
              int *itree, int *iptr, double *centers, double *boxsize, const double *fvals, const int *ifpgh,
@@ -105,6 +108,17 @@ int bfgt_plan_execute_pgh(bfgt_plan plan, int ifpgh, const double *d_fvals, doub
 /* The same on host arrays (leaf boxes copied in and out). */
 int bfgt_plan_execute_pgh_host(bfgt_plan plan, int ifpgh, const double *fvals, double *pot, double *grad,
                                double *hess, void *stream);
+
+/* Replaces bfgt/boxfgt.f step 11 (1494-1563: treedata_trans_nd and
+   treedata_evalt_nd, common/tree_data_routs_nd.f:16-60, 710-780, with the
+   target sort of pts_tree_sort, common/pts_tree_nd.f:1226-1260) on device
+   arrays: out(nd*ncomp, ntarg) = the leaf interpolants of
+   vals(nd*ncomp, norder**2, nboxes) at targs(2, ntarg), overwritten.  ncomp is
+   1 for pot, 2 for grad, 3 for hess.  A target belongs to the leaf reached
+   from the root by child 1 + (x >= cx) + 2 (y >= cy).  Grows its device
+   scratch (coefficients and target leaves) on the first call that needs more. */
+int bfgt_plan_eval_targets(bfgt_plan plan, int ncomp, const double *d_vals, int ntarg, const double *d_targs,
+                           double *d_out, void *stream);
 
 /* No counterpart in the reference (boxfgt has no adjoint; this is the
    differentiation entry point).  Applies the transpose of this plan's discrete

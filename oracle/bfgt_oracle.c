@@ -16,6 +16,11 @@
  *                        gnd_shiftpw 1798-1844, gnd_find_pwshift_ind 1848-1892,
  *                        gnd_shiftpw_loc 1905-1941, gnd_find_msshift_ind 1946-1976,
  *                        gnd_copy_pwexp 1987-2015, gnd_pwzero 2021-2046
+ *   bfgt/boxfgt.f step 11 (extra targets, iffast = 0) 1494-1563 with
+ *   common/tree_data_routs_nd.f treedata_trans_nd 16-60, treedata_evalt_nd 710-780,
+ *   common/pts_tree_nd.f pts_tree_sort 1226-1260, sort_pts_to_children 650-708,
+ *                        find_childbox_ind 713-740,
+ *   common/tensor_prod_routs_nd.f ortho_trans_2d 103-170, ortho_evalt_2d 2030-2066
  *   bfgt/bfgt_local.f    g2d_tens_prod_to_potloc 315-375, g2d_tens_prod_to_pgloc 379-447,
  *                        g2d_tens_prod_to_pghloc 451-552, gnd_find_loctab_ind 1729-1765
  *   bfgt/bfgt_volrouts.f mk_leg2pw_tables 58-143, mk_cheb2pw_tables 151-275,
@@ -1758,6 +1763,136 @@ int oracle_max_threads(void) {
 #else
   return 1;
 #endif
+}
+
+/* ------------------------------------------------------------------------- */
+/* Extra targets: boxfgt.f step 11 (1494-1563) with iffast = 0               */
+/* ------------------------------------------------------------------------- */
+
+/* find_childbox_ind (common/pts_tree_nd.f:713-740): 1 + (dx >= 0) + 2 (dy >= 0) */
+static int find_childbox_ind(const double *src, const double *cen) {
+  int k = 1, inc = 1;
+  for (int i = 0; i < 2; i++) {
+    double dx = src[i] - cen[i];
+    if (dx >= 0) k = k + inc;
+    inc = inc * 2;
+  }
+  return k;
+}
+
+/* pts_tree_sort (common/pts_tree_nd.f:1226-1260) with sort_pts_to_children
+   (650-708): ixy(n) is the sorted order of the points, ixyse(2,nboxes) the
+   range of each box (1-based) */
+static void pts_tree_sort(int n, const double *xys, const int *itree, const int *iptr, int nboxes, int nlevels,
+                          const double *centers, int *ixy, int *ixyse) {
+  for (int i = 1; i <= n; i++) ixy[i - 1] = i;
+  ixyse[0] = 1;
+  ixyse[1] = n;
+  int *isrcbox = malloc(sizeof(int) * (n > 0 ? n : 1)), *isrctmp = malloc(sizeof(int) * (n > 0 ? n : 1));
+  for (int ilev = 0; ilev <= nlevels - 1; ilev++)
+    for (int ibox = LADDR(itree, 1, ilev); ibox <= LADDR(itree, 2, ilev); ibox++) {
+      if (IT(itree, iptr, 4, ibox) <= 0) continue;
+      if (n == 0) {
+        for (int i = 1; i <= 4; i++) {
+          int jbox = ICHILD(itree, iptr, i, ibox);
+          ixyse[2 * (jbox - 1)] = 1;
+          ixyse[2 * (jbox - 1) + 1] = 0;
+        }
+        continue;
+      }
+      int istart = ixyse[2 * (ibox - 1)], iend = ixyse[2 * (ibox - 1) + 1];
+      int nsrc[4] = {0, 0, 0, 0}, ip[5];
+      for (int iss = istart; iss <= iend; iss++) {
+        int k = find_childbox_ind(&xys[2 * (size_t)(ixy[iss - 1] - 1)], &CEN(centers, 1, ibox));
+        isrcbox[iss - istart] = k;
+        nsrc[k - 1]++;
+      }
+      ip[0] = 0;
+      for (int i = 0; i < 4; i++) ip[i + 1] = ip[i] + nsrc[i];
+      for (int i = 1; i <= 4; i++) {
+        int jbox = ICHILD(itree, iptr, i, ibox);
+        ixyse[2 * (jbox - 1)] = istart + ip[i - 1];
+        ixyse[2 * (jbox - 1) + 1] = istart + ip[i] - 1;
+      }
+      for (int iss = istart; iss <= iend; iss++) {
+        int ic = isrcbox[iss - istart];
+        ip[ic - 1]++;
+        isrctmp[ip[ic - 1] - 1] = ixy[iss - 1];
+      }
+      for (int iss = istart; iss <= iend; iss++) ixy[iss - 1] = isrctmp[iss - istart];
+    }
+  free(isrcbox);
+  free(isrctmp);
+}
+
+/* treedata_trans_nd with itype = 0 (common/tree_data_routs_nd.f:16-60) and
+   treedata_evalt_nd (710-780): out(nd, nt) = the leaf interpolant of
+   vals(nd, n*n, nboxes) at the targets (2, nt), overwritten.  leaf (optional,
+   nt entries) receives the 1-based leaf box of every target. */
+void oracle_eval_targets(int nd, int ipoly, int norder, int nboxes, int nlevels, const int *itree, const int *iptr,
+                         const double *centers, const double *boxsize, const double *vals, int nt,
+                         const double *targs, double *out, int *leaf) {
+  const int n = norder, npb = n * n;
+  double *xq = malloc(sizeof(double) * n), *umat = malloc(sizeof(double) * n * n);
+  double *vmat = malloc(sizeof(double) * n * n), *wts = malloc(sizeof(double) * n);
+  if (ipoly == 0) legeexps(2, n, xq, umat, vmat, wts);
+  else chebexps(2, n, xq, umat, vmat, wts);
+  int *ixy = malloc(sizeof(int) * (nt > 0 ? nt : 1)), *ixyse = malloc(sizeof(int) * 2 * (size_t)nboxes);
+  for (int i = 0; i < 2 * nboxes; i++) ixyse[i] = 0;
+  pts_tree_sort(nt, targs, itree, iptr, nboxes, nlevels, centers, ixy, ixyse);
+  double *coefs = malloc(sizeof(double) * (size_t)nd * npb), *work = malloc(sizeof(double) * (size_t)nd * npb);
+  double *px = malloc(sizeof(double) * n), *py = malloc(sizeof(double) * n), *tmp = malloc(sizeof(double) * nd * n);
+  for (int ilev = 0; ilev <= nlevels; ilev++) {
+    double sc = 2.0 / boxsize[ilev];
+    for (int ibox = LADDR(itree, 1, ilev); ibox <= LADDR(itree, 2, ilev); ibox++) {
+      if (IT(itree, iptr, 4, ibox) != 0) continue;
+      int istart = ixyse[2 * (ibox - 1)], iend = ixyse[2 * (ibox - 1) + 1];
+      if (iend - istart + 1 <= 0) continue;
+      /* ortho_trans_2d, itype = 0 */
+      const double *fin = vals + (size_t)nd * npb * (ibox - 1);
+      for (int j = 1; j <= n; j++)
+        for (int k = 1; k <= n; k++)
+          for (int ind = 1; ind <= nd; ind++) {
+            double dd = 0;
+            for (int k1 = 1; k1 <= n; k1++) dd = dd + M2(umat, n, k, k1) * fin[(ind - 1) + (size_t)nd * ((k1 - 1) + (size_t)n * (j - 1))];
+            work[(ind - 1) + (size_t)nd * ((k - 1) + (size_t)n * (j - 1))] = dd;
+          }
+      for (int i = 1; i <= n; i++)
+        for (int k = 1; k <= n; k++)
+          for (int ind = 1; ind <= nd; ind++) {
+            double dd = 0;
+            for (int i1 = 1; i1 <= n; i1++) dd = dd + M2(umat, n, i, i1) * work[(ind - 1) + (size_t)nd * ((k - 1) + (size_t)n * (i1 - 1))];
+            coefs[(ind - 1) + (size_t)nd * ((k - 1) + (size_t)n * (i - 1))] = dd;
+          }
+      for (int it = istart; it <= iend; it++) {
+        int t = ixy[it - 1];
+        double x = (targs[2 * (size_t)(t - 1)] - CEN(centers, 1, ibox)) * sc;
+        double y = (targs[2 * (size_t)(t - 1) + 1] - CEN(centers, 2, ibox)) * sc;
+        if (ipoly == 0) {
+          legepols(x, n - 1, px);
+          legepols(y, n - 1, py);
+        } else {
+          chebpols(x, n - 1, px);
+          chebpols(y, n - 1, py);
+        }
+        /* ortho_evalt_2d (common/tensor_prod_routs_nd.f:2030-2066) */
+        for (int j = 1; j <= n; j++)
+          for (int ind = 1; ind <= nd; ind++) {
+            double pp = 0;
+            for (int k = 1; k <= n; k++) pp = pp + coefs[(ind - 1) + (size_t)nd * ((k - 1) + (size_t)n * (j - 1))] * px[k - 1];
+            tmp[(ind - 1) + (size_t)nd * (j - 1)] = pp;
+          }
+        for (int ind = 1; ind <= nd; ind++) {
+          double pp = 0;
+          for (int j = 1; j <= n; j++) pp = pp + tmp[(ind - 1) + (size_t)nd * (j - 1)] * py[j - 1];
+          out[(ind - 1) + (size_t)nd * (t - 1)] = pp;
+        }
+        if (leaf) leaf[t - 1] = ibox;
+      }
+    }
+  }
+  free(xq); free(umat); free(vmat); free(wts); free(ixy); free(ixyse);
+  free(coefs); free(work); free(px); free(py); free(tmp);
 }
 
 /* Node families used by the leaf grid (for test harnesses). */

@@ -43,6 +43,9 @@ def lib():
         L.oracle_boxfgt_pgh.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                         C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int, _f64p, C.c_void_p,
                                         C.c_void_p]
+        L.oracle_eval_targets.restype = None
+        L.oracle_eval_targets.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p,
+                                          _f64p, C.c_int, _f64p, _f64p, C.c_void_p]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_max_threads.restype = C.c_int
         L.oracle_nodes.argtypes = [C.c_int, C.c_int, _f64p, _f64p, _f64p, _f64p]
@@ -144,6 +147,27 @@ def boxfgt_pgh(tree, fvals, delta, eps, ifpgh, nd=1, threads=0):
                         np.ascontiguousarray(tree.boxsize, dtype=np.float64), fv, int(ifpgh), pot,
                         None if grad is None else grad.ctypes.data, None if hess is None else hess.ctypes.data)
     return pot, grad, hess
+
+
+def eval_targets(tree, vals, targs, nd=1, itree=None):
+    """Leaf interpolant of vals(nd, npbox, nboxes) at targets (ntarg, 2), as the
+    reference's step 11 does (treedata_trans_nd + treedata_evalt_nd with
+    pts_tree_sort).  Returns (out (ntarg, nd), 1-based leaf box per target).
+    itree: the tree array after boxfgt rewrote its colleagues (the sort only
+    reads levels, children and centers, so tree.itree works as well)."""
+    L = lib()
+    t = np.ascontiguousarray(targs, dtype=np.float64).reshape(-1, 2)
+    nt = t.shape[0]
+    out = np.zeros(nd * max(nt, 1))
+    leaf = np.zeros(max(nt, 1), np.int32)
+    it = np.ascontiguousarray(tree.itree if itree is None else itree, dtype=np.int32)
+    L.oracle_eval_targets(int(nd), int(tree.ipoly), int(tree.norder), int(tree.nboxes), int(tree.nlevels), it,
+                          np.ascontiguousarray(tree.iptr, dtype=np.int32),
+                          np.ascontiguousarray(tree.centers, dtype=np.float64).reshape(-1),
+                          np.ascontiguousarray(tree.boxsize, dtype=np.float64),
+                          np.ascontiguousarray(vals, dtype=np.float64).reshape(-1), int(nt), t.reshape(-1), out,
+                          leaf.ctypes.data)
+    return out[: nd * nt].reshape(nt, nd), leaf[:nt]
 
 
 def nodes(ipoly, n):

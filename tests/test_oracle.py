@@ -127,3 +127,25 @@ def test_oracle_gradient_multiple_densities(trees):
     _, g, _ = oracle.boxfgt_pgh(t, fv, 1e-3, 1e-9, 2, nd=nd)
     _, qg, _ = quad.direct_pgh(t, fv, 1e-3, nd=nd, ifpgh=2)
     assert rel_l2(leaf_vals(t, g), leaf_vals(t, qg)) < 1e-7
+
+
+def test_oracle_targets_interpolate_and_sort(trees):
+    """Step 11 restated (treedata_evalt_nd with pts_tree_sort): every target
+    lands in the leaf that contains it, with points on an edge going to the
+    upper child (find_childbox_ind's dx >= 0), and interpolating the density's
+    own leaf values reproduces it to the tree's resolution."""
+    from fgt_autograd import gauss_at_points
+    t = trees["ad_leg_per"]
+    rng = np.random.default_rng(0)
+    h = t.boxsize[t.nlevels]
+    edge = (np.arange(-4, 5) * h)
+    tg = np.concatenate([rng.uniform(-0.5, 0.5, (3000, 2)), np.stack(np.meshgrid(edge, edge), -1).reshape(-1, 2)])
+    out, leaf = oracle.eval_targets(t, t.fvals, tg)
+    lev = t.ilevel()[leaf - 1]
+    c = t.centers[leaf - 1]
+    half = t.boxsize[lev][:, None] / 2
+    assert np.all(t.nchild()[leaf - 1] == 0)
+    assert np.all((tg >= c - half) & (tg < c + half))
+    from conftest import gauss_sum
+    g6 = gauss_sum(2, 6, 0.01, 0.05, amp="normal", log_width=True)
+    assert np.abs(out[:, 0] - gauss_at_points(tg, g6)).max() < 1e-5

@@ -98,10 +98,13 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, NP = a.NP, KA = a.KA;
   const int ncol = ch.y - ch.x;
   const int abytes = 3 * kRows * KA * 2, bbytes = 3 * NP * KA * 2, bufbytes = abytes + bbytes;
-  const int ybytes = kRows * hh * 16;
+  // Y rows padded to an odd number of double2 so that the readout's per-row
+  // stores fall in distinct banks
+  const int ys = hh | 1;
+  const int ybytes = kRows * ys * 16;
   const int ubytes = ((std::max(2 * bufbytes, ybytes) + 127) / 128) * 128;
   unsigned char *U = smem + 128;
-  double2 *sY = reinterpret_cast<double2 *>(U);  // after the tensor-core loop: [row][k2]
+  double2 *sY = reinterpret_cast<double2 *>(U);  // after the tensor-core loop: [row][k2], row stride ys
   double2 *sT = reinterpret_cast<double2 *>(U + ubytes);  // [m][k] n x npw
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, 128);
@@ -226,9 +229,11 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
 #pragma unroll
         for (int i = 0; i < 16; i++) {
           const int j = j0 + i;
-          const double y = ok ? (double)v0[i] + (double)v1[i] : 0.0;
-          if (j < hh) sY[r * hh + j].x = y;
-          else if (j < 2 * hh) sY[r * hh + (j - hh)].y = y;
+          // D0 + D1 in FP32 (one more rounding of 2^-24, below the accumulated
+          // error), then one conversion
+          const double y = ok ? (double)(v0[i] + v1[i]) : 0.0;
+          if (j < hh) sY[r * ys + j].x = y;
+          else if (j < 2 * hh) sY[r * ys + (j - hh)].y = y;
         }
       }
     }
@@ -261,7 +266,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
 #pragma unroll
             for (int i = 0; i < 2; i++) av[i] = zmul((k1b + i < npw) ? sT[m1 * npw + k1b + i] : make_double2(0, 0), ph[i]);
 #pragma unroll
-            for (int j = 0; j < 4; j++) bv[j] = (k2b + j < hh) ? sY[(slot * n + m1) * hh + k2b + j] : make_double2(0, 0);
+            for (int j = 0; j < 4; j++) bv[j] = (k2b + j < hh) ? sY[(slot * n + m1) * ys + k2b + j] : make_double2(0, 0);
 #pragma unroll
             for (int i = 0; i < 2; i++)
 #pragma unroll
@@ -536,7 +541,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
           if (ok && pbc) {
 #pragma unroll
             for (int k2 = 0; k2 < 16; k2++)
-              if (k2 < n) pbc[(size_t)nd * n * k2] = pc[k2] + 2.0 * ((double)v0[k2] + (double)v1[k2]);
+              if (k2 < n) pbc[(size_t)nd * n * k2] = pc[k2] + 2.0 * (double)(v0[k2] + v1[k2]);
           }
         }
       }
@@ -736,7 +741,7 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   // shared memory
   {
     const int abytes = 3 * kRows * sp.KA * 2, bbytes = 3 * sp.NP * sp.KA * 2;
-    const int ybytes = kRows * hh * 16;
+    const int ybytes = kRows * (hh | 1) * 16;
     const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 127) / 128) * 128;
     sp.smem_form = 128 + ubytes + sizeof(double2) * (size_t)n * npw;
     const int eab = 3 * kRows * sp.KE * 2, ebb = 3 * (16 * kEvalBatch) * sp.KE * 2;

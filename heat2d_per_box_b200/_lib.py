@@ -92,6 +92,8 @@ def lib():
     L.bfgt_noalloc_scratch_bytes.argtypes = [C.POINTER(C.c_size_t)]
     L.bfgt_plan_noalloc_need.restype = C.c_int
     L.bfgt_plan_noalloc_need.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
+    L.bfgt_plan_autotune.restype = C.c_int
+    L.bfgt_plan_autotune.argtypes = [C.c_void_p, C.c_void_p, _f64p]
     L.bfgt_plan_check.restype = C.c_int
     L.bfgt_plan_check.argtypes = [C.c_void_p]
     L.bfgt_plan_set_wait_limit.restype = C.c_int

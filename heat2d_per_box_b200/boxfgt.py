@@ -158,6 +158,14 @@ class Plan:
         """Poll limit of the bounded device waits (None restores the default)."""
         _lib.check(self._L.bfgt_plan_set_wait_limit(self._h, 0xFFFFFFFF if polls is None else int(polls)))
 
+    def autotune(self, stream=None):
+        """Times the FP64 kernels' tile shapes on this plan and keeps the fastest
+        (see bfgt_plan_autotune); returns (form ms, eval ms, shapes timed)."""
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        rep = np.zeros(4)
+        _lib.check(self._L.bfgt_plan_autotune(self._h, s, rep))
+        return float(rep[0]), float(rep[1]), int(rep[2] + rep[3])
+
     def check(self):
         """Waits for the device; raises BfgtError if a bounded device wait timed out."""
         _lib.check(self._L.bfgt_plan_check(self._h))
@@ -175,7 +183,7 @@ class Plan:
         out = np.zeros(16, np.int32)
         _lib.check(self._L.bfgt_plan_info(self._h, out))
         keys = ["npwlevel", "npw", "nlevstart", "nlevend", "regime", "nleafbox", "npwleaves", "nnear_targets",
-                "nnear_pairs", "mnlist1", "iperiod_int", "nchunks", "launches"]
+                "nnear_pairs", "mnlist1", "iperiod_int", "nchunks", "launches", "form_tile", "eval_tile"]
         return {k: int(out[i]) for i, k in enumerate(keys)}
 
     def work(self):
@@ -239,6 +247,14 @@ class Batch:
         _lib.check(self._L.bfgt_batch_info(self._h, out))
         keys = ["plans", "launches", "form_items", "eval_items", "translate_blocks", "near_blocks"]
         return {k: int(out[i]) for i, k in enumerate(keys)}
+
+    def autotune(self, stream=None):
+        """Times the FP64 kernels' tile shapes on this plan and keeps the fastest
+        (see bfgt_plan_autotune); returns (form ms, eval ms, shapes timed)."""
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        rep = np.zeros(4)
+        _lib.check(self._L.bfgt_plan_autotune(self._h, s, rep))
+        return float(rep[0]), float(rep[1]), int(rep[2] + rep[3])
 
     def check(self):
         _lib.check(self._L.bfgt_batch_check(self._h))

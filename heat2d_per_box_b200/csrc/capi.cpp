@@ -410,6 +410,10 @@ int bfgt_plan_info(bfgt_plan plan, int *out) {
   out[9] = h.mnlist1;
   out[10] = h.iperiod_int;
   out[11] = plan->dp.nchunks;
+  // FP64 tile shapes in use (100 tm + 10 tn + tiles per lane), 0 for split plans
+  const bool f64 = plan->dp.precision == BFGT_PREC_FP64;
+  out[13] = f64 ? 100 * plan->dp.form_tile[0] + 10 * plan->dp.form_tile[1] + plan->dp.form_tile[2] : 0;
+  out[14] = f64 ? 100 * plan->dp.eval_tile[0] + 10 * plan->dp.eval_tile[1] + plan->dp.eval_tile[2] : 0;
   out[12] = (!plan->dp.direct_only && plan->dp.nchunks > 0 ? 3 : 0) + (plan->dp.nnf > 0 ? 1 : 0);
   return BFGT_OK;
 }
@@ -435,6 +439,16 @@ int bfgt_plan_work(bfgt_plan plan, double *out) {
   for (const auto &r : plan->leaf_runs) run_bytes += 8.0 * plan->dp.nd * plan->dp.n * plan->dp.n * (r.second - r.first);
   out[13] = 2 * run_bytes;  // bfgt_plan_execute_host: fvals and pot up
   out[14] = run_bytes;      // and pot down
+  return BFGT_OK;
+}
+
+int bfgt_plan_autotune(bfgt_plan plan, void *stream, double *report) {
+  g_err.clear();
+  if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  double rep[4];
+  std::string msg;
+  int rc = bfgt::device_plan_autotune(plan->dp, (cudaStream_t)stream, report ? report : rep, msg);
+  if (rc != BFGT_OK) return fail(rc, msg);
   return BFGT_OK;
 }
 

@@ -94,6 +94,12 @@ int build_reduce_groups(DevicePlan &dp, const std::vector<int> &cut_of_chunk, st
 // Allocates and uploads; returns a BFGT_* status and fills msg on failure.
 int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);
 void device_plan_destroy(DevicePlan &dp);
+// Times every compiled FP64 tile shape of the form and eval kernels on this
+// plan's work (scratch inputs; the caller's arrays are not touched), keeps the
+// fastest and remembers it for later plans of the same (norder, npw, nd).
+// report: best form ms, best eval ms, form and eval candidates timed.  No
+// effect on split-precision plans (their shapes are fixed).
+int device_plan_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::string &msg);
 // Uploads the derivative tables used by device_plan_execute_pgh.
 int device_plan_prepare_pgh(DevicePlan &dp, const HostPlan &hp, std::string &msg);
 // pot += K f and, for ifpgh >= 2, grad(nd,2,npbox,nboxes) += grad K f, for

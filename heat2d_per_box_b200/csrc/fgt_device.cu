@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -603,6 +605,97 @@ ReduceArgs reduce_args(const DevicePlan &dp) {
   return ReduceArgs{dp.Mpart, dp.G, dp.M, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups};
 }
 
+// ---- autotuner of the FP64 tile shapes ---------------------------------------
+
+namespace {
+
+std::mutex g_tune_mu;
+std::map<std::array<int, 3>, std::pair<TileChoice, TileChoice>> g_tuned;  // (n, npw, nd) -> (form, eval)
+
+// every compiled tile shape whose lanes cover an a x b output
+std::vector<TileChoice> valid_tiles(int a, int b, const TileChoice *cands, int nc) {
+  std::vector<TileChoice> v;
+  for (int i = 0; i < nc; i++) {
+    const int tiles = ((a + cands[i].tm - 1) / cands[i].tm) * ((b + cands[i].tn - 1) / cands[i].tn);
+    if (32 * cands[i].nt >= tiles) v.push_back(cands[i]);
+  }
+  return v;
+}
+
+}  // namespace
+
+void tuned_tiles(int n, int npw, int nd, TileChoice &form, TileChoice &eval) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tuned.find({n, npw, nd});
+  if (it == g_tuned.end()) return;
+  form = it->second.first;
+  eval = it->second.second;
+}
+
+int device_plan_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::string &msg) {
+  for (int i = 0; i < 4; i++) report[i] = 0;
+  if (dp.precision == BFGT_PREC_SPLIT || dp.direct_only || dp.nchunks == 0) return BFGT_OK;  // no tile choice to make
+  const size_t elems = (size_t)dp.nd * dp.n * dp.n * dp.nboxes;
+  double *f = nullptr, *p = nullptr;
+  if (alloc_bytes((void **)&f, sizeof(double) * elems, msg) != BFGT_OK) return BFGT_ERR_OOM;
+  if (alloc_bytes((void **)&p, sizeof(double) * elems, msg) != BFGT_OK) {
+    cudaFree(f);
+    return BFGT_ERR_OOM;
+  }
+  cudaMemsetAsync(f, 0, sizeof(double) * elems, s);
+  cudaMemsetAsync(p, 0, sizeof(double) * elems, s);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const TileChoice f0{dp.form_tile[0], dp.form_tile[1], dp.form_tile[2]};
+  const TileChoice v0{dp.eval_tile[0], dp.eval_tile[1], dp.eval_tile[2]};
+  auto time_ms = [&](auto &&launch) {
+    launch();  // warm-up
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; r++) launch();
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms / 3.0;
+  };
+  TileChoice bf = f0, be = v0;
+  double tf = 1e30, te = 1e30;
+  const std::vector<TileChoice> fc = valid_tiles(dp.npw, dp.hh, kFormTiles, kNFormTiles);
+  const std::vector<TileChoice> ec = valid_tiles(dp.n, dp.hh, kEvalTiles, kNEvalTiles);
+  for (const TileChoice &t : fc) {
+    FormArgs fa{f, dp.leaves, dp.columns, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, reduce_args(dp), dp.nd, dp.n,
+                dp.npw, dp.hh, dp.nexp};
+    const double ms = time_ms([&] { launch_form_fp64(t, dp.nchunks, dp.smem_form, s, fa); });
+    if (ms < tf) tf = ms, bf = t;
+  }
+  for (const TileChoice &t : ec) {
+    EvalArgs ea{p, dp.leaves, dp.columns, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n,
+                dp.npw, dp.hh, dp.nexp};
+    const double ms = time_ms([&] { launch_eval_fp64(t, dp.nchunks, dp.smem_eval, s, ea); });
+    if (ms < te) te = ms, be = t;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(f);
+  cudaFree(p);
+  if (cudaGetLastError() != cudaSuccess) {
+    msg = "CUDA error while autotuning";
+    return BFGT_ERR_CUDA;
+  }
+  dp.form_tile[0] = bf.tm, dp.form_tile[1] = bf.tn, dp.form_tile[2] = bf.nt;
+  dp.eval_tile[0] = be.tm, dp.eval_tile[1] = be.tn, dp.eval_tile[2] = be.nt;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[{dp.n, dp.npw, dp.nd}] = {bf, be};
+  }
+  report[0] = tf;
+  report[1] = te;
+  report[2] = (double)fc.size();
+  report[3] = (double)ec.size();
+  return BFGT_OK;
+}
+
 int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -669,8 +762,9 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
                                       (size_t)kWarps * ((size_t)n * dp.hh + dp.npw + dp.hh + (npb + 1) / 2));
     dp.smem_eval = sizeof(double2) * ((size_t)n * dp.npw + (size_t)dp.npw * dp.hh +
                                       (size_t)kWarps * ((size_t)n * dp.hh + dp.npw + dp.hh));
-    const TileChoice ft = best_tile(dp.npw, dp.hh, kFormTiles, kNFormTiles);
-    const TileChoice et = best_tile(n, dp.hh, kEvalTiles, kNEvalTiles);
+    TileChoice ft = best_tile(dp.npw, dp.hh, kFormTiles, kNFormTiles);
+    TileChoice et = best_tile(n, dp.hh, kEvalTiles, kNEvalTiles);
+    tuned_tiles(n, dp.npw, dp.nd, ft, et);  // an earlier autotune of this shape wins
     dp.form_tile[0] = ft.tm, dp.form_tile[1] = ft.tn, dp.form_tile[2] = ft.nt;
     dp.eval_tile[0] = et.tm, dp.eval_tile[1] = et.tn, dp.eval_tile[2] = et.nt;
     if (rc == BFGT_OK && (ft.nt == 0 || et.nt == 0)) {

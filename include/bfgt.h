@@ -172,7 +172,9 @@ int bfgt_plan_reserve_events(bfgt_plan plan, int n);
    out[7]=number of near-field target leaves, out[8]=number of near-field
    interactions, out[9]=mnlist1, out[10]=internal iperiod, out[11]=number of
    plane-wave chunks (CTAs of the form and eval kernels), out[12]=kernel
-   launches per execute.  out must hold 16 ints. */
+   launches per execute, out[13]/out[14]=FP64 form/eval tile shape in use
+   (100 tm + 10 tn + tiles per lane; 0 for split plans).  out must hold 16
+   ints. */
 int bfgt_plan_info(bfgt_plan plan, int *out);
 
 /* Algorithmic work of one execute (every real operation counted once, split
@@ -184,6 +186,15 @@ int bfgt_plan_info(bfgt_plan plan, int *out);
    form and eval stages, out[13..14]=bytes bfgt_plan_execute_host moves host to
    device and device to host (leaf boxes only).  out must hold 16. */
 int bfgt_plan_work(bfgt_plan plan, double *out);
+
+/* No counterpart in the reference.  Autotuner of the FP64 kernels' tile
+   shapes: times every compiled shape of the form and eval kernels on this
+   plan's work (on scratch arrays it allocates; synchronous), keeps the fastest
+   for this plan and remembers it for plans of the same (norder, npw, nd)
+   created later in the process.  report (may be NULL) receives the best form
+   and eval ms per launch and the numbers of shapes timed.  Split-precision
+   plans have fixed shapes: nothing is timed. */
+int bfgt_plan_autotune(bfgt_plan plan, void *stream, double *report);
 
 /* Waits for the device and reports failures of earlier executes on this plan:
    BFGT_ERR_TIMEOUT if a bounded device-side wait of the tensor-core pipeline

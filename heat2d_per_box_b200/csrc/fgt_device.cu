@@ -29,6 +29,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/bfgt.h"
 #include "batch.hpp"
 #include "device_plan.hpp"
@@ -899,7 +901,15 @@ cudaEvent_t *next_events(std::vector<std::array<cudaEvent_t, 6>> &evsets, int &n
 
 }  // namespace
 
+// NVTX range around the host-side queuing of one transform (visible to
+// profilers that record NVTX; no cost without one)
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+
 int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cudaStream_t s, std::string &msg) {
+  NvtxRange range(dp.precision == BFGT_PREC_SPLIT ? "bfgt execute (split)" : "bfgt execute (fp64)");
   cudaEvent_t *ev = next_events(dp.evsets, dp.nrec, dp.events);
   if (ev) cudaEventRecord(ev[0], s);
   if (has_pw(dp)) {
@@ -972,6 +982,7 @@ int device_plan_prepare_pgh(DevicePlan &dp, const HostPlan &hp, std::string &msg
 
 int device_plan_execute_pgh(DevicePlan &dp, int ifpgh, const double *d_fvals, double *d_pot, double *d_grad,
                             double *d_hess, cudaStream_t s, std::string &msg) {
+  NvtxRange range("bfgt execute pgh");
   int rc = device_plan_execute(dp, d_fvals, d_pot, s, msg);
   if (rc != BFGT_OK || ifpgh < 2) return rc;
   if (!dp.pgh_ready) {
@@ -1249,6 +1260,7 @@ int device_batch_launches(const DeviceBatch &b) {
 }
 
 int device_batch_execute(DeviceBatch &b, const double *d_fvals, double *d_pot, cudaStream_t s, std::string &msg) {
+  NvtxRange range("bfgt batch execute");
   cudaEvent_t *ev = next_events(b.evsets, b.nrec, b.events);
   if (ev) cudaEventRecord(ev[0], s);
   split_batch_form(b.split, d_fvals, s);

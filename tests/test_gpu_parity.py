@@ -146,3 +146,29 @@ def test_golden_vectors_gpu():
         ref = np.array(case["sample_pot"])
         err = rel_l2(got[idx[:, 0], idx[:, 1]], ref)
         assert err < 10 * case["eps"], (case["name"], err)
+
+
+@pytest.mark.parametrize("precision", [hb.BFGT_PREC_FP64, hb.BFGT_PREC_SPLIT])
+@pytest.mark.parametrize("delta,level,regime", [(4e-5, 5, 2), (4e-5, 6, 1), (1e-3, 4, 1), (1e-2, 4, 0)])
+def test_fourier_mode_kat_gpu(precision, delta, level, regime):
+    """The reference's own known-answer test (hpots/test_initpot.f:58-80, 239-250,
+    367-373) through the CUDA path: for f = sin(2 pi 2x) cos(2 pi 2y) on a
+    periodic Chebyshev order-8 tree, pot / (pi delta) = exp(-8 pi^2 delta) f, in
+    every regime.  The n = 8 leaf interpolant bounds the error (1e-7); the split
+    path adds its 1e-6."""
+    import torch
+    from test_oracle import kat_tree
+    eps = 1e-9
+    t = kat_tree(level, ipoly=1)
+    plan = hb.Plan(t, delta, eps, precision=precision)
+    assert plan.info()["regime"] == regime
+    f = torch.from_numpy(np.ascontiguousarray(t.fvals).reshape(-1)).cuda()
+    p = torch.zeros_like(f)
+    plan.execute(f, p)
+    plan.check()
+    plan.close()
+    lv = t.leaves()
+    exact = np.exp(-np.pi ** 2 * 8 * delta) * t.fvals[lv]
+    got = p.cpu().numpy().reshape(t.nboxes, -1)[lv] / (np.pi * delta)
+    err = np.abs(got - exact).max() / np.abs(exact).max()
+    assert err < (1e-7 if precision == hb.BFGT_PREC_FP64 else 2e-6), err

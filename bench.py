@@ -270,6 +270,61 @@ def run_uneven(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_uniform5(args):
+    """Plain FP64 periodic boxfgt on a uniform level-5 quadtree (1024 leaves),
+    Legendre order 8 (65,536 points), nd=1, delta=1e-3, eps=1e-9; density = 3
+    Gaussians (seed 1, centres uniform in the box, widths uniform in
+    [0.05, 0.1], amplitudes uniform in [-1, 1]).  FP64 and split plans, CUDA
+    events over back-to-back executes, and the oracle on the host cores."""
+    import torch
+    import heat2d_per_box_b200 as hb
+    from oracle import oracle
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(1)
+    g = hb.gauss_params(rng.uniform(-0.5, 0.5, (3, 2)), rng.uniform(0.05, 0.1, 3), rng.uniform(-1, 1, 3))
+    t = hb.build_uniform(5, g, norder=8, ipoly=0, iperiod=1)
+    delta, eps = 1e-3, 1e-9
+    npts = len(t.leaves()) * t.npbox
+    f = torch.from_numpy(t.fvals.reshape(-1)).cuda()
+    stream = torch.cuda.current_stream()
+    res = {}
+    for prec in (hb.BFGT_PREC_FP64, hb.BFGT_PREC_SPLIT):
+        plan = hb.Plan(t, delta, eps, precision=prec)
+        plan.autotune(stream)
+        p = torch.zeros_like(f)
+        for _ in range(args.warmup):
+            plan.execute(f, p, stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.execute(f, p, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[prec] = (e0.elapsed_time(e1) / args.steps, plan.info())
+        plan.close()
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    oracle.boxfgt(t, t.fvals, delta, eps)
+    reps, t0 = 0, time.perf_counter()
+    while reps < 50 and time.perf_counter() - t0 < 5.0:
+        oracle.boxfgt(t, t.fvals, delta, eps)
+        reps += 1
+    cpu_ms = (time.perf_counter() - t0) / reps * 1e3
+    ms64, info = res[hb.BFGT_PREC_FP64]
+    line = {"metric": METRIC, "value": npts / (ms64 * 1e-3), "unit": "leaf points/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms64, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "uniform level-5 periodic tree, Legendre order 8, 3 Gaussians (seed 1), nd=1, "
+                                   "delta=1e-3, eps=1e-9", "leaves": int(len(t.leaves())), "points": int(npts),
+                       "npw": info["npw"], "npwlevel": info["npwlevel"], "regime": info["regime"]},
+            "split_value": npts / (res[hb.BFGT_PREC_SPLIT][0] * 1e-3),
+            "split_ms_per_step": res[hb.BFGT_PREC_SPLIT][0],
+            "cpu_baseline": {"value": npts / (cpu_ms * 1e-3), "unit": "leaf points/s", "cores": threads,
+                             "kind": "port", "sample": f"{reps} full transforms (oracle, OpenMP {threads} threads)"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -281,9 +336,10 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "split"])
     ap.add_argument("--small", action="store_true", help="level-6 base tree (for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="adaptive16", choices=["adaptive16", "uneven64"],
+    ap.add_argument("--workload", default="adaptive16", choices=["adaptive16", "uneven64", "uniform5"],
                     help="adaptive16: one adaptive order-16 tree (default); uneven64: 64 uneven order-8 trees, "
-                         "nd=8, batched in one graph")
+                         "nd=8, batched in one graph; uniform5: the plain FP64 case on a uniform level-5 order-8 "
+                         "tree")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -296,6 +352,9 @@ def main():
         return
     if args.workload == "uneven64":
         run_uneven(args, rank, world)
+        return
+    if args.workload == "uniform5":
+        run_uniform5(args)
         return
 
     import torch

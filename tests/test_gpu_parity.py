@@ -172,3 +172,37 @@ def test_fourier_mode_kat_gpu(precision, delta, level, regime):
     got = p.cpu().numpy().reshape(t.nboxes, -1)[lv] / (np.pi * delta)
     err = np.abs(got - exact).max() / np.abs(exact).max()
     assert err < (1e-7 if precision == hb.BFGT_PREC_FP64 else 2e-6), err
+
+
+@pytest.mark.parametrize("lev,delta,eps", [(0, 1e-1, 1e-6), (1, 1e-3, 1e-9), (1, 1e-5, 1e-9), (1, 1e-1, 1e-6)])
+def test_degenerate_trees_match_oracle(lev, delta, eps):
+    """A root-only tree (one leaf) and a one-level tree, in the periodic
+    Fourier regime and near field only, FP64 and split."""
+    import torch
+    g = hb.gauss_params(np.array([[0.1, 0.2]]), np.array([0.2]), np.array([1.0]))
+    t = hb.build_uniform(lev, g, norder=8, ipoly=0, iperiod=1)
+    ref = oracle.boxfgt(t, t.fvals, delta, eps).reshape(t.nboxes, -1)
+    lv = t.leaves()
+    for prec, bar in ((hb.BFGT_PREC_FP64, 1e-11), (hb.BFGT_PREC_SPLIT, 1e-6)):
+        plan = hb.Plan(t, delta, eps, precision=prec)
+        f = torch.from_numpy(t.fvals.reshape(-1)).cuda()
+        p = torch.zeros_like(f)
+        plan.execute(f, p)
+        plan.check()
+        plan.close()
+        assert rel_l2(p.cpu().numpy().reshape(t.nboxes, -1)[lv], ref[lv]) < bar
+
+
+def test_beyond_capacity_fails_cleanly():
+    """npw = 93 (a root-only tree at delta = 1e-3, periodic Fourier regime) is
+    beyond the compiled FP64 tile shapes (npw up to about 88) and the split
+    path (npw <= 64): plan creation reports BFGT_ERR_CAPACITY and the device
+    stays usable."""
+    import torch
+    g = hb.gauss_params(np.array([[0.1, 0.2]]), np.array([0.2]), np.array([1.0]))
+    t = hb.build_uniform(0, g, norder=8, ipoly=0, iperiod=1)
+    for prec in (hb.BFGT_PREC_FP64, hb.BFGT_PREC_SPLIT):
+        with pytest.raises(hb.BfgtError) as e:
+            hb.Plan(t, 1e-3, 1e-9, precision=prec)
+        assert e.value.code == 3  # BFGT_ERR_CAPACITY
+    torch.zeros(4, device="cuda").sum().item()

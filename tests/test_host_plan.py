@@ -59,3 +59,12 @@ def test_invalid_tree_is_rejected():
         hb.host_plan_dump(bad, 1e-3, 1e-9)
     with pytest.raises(hb.BfgtError):
         hb.host_plan_dump(t, -1.0, 1e-9)     # delta <= 0
+
+
+def test_npw_beyond_reference_capacity_is_rejected():
+    """The reference sizes ws(200), ts(200) (boxfgt.f:434) without a check; here a
+    transform that would need more than 200 plane waves is rejected."""
+    g = hb.gauss_params(np.array([[0.1, 0.2]]), np.array([0.2]), np.array([1.0]))
+    t = hb.build_uniform(0, g, norder=8, ipoly=0, iperiod=1)
+    with pytest.raises(hb.BfgtError, match="npw > 200"):
+        hb.host_plan_dump(t, 1e-5, 1e-9)

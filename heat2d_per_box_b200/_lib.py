@@ -103,6 +103,7 @@ def lib():
     for name, args in (("bfgt_batch_create", [C.POINTER(C.c_void_p), C.c_int, C.c_void_p]),
                        ("bfgt_batch_layout", [C.c_void_p, C.c_void_p]),
                        ("bfgt_batch_execute", [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+                       ("bfgt_batch_execute_adjoint", [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
                        ("bfgt_batch_graph_capture", [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
                        ("bfgt_batch_graph_launch", [C.c_void_p, C.c_void_p]),
                        ("bfgt_batch_stage_ms", [C.c_void_p, _f64p]),

@@ -229,6 +229,11 @@ class Batch:
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         _lib.check(self._L.bfgt_batch_execute(self._h, Plan._ptr(d_fvals), Plan._ptr(d_pot), s))
 
+    def execute_adjoint(self, d_potbar, d_fbar, stream=None):
+        """fbar += K_i^T potbar for every plan i (packed arrays, same layout)."""
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._L.bfgt_batch_execute_adjoint(self._h, Plan._ptr(d_potbar), Plan._ptr(d_fbar), s))
+
     def graph_capture(self, d_fvals, d_pot, stream=None):
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         _lib.check(self._L.bfgt_batch_graph_capture(self._h, Plan._ptr(d_fvals), Plan._ptr(d_pot), s))

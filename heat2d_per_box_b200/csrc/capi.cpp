@@ -26,6 +26,7 @@ struct bfgt_tree_s {
 struct bfgt_batch_s {
   std::vector<bfgt_plan> plans;  // not owned; must outlive the batch
   bfgt::DeviceBatch db;
+  std::unique_ptr<bfgt::DeviceBatch> adj;  // the plans' transposed transforms, built on first use
   int device = 0;
 };
 
@@ -730,6 +731,32 @@ int bfgt_batch_execute(bfgt_batch batch, const double *d_fvals, double *d_pot, v
   return BFGT_OK;
 }
 
+int bfgt_batch_execute_adjoint(bfgt_batch batch, const double *d_potbar, double *d_fbar, void *stream) {
+  g_err.clear();
+  if (!batch) return fail(BFGT_ERR_ARG, "batch is NULL");
+  if (!d_potbar || !d_fbar) return fail(BFGT_ERR_ARG, "potbar/fbar device pointers are NULL");
+  if (!batch->adj) {
+    std::vector<bfgt::DevicePlan *> dps;
+    for (bfgt_plan p : batch->plans) {
+      int rc = ensure_adjoint(p);
+      if (rc != BFGT_OK) return rc;
+      dps.push_back(p->adj_dp.get());
+    }
+    std::unique_ptr<bfgt::DeviceBatch> b(new bfgt::DeviceBatch());
+    std::string msg;
+    int rc = bfgt::device_batch_create(*b, dps, msg);
+    if (rc != BFGT_OK) {
+      bfgt::device_batch_destroy(*b);
+      return fail(rc, msg);
+    }
+    batch->adj = std::move(b);
+  }
+  std::string msg;
+  int rc = bfgt::device_batch_execute(*batch->adj, d_potbar, d_fbar, (cudaStream_t)stream, msg);
+  if (rc != BFGT_OK) return fail(rc, msg);
+  return BFGT_OK;
+}
+
 int bfgt_batch_graph_capture(bfgt_batch batch, const double *d_fvals, double *d_pot, void *stream) {
   g_err.clear();
   if (!batch) return fail(BFGT_ERR_ARG, "batch is NULL");
@@ -805,6 +832,7 @@ int bfgt_batch_destroy(bfgt_batch batch) {
   g_err.clear();
   if (!batch) return BFGT_OK;
   bfgt::device_batch_destroy(batch->db);
+  if (batch->adj) bfgt::device_batch_destroy(*batch->adj);
   delete batch;
   return BFGT_OK;
 }

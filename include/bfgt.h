@@ -231,6 +231,11 @@ int bfgt_batch_create(bfgt_batch *batch, int nplans, const bfgt_plan *plans);
 int bfgt_batch_layout(bfgt_batch batch, int64_t *offsets);
 /* pot += K_i fvals for every plan i, on the packed device arrays; asynchronous. */
 int bfgt_batch_execute(bfgt_batch batch, const double *d_fvals, double *d_pot, void *stream);
+/* The transposed transforms of every plan (bfgt_plan_execute_adjoint),
+   batched the same way, on packed arrays with the same layout:
+   fbar += K_i^T potbar for every plan i.  The first call builds the plans'
+   transposed tables and the batch over them (synchronous). */
+int bfgt_batch_execute_adjoint(bfgt_batch batch, const double *d_potbar, double *d_fbar, void *stream);
 /* Capture bfgt_batch_execute for these buffers into a CUDA graph / replay it. */
 int bfgt_batch_graph_capture(bfgt_batch batch, const double *d_fvals, double *d_pot, void *stream);
 int bfgt_batch_graph_launch(bfgt_batch batch, void *stream);

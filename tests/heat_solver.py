@@ -14,8 +14,8 @@ with F(s) at 4 Gauss-Legendre nodes extrapolated from F^n..F^{n-3}
 
 Gradient of J = 0.5 |u^N - g|^2 with respect to u^0: adjoint stepping with
 checkpoints every `ckpt` steps; the forward states of a segment are recomputed
-from its checkpoint (the step is nonlinear through u^3), and every transform's
-transpose is bfgt_plan_execute_adjoint.
+from its checkpoint (the step is nonlinear through u^3), and the transposes of a
+step's 5 transforms are one batched adjoint (bfgt_batch_execute_adjoint).
 """
 from __future__ import annotations
 
@@ -97,6 +97,14 @@ class HeatStepper:
             fh = [self.forcing(u, (n + 1) * self.dt)] + fh[:3]
         return u
 
+    def adjoint_all(self, lam):
+        """[K_k^T lam for every transform k of the step] by one batched adjoint."""
+        m = self.m
+        pin = lam.repeat(NQ + 1)
+        out = torch.zeros_like(pin)
+        self.batch.execute_adjoint(pin, out, self.stream)
+        return [out[k * m:(k + 1) * m] for k in range(NQ + 1)]
+
     def adjoint_apply(self, k, lam):
         """K_k^T lam for transform k of the batch (0: the initial-value one)."""
         out = torch.zeros_like(lam)
@@ -122,8 +130,9 @@ class HeatStepper:
             for n in reversed(range(s0, s1)):
                 un, fh = wins[n - s0]
                 l1 = lam[0]  # dJ/du^{n+1}
-                gu = self.c0 * self.adjoint_apply(0, l1)
-                wq = [self.cq[q] * self.adjoint_apply(q + 1, l1) for q in range(NQ)]
+                kt = self.adjoint_all(l1)  # K_k^T l1 for the 5 transforms of the step, one batch
+                gu = self.c0 * kt[0]
+                wq = [self.cq[q] * kt[q + 1] for q in range(NQ)]
                 # u^{n+1} depends on u^n directly and on F^{n-j}(u^{n-j}), j = 0..3
                 new = [torch.zeros_like(u0) for _ in range(4)]
                 new[0] = gu

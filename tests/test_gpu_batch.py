@@ -132,3 +132,34 @@ def test_batch_uneven_trees_nd8():
     check_oracle(specs, out, fv)
     # one launch per stage and kernel variant, not per tree
     assert info["launches"] < 2 * len(specs)
+
+
+def test_batch_adjoint_matches_single_plan_adjoints(trees):
+    """bfgt_batch_execute_adjoint: each plan's slice equals its own
+    bfgt_plan_execute_adjoint bit for bit, and sum(g K f) = sum(f K^T g)."""
+    import torch
+    S, F = hb.BFGT_PREC_SPLIT, hb.BFGT_PREC_FP64
+    specs = [(trees["ad16_leg_per"], 1e-4, 1e-6, 1, S), (trees["ad_cheb_free"], 1e-4, 1e-9, 2, F),
+             (trees["uni3_leg_per"], 4e-4, 1e-9, 1, S), (trees["lev1_leaf_per"], 1e-3, 1e-6, 1, S)]
+    plans = [hb.Plan(t, d, e, nd=nd, precision=p) for (t, d, e, nd, p) in specs]
+    batch = hb.Batch(plans)
+    off = batch.offsets
+    g = [leaf_values(t, nd, 300 + i) for i, (t, _, _, nd, _) in enumerate(specs)]
+    f = [leaf_values(t, nd, 400 + i) for i, (t, _, _, nd, _) in enumerate(specs)]
+    G = torch.from_numpy(np.concatenate([x.reshape(-1) for x in g])).cuda()
+    Fv = torch.from_numpy(np.concatenate([x.reshape(-1) for x in f])).cuda()
+    KtG = torch.zeros_like(G)
+    KF = torch.zeros_like(Fv)
+    batch.execute_adjoint(G, KtG)
+    batch.execute(Fv, KF)
+    batch.check()
+    for i, pl in enumerate(plans):
+        gi = torch.from_numpy(g[i].reshape(-1)).cuda()
+        ai = torch.zeros_like(gi)
+        pl.execute_adjoint(gi, ai)
+        np.testing.assert_array_equal(KtG[off[i]:off[i + 1]].cpu().numpy(), ai.cpu().numpy())
+    a, b = torch.dot(KF, G).item(), torch.dot(Fv, KtG).item()
+    assert abs(a - b) <= 1e-6 * KF.norm().item() * G.norm().item()
+    batch.close()
+    for pl in plans:
+        pl.close()

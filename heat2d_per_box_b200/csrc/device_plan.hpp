@@ -14,6 +14,7 @@ namespace bfgt {
 // Tensor-core (split precision) part of a plan.
 struct SplitPlan {
   int cpc = 0, KA = 0, NP = 0, KH = 0, KE = 0, NB = 0, nt = 0, nchunks = 0;
+  int lslots = 1;  // densities whose L the eval kernel holds in shared memory at once
   int4 *chunks = nullptr;
   int *step_begin = nullptr, *steps = nullptr;
   uint16_t *TyB = nullptr, *EyB = nullptr;

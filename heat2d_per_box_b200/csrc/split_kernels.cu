@@ -37,6 +37,9 @@ constexpr uint32_t kWaitIters = 1u << 26;  // bounded spin on an mbarrier
 // dynamic shared memory opt-in: the 227 KB per-block limit minus room for the
 // kernels' static shared variables
 constexpr int kMaxDynSmem = 227 * 1024 - 1024;
+// dynamic shared memory of an eval CTA that still lets two CTAs share an SM
+// (228 KB per SM, 1 KB reserved per CTA, the kernel's static variables)
+constexpr int kEvalSmemTwoPerSm = 112 * 1024;
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -81,9 +84,33 @@ __device__ __forceinline__ int load_desc(const Launch &lp, Args &dst, int *s_ite
   return *s_item;
 }
 
+// Densities packed into the MMA rows.  A chunk of ncol columns fills
+// rpd = ncol n rows per density, so dpc = min(nd, 128 / rpd) densities share
+// one pass through the chunk's steps.  MMA row (and TMEM lane)
+// R = (slot n + m) dpc + dl holds density dl of the pass, the density index
+// fastest: the lanes of a warp then cover consecutive densities of a leaf
+// point, which are adjacent in the (nd, n, n) leaf layout, so their loads and
+// stores of fvals and pot are coalesced.  The passes are balanced:
+// npass = ceil(nd / dpc) passes of ceil(nd / npass) densities (the last one
+// possibly fewer, never none).
+struct DensityPass {
+  int rpd, dpc, npass;
+};
+__device__ __forceinline__ DensityPass density_pass(int ncol, int n, int nd) {
+  DensityPass d;
+  d.rpd = ncol * n;
+  const int dpc = max(min(nd, kRows / d.rpd), 1);
+  d.npass = (nd + dpc - 1) / dpc;
+  d.dpc = (nd + d.npass - 1) / d.npass;
+  return d;
+}
+
 // kBatch: the arguments come from the per-plan descriptors (copied to shared
-// memory) instead of the launch's own parameter block.
-template <int NT, bool kBatch>
+// memory) instead of the launch's own parameter block.  kPack: densities are
+// packed into the rows (plans with nd > 1); without it one density per pass,
+// with the row arithmetic folded at compile time, and NT x-contraction tiles
+// per thread (1 or 2; unused when packed).
+template <bool kBatch, bool kPack, int NT>
 __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ FormTcLaunch lp) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ FormTcArgs s_desc;
@@ -97,6 +124,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
   const int4 ch = a.chunks[chunk];
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, NP = a.NP, KA = a.KA;
   const int ncol = ch.y - ch.x;
+  const DensityPass pk = kPack ? density_pass(ncol, n, nd) : DensityPass{ncol * n, 1, nd};
   const int abytes = 3 * kRows * KA * 2, bbytes = 3 * NP * KA * 2, bufbytes = abytes + bbytes;
   // Y rows padded to an odd number of double2 so that the readout's per-row
   // stores fall in distinct banks
@@ -130,20 +158,23 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
   const int stride = 1 + cpc;
   const uint16_t *tyb = a.TyB + a.tyb_off[ch.w];
   bool ok = true;
-  const int r = tid, rslot = r / n, rm1 = r - rslot * n;
+  // this thread's A row R = (rslot n + rm1) dpc + rdl
+  const int r = tid, rdl = r % pk.dpc, rsk = r / pk.dpc, rslot = rsk / n, rm1 = rsk - rslot * n;
 
   // per-thread share of a B tile (16-byte pieces)
   const int bpieces = bbytes / 16;
   constexpr int kMaxPieces = 4;  // bbytes <= 3*64*16*2 = 6 KB -> 384 pieces / 128 threads = 3
-  for (int ind = 0; ind < nd; ind++) {
+  for (int pass = 0; pass < pk.npass; pass++) {
+    const int d0 = pass * pk.dpc, dcnt = kPack ? min(pk.dpc, nd - d0) : 1;
+    const bool rowok = rdl < dcnt && rsk < pk.rpd;
     // software pipeline: the leaf values and the B tile of step s+1 are
     // loaded into registers while step s is converted and multiplied
     double fnext[16];
     uint4 bnext[kMaxPieces];
     auto load_step = [&](int s2) {
       const int *st2 = a.steps + (size_t)(sb + s2) * stride;
-      const int box = st2[1 + rslot];
-      const double *fv = fvals + (size_t)(box < 0 ? 0 : box) * nd * npb + ind + (size_t)nd * rm1;
+      const int box = rowok ? st2[1 + rslot] : -1;
+      const double *fv = fvals + (size_t)(box < 0 ? 0 : box) * nd * npb + (d0 + rdl) + (size_t)nd * rm1;
 #pragma unroll
       for (int k = 0; k < 16; k++) fnext[k] = (box >= 0 && k < n) ? fv[(size_t)nd * n * k] : 0.0;
       const uint4 *src = reinterpret_cast<const uint4 *>(tyb + (size_t)st2[0] * a.tyb_tile);
@@ -155,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
     };
     if (nsteps > 0) load_step(0);
     for (int s = 0; s < nsteps; s++) {
-      const int g = ind * nsteps + s, b = g & 1;
+      const int g = pass * nsteps + s, b = g & 1;
       double fcur[16];
       uint4 bcur[kMaxPieces];
 #pragma unroll
@@ -168,7 +199,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
         atomicExch(a.err, 1);
       }
       unsigned char *Ab = U + b * bufbytes, *Bb = Ab + abytes;
-      // A row r = (slot, m1): F(m1, m2) for m2 = 0..n-1, zero-padded to KA
+      // A row r = (slot, m1, dl): F(m1, m2) for m2 = 0..n-1, zero-padded to KA
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         if (h >= KA / 8) break;
@@ -211,7 +242,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
       }
     }
     if (nsteps > 0) {
-      const int gl = ind * nsteps + nsteps - 1;
+      const int gl = pass * nsteps + nsteps - 1;
       if (ok && !tc::mbar_wait(&mbar[gl & 1], (gl >> 1) & 1, a.wait_iters)) {
         ok = false;
         atomicExch(a.err, 1);
@@ -239,15 +270,19 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
     }
     tc::fence_before_sync();
     __syncthreads();
-    // x contraction (FP64): M(k1,k2) = sum_{slot,m1} T(m1,k1) conj(ph_ox(k1)) Y(slot,m1,k2)
+    // x contraction (FP64) of each density dl of the pass:
+    // M(k1,k2) = sum_{slot,m1} T(m1,k1) conj(ph_ox(k1)) Y((slot n + m1) dpc + dl, k2),
+    // in 2 x 4 tiles (k1 pair, k2 quad): NT per thread unpacked, (dl, tile)
+    // pairs over the block packed
     {
-      const int ntm = (npw + 1) / 2, ntn = (hh + 3) / 4, ntiles = ntm * ntn;
-      double2 *out = a.Mpart + ((size_t)chunk * nd + ind) * a.nexp;
-#pragma unroll
-      for (int t = 0; t < NT; t++) {
-        const int tile = tid + kThreads * t;
-        if (tile >= ntiles) continue;
-        const int k1b = (tile % ntm) * 2, k2b = (tile / ntm) * 4;
+      const int ntm = (npw + 1) / 2, ntd = ntm * ((hh + 3) / 4), ntiles = dcnt * ntd;
+      const int yst = pk.dpc * ys;  // row stride between grid points of one density
+      for (int it = 0; kPack || it < NT; it++) {
+        const int tile = tid + kThreads * it;
+        if (tile >= ntiles) break;
+        const int dl = kPack ? tile / ntd : 0, tt = tile - dl * ntd;
+        const int k1b = (tt % ntm) * 2, k2b = (tt / ntm) * 4;
+        const double2 *Yd = sY + (size_t)dl * ys;
         double2 acc[2][4];
 #pragma unroll
         for (int i = 0; i < 2; i++)
@@ -266,7 +301,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
 #pragma unroll
             for (int i = 0; i < 2; i++) av[i] = zmul((k1b + i < npw) ? sT[m1 * npw + k1b + i] : make_double2(0, 0), ph[i]);
 #pragma unroll
-            for (int j = 0; j < 4; j++) bv[j] = (k2b + j < hh) ? sY[(slot * n + m1) * ys + k2b + j] : make_double2(0, 0);
+            for (int j = 0; j < 4; j++) bv[j] = (k2b + j < hh) ? Yd[(slot * n + m1) * yst + k2b + j] : make_double2(0, 0);
 #pragma unroll
             for (int i = 0; i < 2; i++)
 #pragma unroll
@@ -278,6 +313,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
               }
           }
         }
+        double2 *out = a.Mpart + ((size_t)chunk * nd + d0 + dl) * a.nexp;
 #pragma unroll
         for (int i = 0; i < 2; i++)
 #pragma unroll
@@ -310,6 +346,7 @@ struct EvalTcArgs {
   const double2 *L;
   int *err;
   int nd, n, npw, hh, nexp, cpc, NB, KE, KH;
+  int lslots;              // densities whose L the shared memory holds at once
   uint32_t wait_iters;
   long long elem_off;      // start of this plan's leaf arrays in the (packed) pot
 };
@@ -326,15 +363,81 @@ struct EvalTcLaunch {
 constexpr int kEvalBatch = 8;
 constexpr int kEvalThreads = 256;
 
+// H rows of kT 8-row tiles that share one density's L, on the FP64 tensor
+// cores: the real GEMM [Hr Hi] = [Er Ei] [[Lr Li], [-Li Lr]] with K = (m1,
+// re/im) and N = (m2, re/im) interleaved, E(m1,k1) phase_ox(m1) formed on the
+// fly.  Lane (g8, t4) of tile mt has row slot rs[mt] and grid index rk[mt].
+template <int NNT, int kT>
+__device__ __forceinline__ void h_tiles(double (&c)[kT][NNT][2], const double2 *sE, const double2 *sph,
+                                        const double2 *Lt, const int (&rs)[kT], const int (&rk)[kT], int n, int npw,
+                                        int hh, int g8, int t4) {
+#pragma unroll
+  for (int mt = 0; mt < kT; mt++)
+#pragma unroll
+    for (int i = 0; i < NNT; i++) c[mt][i][0] = c[mt][i][1] = 0.0;
+  const int p = t4 & 1, q = g8 & 1;
+  for (int j = 0; j < (npw + 1) / 2; j++) {
+    const int m1 = 2 * j + (t4 >> 1);
+    const bool mok = m1 < npw;
+    double av[kT];
+#pragma unroll
+    for (int mt = 0; mt < kT; mt++) {
+      double v = 0.0;
+      if (mok) {
+        const double2 e = zmul(sE[m1 * n + rk[mt]], sph[rs[mt] * npw + m1]);
+        v = p ? e.y : e.x;
+      }
+      av[mt] = v;
+    }
+#pragma unroll
+    for (int i = 0; i < NNT; i++) {
+      const int m2 = 4 * i + (g8 >> 1);
+      double bv = 0.0;
+      if (mok && m2 < hh) {
+        const double2 l = Lt[m1 * hh + m2];
+        bv = p == 0 ? (q == 0 ? l.x : l.y) : (q == 0 ? -l.y : l.x);
+      }
+#pragma unroll
+      for (int mt = 0; mt < kT; mt++) tc::dmma_8x8x4(c[mt][i], av[mt], bv);
+    }
+  }
+}
+
+// Lane (g8, t4) holds (Hr, Hi) of row r at m2 = 4i + t4: split into the three
+// BF16 slices of the A operand (K = re/im x m2).
+template <int NNT>
+__device__ __forceinline__ void h_to_operand(unsigned char *sA, int r, const double (&c)[NNT][2], int t4, int hh,
+                                             int KH, int KE) {
+#pragma unroll
+  for (int i = 0; i < NNT; i++) {
+    const int m2 = 4 * i + t4;
+    if (m2 >= hh) continue;
+    uint16_t s0, s1, s2;
+    const uint32_t ore = tc::kmajor_off(r, m2, kRows), oim = tc::kmajor_off(r, KH + m2, kRows);
+    tc::split3_bf16x1(c[i][0], s0, s1, s2);
+    *reinterpret_cast<uint16_t *>(sA + ore) = s0;
+    *reinterpret_cast<uint16_t *>(sA + kRows * KE * 2 + ore) = s1;
+    *reinterpret_cast<uint16_t *>(sA + 2 * kRows * KE * 2 + ore) = s2;
+    tc::split3_bf16x1(c[i][1], s0, s1, s2);
+    *reinterpret_cast<uint16_t *>(sA + oim) = s0;
+    *reinterpret_cast<uint16_t *>(sA + kRows * KE * 2 + oim) = s1;
+    *reinterpret_cast<uint16_t *>(sA + 2 * kRows * KE * 2 + oim) = s2;
+  }
+}
+
 // Cutoff expansions -> leaf values (steps 4+5).  One CTA of 8 warps per chunk,
 // two CTAs per SM.  H(k1,m2) = sum_m1 E(m1,k1) phase_ox(m1) L(m1,m2) is formed
-// in FP64 once per chunk and split into the A operand (rows (slot,k1), K =
-// re/im x m2).  The steps are then taken kEvalBatch at a time: their Ey tiles
-// are copied side by side into one B operand (cp.async, issued while the
-// previous group is read out), 18 MMAs with N = 16 x steps produce the values
-// of every leaf of the group, and the readout adds 2 (D0 + D1) into pot.
-// Warps w and w+4 share TMEM lanes 32 (w%4).. and split the group's steps.
-template <int NNT, bool kBatch>
+// in FP64 once per chunk and density, on 8-row tiles of one density each, and
+// split into the A operand (row (slot n + k1) dpc + dl, K = re/im x m2).  The
+// steps are then taken kEvalBatch at a time: their Ey tiles are copied side by
+// side into one B operand (cp.async, issued while the previous group is read
+// out), 18 MMAs with N = 16 x steps produce the values of every leaf of the
+// group, and the readout adds 2 (D0 + D1) into pot.  Warps w and w+4 share
+// TMEM lanes 32 (w%4).. and split the group's steps.  H is formed for
+// a.lslots densities at a time (their L in shared memory), so the packing of
+// densities into rows does not depend on the shared-memory size.
+// Shared memory: [A][B][E (npw x n)][phases (cpc x npw)][L (lslots x npw x hh)].
+template <int NNT, bool kBatch, bool kPack>
 __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_constant__ EvalTcLaunch lp) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ EvalTcArgs s_desc;
@@ -348,12 +451,14 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
   const int4 ch = a.chunks[chunk];
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, KE = a.KE, KH = a.KH;
   const int ncol = ch.y - ch.x;
+  const DensityPass pk = kPack ? density_pass(ncol, n, nd) : DensityPass{ncol * n, 1, nd};
+  const int nl = npw * hh;  // L entries per density
   const int abytes = 3 * kRows * KE * 2, bbytes = 3 * (16 * kEvalBatch) * KE * 2;
   unsigned char *sA = smem + 128;
   unsigned char *sB = sA + ((abytes + 127) / 128) * 128;
-  double2 *sL = reinterpret_cast<double2 *>(sB + ((bbytes + 127) / 128) * 128);  // [m1][m2]
-  double2 *sE = sL + (size_t)npw * hh;                                             // [m1][k1]
-  double2 *sph = sE + (size_t)npw * n;                                             // [slot][m1]
+  double2 *sE = reinterpret_cast<double2 *>(sB + ((bbytes + 127) / 128) * 128);  // [m1][k1]
+  double2 *sph = sE + (size_t)npw * n;                                            // [slot][m1]
+  double2 *sL = sph + (size_t)cpc * npw;                                          // [dl][m1][m2]
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, 256);
   if (tid == 0) {
@@ -406,75 +511,54 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
   bool ok = true;
   int g = 0;  // MMA groups issued so far (mbarrier phase)
 
-  for (int ind = 0; ind < nd; ind++) {
-    const double2 *Lg = a.L + ((size_t)ch.z * nd + ind) * a.nexp;
-    for (int e = tid; e < a.nexp; e += kEvalThreads) {
-      const int m2 = e / npw, m1 = e - m2 * npw;
-      sL[m1 * hh + m2] = Lg[e];
-    }
-    __syncthreads();
-    // H(r, m2) for rows r = (slot, k1) on the FP64 tensor cores: the real GEMM
-    // [Hr Hi] = [Er Ei] [[Lr Li], [-Li Lr]] with K = (m1, re/im) and N = (m2,
-    // re/im) interleaved, E(m1,k1) phase_ox(m1) formed on the fly.  Warp w owns
-    // rows 16w..16w+15 (two 8-row tiles) and all NNT column tiles.
-    {
+  for (int pass = 0; pass < pk.npass; pass++) {
+    const int d0 = pass * pk.dpc, dcnt = kPack ? min(pk.dpc, nd - d0) : 1;
+    // H for logical rows r = (dl, slot, k1) (h_tiles).  Warp w owns logical
+    // rows 16w..16w+15 (two 8-row tiles, each of one density dl) and all NNT
+    // column tiles.  Densities [dg, dg + lslots) are formed together; a tile
+    // whose density is outside that range waits for its own group.
+    for (int dg = 0; dg < dcnt; dg += a.lslots) {
+      const int gcnt = min(a.lslots, dcnt - dg);
+      if (dg > 0) __syncthreads();  // every warp is done with the previous group's L
+      for (int e = tid; e < gcnt * nl; e += kEvalThreads) {
+        const int dl = e / nl, el = e - dl * nl;
+        const int m2 = el / npw, m1 = el - m2 * npw;
+        sL[(size_t)dl * nl + m1 * hh + m2] = a.L[((size_t)ch.z * nd + d0 + dg + dl) * a.nexp + el];
+      }
+      __syncthreads();
       const int g8 = lane >> 2, t4 = lane & 3;
-      int rs[2], rk[2];
+      // the warp's two 8-row tiles of logical rows (dl, slot, k1): slot and
+      // grid index of this lane's row, its MMA row (slot n + k1) dpc + dl,
+      // offset of the tile density's L in sL, and whether that density is in
+      // the group
+      int rs[2], rk[2], lo[2], prow[2];
+      bool tv[2];
 #pragma unroll
       for (int mt = 0; mt < 2; mt++) {
-        const int r = 16 * warp + 8 * mt + g8;
-        rs[mt] = r / n;
-        rk[mt] = r - rs[mt] * n;
+        const int r0 = 16 * warp + 8 * mt;
+        const int dl = r0 / pk.rpd;
+        tv[mt] = dl >= dg && dl < dg + gcnt;
+        lo[mt] = (dl - dg) * nl;
+        const int rr = r0 + g8 - dl * pk.rpd;
+        rs[mt] = rr / n;
+        rk[mt] = rr - rs[mt] * n;
+        prow[mt] = rr * pk.dpc + dl;
       }
-      double c[2][NNT][2];
-#pragma unroll
-      for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-        for (int i = 0; i < NNT; i++) c[mt][i][0] = c[mt][i][1] = 0.0;
-      const int p = t4 & 1, q = g8 & 1;
-      for (int j = 0; j < (npw + 1) / 2; j++) {
-        const int m1 = 2 * j + (t4 >> 1);
-        const bool mok = m1 < npw;
-        double av[2];
-#pragma unroll
+      if (tv[0] && tv[1] && lo[0] == lo[1]) {
+        // both tiles, one density (every full-width chunk)
+        double c[2][NNT][2];
+        h_tiles<NNT, 2>(c, sE, sph, sL + lo[0], rs, rk, n, npw, hh, g8, t4);
+        h_to_operand<NNT>(sA, prow[0], c[0], t4, hh, KH, KE);
+        h_to_operand<NNT>(sA, prow[1], c[1], t4, hh, KH, KE);
+      } else {
+        // tiles of two densities, or one tile in the group: one tile at a time
+#pragma unroll 1
         for (int mt = 0; mt < 2; mt++) {
-          double v = 0.0;
-          if (mok && rs[mt] < ncol) {
-            const double2 e = zmul(sE[m1 * n + rk[mt]], sph[rs[mt] * npw + m1]);
-            v = p ? e.y : e.x;
-          }
-          av[mt] = v;
-        }
-#pragma unroll
-        for (int i = 0; i < NNT; i++) {
-          const int m2 = 4 * i + (g8 >> 1);
-          double bv = 0.0;
-          if (mok && m2 < hh) {
-            const double2 l = sL[m1 * hh + m2];
-            bv = p == 0 ? (q == 0 ? l.x : l.y) : (q == 0 ? -l.y : l.x);
-          }
-          tc::dmma_8x8x4(c[0][i], av[0], bv);
-          tc::dmma_8x8x4(c[1][i], av[1], bv);
-        }
-      }
-      // lane holds (Hr, Hi) of row 16w + 8mt + g8, m2 = 4i + t4: split into the A operand
-#pragma unroll
-      for (int mt = 0; mt < 2; mt++) {
-        const int r = 16 * warp + 8 * mt + g8;
-#pragma unroll
-        for (int i = 0; i < NNT; i++) {
-          const int m2 = 4 * i + t4;
-          if (m2 >= hh) continue;
-          uint16_t s0, s1, s2;
-          const uint32_t ore = tc::kmajor_off(r, m2, kRows), oim = tc::kmajor_off(r, KH + m2, kRows);
-          tc::split3_bf16x1(c[mt][i][0], s0, s1, s2);
-          *reinterpret_cast<uint16_t *>(sA + ore) = s0;
-          *reinterpret_cast<uint16_t *>(sA + kRows * KE * 2 + ore) = s1;
-          *reinterpret_cast<uint16_t *>(sA + 2 * kRows * KE * 2 + ore) = s2;
-          tc::split3_bf16x1(c[mt][i][1], s0, s1, s2);
-          *reinterpret_cast<uint16_t *>(sA + oim) = s0;
-          *reinterpret_cast<uint16_t *>(sA + kRows * KE * 2 + oim) = s1;
-          *reinterpret_cast<uint16_t *>(sA + 2 * kRows * KE * 2 + oim) = s2;
+          if (!(mt ? tv[1] : tv[0])) continue;
+          const int rs1[1] = {mt ? rs[1] : rs[0]}, rk1[1] = {mt ? rk[1] : rk[0]};
+          double c[1][NNT][2];
+          h_tiles<NNT, 1>(c, sE, sph, sL + (mt ? lo[1] : lo[0]), rs1, rk1, n, npw, hh, g8, t4);
+          h_to_operand<NNT>(sA, mt ? prow[1] : prow[0], c[0], t4, hh, KH, KE);
         }
       }
     }
@@ -489,7 +573,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
         const uint32_t aA = tc::smem_u32(sA), aB = tc::smem_u32(sB);
         const uint32_t lboA = (kRows / 8) * 128, lboB = (uint32_t)(N / 8) * 128;
         const uint32_t idesc = tc::idesc_bf16_f32(kRows, N);
-        const uint32_t d0 = tmem, d1 = tmem + 128;
+        const uint32_t d0t = tmem, d1t = tmem + 128;
         for (int kk = 0; kk < KE / 16; kk++) {
           uint64_t ad[3], bd[3];
 #pragma unroll
@@ -498,12 +582,12 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
             bd[c] = tc::smem_desc(aB + c * N * KE * 2 + kk * 2 * lboB, lboB, 128);
           }
           const uint32_t acc = kk > 0 ? 1u : 0u;
-          tc::mma_bf16(d0, ad[0], bd[0], idesc, acc);
-          tc::mma_bf16(d1, ad[0], bd[1], idesc, acc);
-          tc::mma_bf16(d1, ad[1], bd[0], idesc, 1u);
-          tc::mma_bf16(d1, ad[0], bd[2], idesc, 1u);
-          tc::mma_bf16(d1, ad[1], bd[1], idesc, 1u);
-          tc::mma_bf16(d1, ad[2], bd[0], idesc, 1u);
+          tc::mma_bf16(d0t, ad[0], bd[0], idesc, acc);
+          tc::mma_bf16(d1t, ad[0], bd[1], idesc, acc);
+          tc::mma_bf16(d1t, ad[1], bd[0], idesc, 1u);
+          tc::mma_bf16(d1t, ad[0], bd[2], idesc, 1u);
+          tc::mma_bf16(d1t, ad[1], bd[1], idesc, 1u);
+          tc::mma_bf16(d1t, ad[2], bd[0], idesc, 1u);
         }
         tc::commit(&mbar[0]);
       }
@@ -514,16 +598,18 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
       tc::fence_after_sync();
       // the B buffer is free again: fetch the next group's tiles during the readout
       if (j + 1 < nbatch) load_batch(s0 + kEvalBatch, min(kEvalBatch, nsteps - s0 - kEvalBatch));
-      else if (ind + 1 < nd) load_batch(0, min(kEvalBatch, nsteps));
+      else if (pass + 1 < pk.npass) load_batch(0, min(kEvalBatch, nsteps));
       // readout: warp w covers TMEM lanes 32 (w%4)..; warps 0-3 take even steps, 4-7 odd steps
       {
-        const int q = warp & 3, r = 32 * q + lane, rslot = r / n, rk1 = r - rslot * n;
-        const uint32_t lb = (uint32_t)(32 * q) << 16;
+        const int qw = warp & 3, r = 32 * qw + lane, rdl = r % pk.dpc, rsk = r / pk.dpc;
+        const int rslot = rsk / n, rk1 = rsk - rslot * n;
+        const bool rowok = rdl < dcnt && rsk < pk.rpd;
+        const uint32_t lb = (uint32_t)(32 * qw) << 16;
         double pv[16];
         double *pb = nullptr;
         auto load_pot = [&](int st) {
-          const int box = st < S ? a.steps[(size_t)(sb + s0 + st) * stride + 1 + rslot] : -1;
-          pb = box >= 0 ? pot + (size_t)box * nd * npb + ind + (size_t)nd * rk1 : nullptr;
+          const int box = (rowok && st < S) ? a.steps[(size_t)(sb + s0 + st) * stride + 1 + rslot] : -1;
+          pb = box >= 0 ? pot + (size_t)box * nd * npb + (d0 + rdl) + (size_t)nd * rk1 : nullptr;
 #pragma unroll
           for (int k2 = 0; k2 < 16; k2++) pv[k2] = (pb && k2 < n) ? pb[(size_t)nd * n * k2] : 0.0;
         };
@@ -561,9 +647,12 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
 // cheap to repeat).
 void set_split_smem_attrs() {
 #define SMEM_ATTR(K) cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  SMEM_ATTR((k_form_tc<1, false>)) SMEM_ATTR((k_form_tc<1, true>))
-  SMEM_ATTR((k_form_tc<2, false>)) SMEM_ATTR((k_form_tc<2, true>))
-#define SMEM_EVAL(X) SMEM_ATTR((k_eval_tc<X, false>)) SMEM_ATTR((k_eval_tc<X, true>))
+  SMEM_ATTR((k_form_tc<false, false, 1>)) SMEM_ATTR((k_form_tc<true, false, 1>))
+  SMEM_ATTR((k_form_tc<false, false, 2>)) SMEM_ATTR((k_form_tc<true, false, 2>))
+  SMEM_ATTR((k_form_tc<false, true, 1>)) SMEM_ATTR((k_form_tc<true, true, 1>))
+#define SMEM_EVAL(X)                                                             \
+  SMEM_ATTR((k_eval_tc<X, false, false>)) SMEM_ATTR((k_eval_tc<X, true, false>)) \
+  SMEM_ATTR((k_eval_tc<X, false, true>)) SMEM_ATTR((k_eval_tc<X, true, true>))
   SMEM_EVAL(1) SMEM_EVAL(2) SMEM_EVAL(3) SMEM_EVAL(4) SMEM_EVAL(5) SMEM_EVAL(6) SMEM_EVAL(7) SMEM_EVAL(8)
 #undef SMEM_EVAL
 #undef SMEM_ATTR
@@ -744,16 +833,20 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     const int ybytes = kRows * (hh | 1) * 16;
     const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 127) / 128) * 128;
     sp.smem_form = 128 + ubytes + sizeof(double2) * (size_t)n * npw;
+    // eval: operands, E, the chunk's phases and lslots densities' L.  As many
+    // L slots as keep two CTAs per SM (up to the densities a pass can pack:
+    // cpc, and 3 nd for the gradient and Hessian views), at least one.
     const int eab = 3 * kRows * sp.KE * 2, ebb = 3 * (16 * kEvalBatch) * sp.KE * 2;
-    sp.smem_eval = 128 + ((eab + 127) / 128) * 128 + ((ebb + 127) / 128) * 128 +
-                   sizeof(double2) * ((size_t)npw * hh + (size_t)npw * n + (size_t)sp.cpc * npw);
+    const size_t ebase = 128 + ((eab + 127) / 128) * 128 + ((ebb + 127) / 128) * 128 +
+                         sizeof(double2) * ((size_t)npw * n + (size_t)sp.cpc * npw);
+    const size_t lbytes = sizeof(double2) * (size_t)npw * hh;
+    const int lcap = std::min(sp.cpc, 3 * hp.nd);
+    sp.lslots = 1;
+    while (sp.lslots < lcap && ebase + (sp.lslots + 1) * lbytes <= (size_t)kEvalSmemTwoPerSm) sp.lslots++;
+    sp.smem_eval = ebase + sp.lslots * lbytes;
   }
-  const int ntiles = ((npw + 1) / 2) * ((hh + 3) / 4);
-  sp.nt = (ntiles + kThreads - 1) / kThreads;
-  if (sp.nt > 2) {
-    msg = "split precision: x-contraction tile count exceeds the built kernels";
-    return BFGT_ERR_CAPACITY;
-  }
+  // x-contraction tiles per form thread (npw <= 64: at most 256 tiles)
+  sp.nt = ((((npw + 1) / 2) * ((hh + 3) / 4)) + kThreads - 1) / kThreads;
   if (sp.smem_form > (size_t)kMaxDynSmem || sp.smem_eval > (size_t)kMaxDynSmem) {
     msg = "split precision: shared memory need exceeds 227 KB";
     return BFGT_ERR_CAPACITY;
@@ -788,29 +881,40 @@ EvalTcArgs eval_args(const DevicePlan &dp, long long elem_off) {
   const SplitPlan &sp = dp.split;
   return EvalTcArgs{sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, dp.E, dp.PH,
                     dp.ph_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
-                    sp.wait_iters, elem_off};
+                    sp.lslots, sp.wait_iters, elem_off};
 }
 
-void launch_form(int nt, int grid, size_t smem, cudaStream_t s, const FormTcLaunch &lp) {
+// variant: 0, 1 = unpacked with 1, 2 x-contraction tiles per thread; 2 = packed
+int form_variant(const DevicePlan &dp) { return dp.nd > 1 ? 2 : dp.split.nt - 1; }
+
+void launch_form(int variant, int grid, size_t smem, cudaStream_t s, const FormTcLaunch &lp) {
   if (grid <= 0) return;
   const bool b = lp.descs != nullptr;
-  if (nt == 1) {
-    if (b) k_form_tc<1, true><<<grid, kThreads, smem, s>>>(lp);
-    else k_form_tc<1, false><<<grid, kThreads, smem, s>>>(lp);
+  if (variant == 2) {
+    if (b) k_form_tc<true, true, 1><<<grid, kThreads, smem, s>>>(lp);
+    else k_form_tc<false, true, 1><<<grid, kThreads, smem, s>>>(lp);
+  } else if (variant == 1) {
+    if (b) k_form_tc<true, false, 2><<<grid, kThreads, smem, s>>>(lp);
+    else k_form_tc<false, false, 2><<<grid, kThreads, smem, s>>>(lp);
   } else {
-    if (b) k_form_tc<2, true><<<grid, kThreads, smem, s>>>(lp);
-    else k_form_tc<2, false><<<grid, kThreads, smem, s>>>(lp);
+    if (b) k_form_tc<true, false, 1><<<grid, kThreads, smem, s>>>(lp);
+    else k_form_tc<false, false, 1><<<grid, kThreads, smem, s>>>(lp);
   }
 }
 
-void launch_eval(int nnt, int grid, size_t smem, cudaStream_t s, const EvalTcLaunch &lp) {
+void launch_eval(int nnt, bool pack, int grid, size_t smem, cudaStream_t s, const EvalTcLaunch &lp) {
   if (grid <= 0) return;
   const bool b = lp.descs != nullptr;
   switch (nnt) {
 #define EVAL_NNT(X)                                                         \
   case X:                                                                   \
-    if (b) k_eval_tc<X, true><<<grid, kEvalThreads, smem, s>>>(lp);         \
-    else k_eval_tc<X, false><<<grid, kEvalThreads, smem, s>>>(lp);          \
+    if (pack) {                                                              \
+      if (b) k_eval_tc<X, true, true><<<grid, kEvalThreads, smem, s>>>(lp);  \
+      else k_eval_tc<X, false, true><<<grid, kEvalThreads, smem, s>>>(lp);  \
+    } else {                                                                 \
+      if (b) k_eval_tc<X, true, false><<<grid, kEvalThreads, smem, s>>>(lp); \
+      else k_eval_tc<X, false, false><<<grid, kEvalThreads, smem, s>>>(lp); \
+    }                                                                        \
     break;
     EVAL_NNT(1) EVAL_NNT(2) EVAL_NNT(3) EVAL_NNT(4) EVAL_NNT(5) EVAL_NNT(6) EVAL_NNT(7) EVAL_NNT(8)
 #undef EVAL_NNT
@@ -821,12 +925,12 @@ void launch_eval(int nnt, int grid, size_t smem, cudaStream_t s, const EvalTcLau
 
 void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
   FormTcLaunch lp{form_args(dp, 0), nullptr, nullptr, d_fvals};
-  launch_form(dp.split.nt, dp.split.nchunks, dp.split.smem_form, s, lp);
+  launch_form(form_variant(dp), dp.split.nchunks, dp.split.smem_form, s, lp);
 }
 
 void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
   EvalTcLaunch lp{eval_args(dp, 0), nullptr, nullptr, d_pot};
-  launch_eval((dp.hh + 3) / 4, dp.split.nchunks, dp.split.smem_eval, s, lp);
+  launch_eval((dp.hh + 3) / 4, dp.nd > 1, dp.split.nchunks, dp.split.smem_eval, s, lp);
 }
 
 int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, const std::vector<long long> &offs,
@@ -834,31 +938,31 @@ int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, co
   split_batch_destroy(b);
   std::vector<FormTcArgs> fd;
   std::vector<EvalTcArgs> ed;
-  // one work item per chunk, grouped by kernel variant (tile count of the
-  // form kernel, column-tile count of the eval kernel); within a group the
-  // plans keep their order
-  std::vector<std::vector<int2>> fw(3), ew(9);
-  std::vector<size_t> fsm(3, 0), esm(9, 0);
+  // one work item per chunk, grouped by kernel variant: form_variant for
+  // form; density packing (nd > 1) and the column-tile count of H for eval
+  // (variant = nnt + 16 pack); within a group the plans keep their order
+  std::vector<std::vector<int2>> fw(3), ew(32);
+  std::vector<size_t> fsm(3, 0), esm(32, 0);
   for (size_t i = 0; i < plans.size(); i++) {
     DevicePlan &dp = *plans[i];
     fd.push_back(form_args(dp, offs[i]));
     ed.push_back(eval_args(dp, offs[i]));
     if (dp.precision != BFGT_PREC_SPLIT || dp.direct_only) continue;
-    const int nt = dp.split.nt, nnt = (dp.hh + 3) / 4;
+    const int fv = form_variant(dp), ev = (dp.hh + 3) / 4 + 16 * (dp.nd > 1 ? 1 : 0);
     for (int c = 0; c < dp.split.nchunks; c++) {
-      fw[nt].push_back(make_int2((int)i, c));
-      ew[nnt].push_back(make_int2((int)i, c));
+      fw[fv].push_back(make_int2((int)i, c));
+      ew[ev].push_back(make_int2((int)i, c));
     }
-    fsm[nt] = std::max(fsm[nt], dp.split.smem_form);
-    esm[nnt] = std::max(esm[nnt], dp.split.smem_eval);
+    fsm[fv] = std::max(fsm[fv], dp.split.smem_form);
+    esm[ev] = std::max(esm[ev], dp.split.smem_eval);
   }
   std::vector<int2> fall, eall;
-  for (int v = 1; v <= 2; v++)
+  for (int v = 0; v < 3; v++)
     if (!fw[v].empty()) {
       b.form_groups.push_back(SplitBatch::Group{v, (int)fall.size(), (int)fw[v].size(), fsm[v]});
       fall.insert(fall.end(), fw[v].begin(), fw[v].end());
     }
-  for (int v = 1; v <= 8; v++)
+  for (int v = 0; v < 32; v++)
     if (!ew[v].empty()) {
       b.eval_groups.push_back(SplitBatch::Group{v, (int)eall.size(), (int)ew[v].size(), esm[v]});
       eall.insert(eall.end(), ew[v].begin(), ew[v].end());
@@ -894,7 +998,7 @@ void split_batch_eval(const SplitBatch &b, double *pbase, cudaStream_t s) {
     lp.descs = static_cast<const EvalTcArgs *>(b.eval_descs);
     lp.work = b.eval_work + g.begin;
     lp.pbase = pbase;
-    launch_eval(g.variant, g.count, g.smem, s, lp);
+    launch_eval(g.variant & 15, g.variant >= 16, g.count, g.smem, s, lp);
   }
 }
 

@@ -203,7 +203,7 @@ def run_uneven(args, rank, world):
     import heat2d_per_box_b200 as hb
     torch.cuda.set_device(0)
     nd, eps = 8, 1e-6
-    trees = make_uneven_trees(6)
+    trees = make_uneven_trees(6)[:max(1, min(args.trees, 64))]
     plans = [hb.Plan(t, d, eps, nd=nd, precision=hb.BFGT_PREC_SPLIT) for t, d in trees]
     batch = hb.Batch(plans)
     off = batch.offsets
@@ -256,7 +256,7 @@ def run_uneven(args, rank, world):
     line = {"metric": METRIC, "value": npts / (ms * 1e-3), "unit": "leaf points/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f16-split/f32acc/f64", "data": "synthetic",
-            "config": {"workload": "64 uneven periodic order-8 trees, nd=8, delta log-U[1e-5,1e-1] per tree, "
+            "config": {"workload": f"{len(trees)} uneven periodic order-8 trees, nd=8, delta log-U[1e-5,1e-1] per tree, "
                                    "eps=1e-6, one batch captured as one CUDA graph",
                        "trees": len(trees), "leaves_total": int(sum(leaves)), "leaves_min": int(min(leaves)),
                        "leaves_max": int(max(leaves)), "points_x_nd": int(npts),
@@ -340,6 +340,8 @@ def main():
                     help="adaptive16: one adaptive order-16 tree (default); uneven64: 64 uneven order-8 trees, "
                          "nd=8, batched in one graph; uniform5: the plain FP64 case on a uniform level-5 order-8 "
                          "tree")
+    ap.add_argument("--trees", type=int, default=64,
+                    help="uneven64: use only the first N of the 64 trees (for profiler captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -15,6 +15,10 @@ namespace bfgt {
 struct SplitPlan {
   int cpc = 0, KA = 0, NP = 0, KH = 0, KE = 0, NB = 0, nt = 0, nchunks = 0;
   int lslots = 1;  // densities whose L the eval kernel holds in shared memory at once
+  // work items {chunk, pass} when densities are packed (nd > 1): one CTA per
+  // pass of a chunk; null: one CTA per chunk running all its passes
+  int2 *items = nullptr;
+  int nitems = 0, items_nd = 0;  // items_nd: the density count the passes were cut for
   int4 *chunks = nullptr;
   int *step_begin = nullptr, *steps = nullptr;
   uint16_t *TyB = nullptr, *EyB = nullptr;
@@ -90,7 +94,9 @@ struct DevicePlan {
 
 struct ReduceArgs;
 // (Re)builds the reduction groups for a chunk list sorted by cutoff box.
-int build_reduce_groups(DevicePlan &dp, const std::vector<int> &cut_of_chunk, std::string &msg);
+// arrivals: CTAs that write each chunk's partials (empty: one per chunk)
+int build_reduce_groups(DevicePlan &dp, const std::vector<int> &cut_of_chunk, std::string &msg,
+                        const std::vector<int> &arrivals = {});
 
 // Allocates and uploads; returns a BFGT_* status and fills msg on failure.
 int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);

@@ -11,14 +11,16 @@ namespace bfgt {
 // group's partials in chunk order (into M directly when the box has one group,
 // else into G(group)); the last group of a box sums the box's groups in order
 // into M.  Counters are re-armed for the next transform.  This completes the
-// merge to the cutoff level of boxfgt.f:764-783.
+// merge to the cutoff level of boxfgt.f:764-783.  A group expects groups[g].w
+// arrivals: one per CTA that writes partials of its chunks (a chunk's
+// densities may be split over several CTAs).
 struct ReduceArgs {
   const double2 *Mpart;
   double2 *G;
   double2 *M;
   int *gcnt, *bcnt;
   const int *chunk_group;   // chunk -> group
-  const int4 *groups;       // {chunk begin, chunk end, icut, -}
+  const int4 *groups;       // {chunk begin, chunk end, icut, arrivals}
   const int *box_groups;    // icut -> first group (ncut + 1 entries)
 };
 
@@ -43,7 +45,7 @@ __device__ __forceinline__ void finish_cutoff_box(const ReduceArgs &r, int chunk
   const int bg0 = r.box_groups[icut], bg1 = r.box_groups[icut + 1];
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) *s_flag = (atomicAdd(&r.gcnt[g], 1) == gi.y - gi.x - 1) ? 1 : 0;
+  if (threadIdx.x == 0) *s_flag = (atomicAdd(&r.gcnt[g], 1) == gi.w - 1) ? 1 : 0;
   __syncthreads();
   if (!*s_flag) return;
   __threadfence();

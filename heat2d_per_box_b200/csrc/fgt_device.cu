@@ -558,7 +558,8 @@ int alloc_bytes(void **p, size_t bytes, std::string &msg) {
 
 // Groups of at most 32 chunks per cutoff box for the fixed-order reduction
 // done at the end of the form kernels (fgt_common.cuh).
-int build_reduce_groups(DevicePlan &dp, const std::vector<int> &cut_of_chunk, std::string &msg) {
+int build_reduce_groups(DevicePlan &dp, const std::vector<int> &cut_of_chunk, std::string &msg,
+                        const std::vector<int> &arrivals) {
   const void *old[] = {dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups};
   for (const void *p : old)
     if (p) cudaFree(const_cast<void *>(p));
@@ -575,8 +576,12 @@ int build_reduce_groups(DevicePlan &dp, const std::vector<int> &cut_of_chunk, st
     while (c1 < nch && cut_of_chunk[c1] == ic) c1++;
     for (int g0 = c; g0 < c1; g0 += 32) {
       const int g1 = std::min(g0 + 32, c1);
-      for (int q = g0; q < g1; q++) chunk_group[q] = (int)groups.size();
-      groups.push_back(make_int4(g0, g1, ic, 0));
+      int arr = 0;
+      for (int q = g0; q < g1; q++) {
+        chunk_group[q] = (int)groups.size();
+        arr += arrivals.empty() ? 1 : arrivals[q];
+      }
+      groups.push_back(make_int4(g0, g1, ic, arr));
     }
     c = c1;
   }

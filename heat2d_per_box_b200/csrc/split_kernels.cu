@@ -62,10 +62,13 @@ struct FormTcArgs {
   int nd, n, npw, hh, nexp, cpc, NP, KA;
   uint32_t wait_iters;
   long long elem_off;      // start of this plan's leaf arrays in the (packed) fvals
+  const int2 *items;       // {chunk, pass} per CTA; null: CTA b = chunk b, all passes
 };
 
-// One launch of the form kernel: a single plan (descs null, CTA b = chunk b of
-// `one`), or a batch of plans (CTA b = chunk work[b].y of plan work[b].x).
+// One launch of the form kernel: a single plan (descs null, CTA b = work item b
+// of `one`), or a batch of plans (CTA b = work item work[b].y of plan
+// work[b].x).  A plan's work item is a chunk (all its density passes), or
+// one pass of a chunk when the plan lists items.
 struct FormTcLaunch {
   FormTcArgs one;
   const FormTcArgs *descs;
@@ -73,7 +76,7 @@ struct FormTcLaunch {
   const double *fbase;
 };
 
-// Copies this CTA's plan descriptor into shared memory and returns its chunk.
+// Copies this CTA's plan descriptor into shared memory and returns its work item.
 template <typename Args, typename Launch>
 __device__ __forceinline__ int load_desc(const Launch &lp, Args &dst, int *s_item) {
   const Args *src = lp.descs ? lp.descs + lp.work[blockIdx.x].x : &lp.one;
@@ -115,8 +118,9 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ FormTcArgs s_desc;
   __shared__ int s_item;
-  const int chunk = kBatch ? load_desc(lp, s_desc, &s_item) : (int)blockIdx.x;
+  const int item = kBatch ? load_desc(lp, s_desc, &s_item) : (int)blockIdx.x;
   const FormTcArgs &a = kBatch ? s_desc : lp.one;
+  const int chunk = (kPack && a.items) ? a.items[item].x : item;  // items exist for nd > 1 only
   const double *fvals = lp.fbase + a.elem_off;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);  // [0],[1] operand buffers, [2] drain
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 64);
@@ -125,6 +129,9 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, NP = a.NP, KA = a.KA;
   const int ncol = ch.y - ch.x;
   const DensityPass pk = kPack ? density_pass(ncol, n, nd) : DensityPass{ncol * n, 1, nd};
+  // this CTA's density passes: one of an item, or all of the chunk
+  const int pitem = (kPack && a.items) ? a.items[item].y : -1;
+  const int pbeg = pitem < 0 ? 0 : pitem, pend = pitem < 0 ? pk.npass : pitem + 1;
   const int abytes = 3 * kRows * KA * 2, bbytes = 3 * NP * KA * 2, bufbytes = abytes + bbytes;
   // Y rows padded to an odd number of double2 so that the readout's per-row
   // stores fall in distinct banks
@@ -164,7 +171,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
   // per-thread share of a B tile (16-byte pieces)
   const int bpieces = bbytes / 16;
   constexpr int kMaxPieces = 4;  // bbytes <= 3*64*16*2 = 6 KB -> 384 pieces / 128 threads = 3
-  for (int pass = 0; pass < pk.npass; pass++) {
+  for (int pass = pbeg; pass < pend; pass++) {
     const int d0 = pass * pk.dpc, dcnt = kPack ? min(pk.dpc, nd - d0) : 1;
     const bool rowok = rdl < dcnt && rsk < pk.rpd;
     // software pipeline: the leaf values and the B tile of step s+1 are
@@ -186,7 +193,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
     };
     if (nsteps > 0) load_step(0);
     for (int s = 0; s < nsteps; s++) {
-      const int g = pass * nsteps + s, b = g & 1;
+      const int g = (pass - pbeg) * nsteps + s, b = g & 1;  // operand buffer uses so far
       double fcur[16];
       uint4 bcur[kMaxPieces];
 #pragma unroll
@@ -242,7 +249,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
       }
     }
     if (nsteps > 0) {
-      const int gl = pass * nsteps + nsteps - 1;
+      const int gl = (pass - pbeg) * nsteps + nsteps - 1;
       if (ok && !tc::mbar_wait(&mbar[gl & 1], (gl >> 1) & 1, a.wait_iters)) {
         ok = false;
         atomicExch(a.err, 1);
@@ -349,6 +356,7 @@ struct EvalTcArgs {
   int lslots;              // densities whose L the shared memory holds at once
   uint32_t wait_iters;
   long long elem_off;      // start of this plan's leaf arrays in the (packed) pot
+  const int2 *items;       // {chunk, pass} per CTA; null: CTA b = chunk b, all passes
 };
 
 struct EvalTcLaunch {
@@ -442,8 +450,9 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ EvalTcArgs s_desc;
   __shared__ int s_item;
-  const int chunk = kBatch ? load_desc(lp, s_desc, &s_item) : (int)blockIdx.x;
+  const int item = kBatch ? load_desc(lp, s_desc, &s_item) : (int)blockIdx.x;
   const EvalTcArgs &a = kBatch ? s_desc : lp.one;
+  const int chunk = (kPack && a.items) ? a.items[item].x : item;  // items exist for nd > 1 only
   double *pot = lp.pbase + a.elem_off;
   uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);  // [0] MMA group done, [1] drain
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 64);
@@ -452,6 +461,9 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
   const int n = a.n, npw = a.npw, hh = a.hh, nd = a.nd, npb = n * n, cpc = a.cpc, KE = a.KE, KH = a.KH;
   const int ncol = ch.y - ch.x;
   const DensityPass pk = kPack ? density_pass(ncol, n, nd) : DensityPass{ncol * n, 1, nd};
+  // this CTA's density passes: one of an item, or all of the chunk
+  const int pitem = (kPack && a.items) ? a.items[item].y : -1;
+  const int pbeg = pitem < 0 ? 0 : pitem, pend = pitem < 0 ? pk.npass : pitem + 1;
   const int nl = npw * hh;  // L entries per density
   const int abytes = 3 * kRows * KE * 2, bbytes = 3 * (16 * kEvalBatch) * KE * 2;
   unsigned char *sA = smem + 128;
@@ -511,7 +523,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
   bool ok = true;
   int g = 0;  // MMA groups issued so far (mbarrier phase)
 
-  for (int pass = 0; pass < pk.npass; pass++) {
+  for (int pass = pbeg; pass < pend; pass++) {
     const int d0 = pass * pk.dpc, dcnt = kPack ? min(pk.dpc, nd - d0) : 1;
     // H for logical rows r = (dl, slot, k1) (h_tiles).  Warp w owns logical
     // rows 16w..16w+15 (two 8-row tiles, each of one density dl) and all NNT
@@ -598,7 +610,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
       tc::fence_after_sync();
       // the B buffer is free again: fetch the next group's tiles during the readout
       if (j + 1 < nbatch) load_batch(s0 + kEvalBatch, min(kEvalBatch, nsteps - s0 - kEvalBatch));
-      else if (pass + 1 < pk.npass) load_batch(0, min(kEvalBatch, nsteps));
+      else if (pass + 1 < pend) load_batch(0, min(kEvalBatch, nsteps));
       // readout: warp w covers TMEM lanes 32 (w%4)..; warps 0-3 take even steps, 4-7 odd steps
       {
         const int qw = warp & 3, r = 32 * qw + lane, rdl = r % pk.dpc, rsk = r / pk.dpc;
@@ -824,7 +836,25 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     std::vector<int> cut_of_chunk(chunks.size());
     for (size_t c = 0; c < chunks.size(); c++) cut_of_chunk[c] = chunks[c].z;
     dp.nchunks = (int)chunks.size();
-    chk(build_reduce_groups(dp, cut_of_chunk, msg));
+    // nd > 1: one CTA per density pass of a chunk (the passes write disjoint
+    // densities; a wide chunk's passes would otherwise run one after another
+    // in one CTA).  The pass count is the kernels' density_pass.
+    std::vector<int> arrivals;
+    if (dp.nd > 1) {
+      std::vector<int2> items;
+      arrivals.resize(chunks.size());
+      for (size_t c = 0; c < chunks.size(); c++) {
+        const int rpd = (chunks[c].y - chunks[c].x) * n;
+        const int dpc = std::max(std::min(dp.nd, kRows / rpd), 1);
+        const int npass = (dp.nd + dpc - 1) / dpc;
+        arrivals[c] = npass;
+        for (int p = 0; p < npass; p++) items.push_back(make_int2((int)c, p));
+      }
+      chk(upload_vec(sp.items, items, msg));
+      sp.nitems = (int)items.size();
+      sp.items_nd = dp.nd;
+    }
+    chk(build_reduce_groups(dp, cut_of_chunk, msg, arrivals));
   }
   dp.nchunks = (int)chunks.size();
   // shared memory
@@ -862,7 +892,7 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
 
 void split_plan_destroy(DevicePlan &dp) {
   SplitPlan &sp = dp.split;
-  void *ptrs[] = {sp.chunks, sp.step_begin, sp.steps, sp.TyB, sp.EyB, sp.tyb_off, sp.eyb_off, sp.err};
+  void *ptrs[] = {sp.chunks, sp.step_begin, sp.steps, sp.TyB, sp.EyB, sp.tyb_off, sp.eyb_off, sp.err, sp.items};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   sp = SplitPlan();
@@ -870,18 +900,26 @@ void split_plan_destroy(DevicePlan &dp) {
 
 namespace {
 
+// The plan's {chunk, pass} items if they were cut for its density count (a
+// gradient or Hessian view of the eval stage has 2 nd or 3 nd densities and
+// runs whole chunks), and the CTA count that goes with the choice.
+const int2 *split_items(const DevicePlan &dp) {
+  return dp.split.items && dp.nd == dp.split.items_nd ? dp.split.items : nullptr;
+}
+int split_ctas(const DevicePlan &dp) { return split_items(dp) ? dp.split.nitems : dp.split.nchunks; }
+
 FormTcArgs form_args(const DevicePlan &dp, long long elem_off) {
   const SplitPlan &sp = dp.split;
   return FormTcArgs{sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.TyB, sp.tyb_off, sp.tyb_tile, dp.T, dp.PH,
                     dp.ph_off, dp.Mpart, reduce_args(dp), sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc,
-                    sp.NP, sp.KA, sp.wait_iters, elem_off};
+                    sp.NP, sp.KA, sp.wait_iters, elem_off, split_items(dp)};
 }
 
 EvalTcArgs eval_args(const DevicePlan &dp, long long elem_off) {
   const SplitPlan &sp = dp.split;
   return EvalTcArgs{sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, dp.E, dp.PH,
                     dp.ph_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
-                    sp.lslots, sp.wait_iters, elem_off};
+                    sp.lslots, sp.wait_iters, elem_off, split_items(dp)};
 }
 
 // variant: 0, 1 = unpacked with 1, 2 x-contraction tiles per thread; 2 = packed
@@ -925,12 +963,12 @@ void launch_eval(int nnt, bool pack, int grid, size_t smem, cudaStream_t s, cons
 
 void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
   FormTcLaunch lp{form_args(dp, 0), nullptr, nullptr, d_fvals};
-  launch_form(form_variant(dp), dp.split.nchunks, dp.split.smem_form, s, lp);
+  launch_form(form_variant(dp), split_ctas(dp), dp.split.smem_form, s, lp);
 }
 
 void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
   EvalTcLaunch lp{eval_args(dp, 0), nullptr, nullptr, d_pot};
-  launch_eval((dp.hh + 3) / 4, dp.nd > 1, dp.split.nchunks, dp.split.smem_eval, s, lp);
+  launch_eval((dp.hh + 3) / 4, dp.nd > 1, split_ctas(dp), dp.split.smem_eval, s, lp);
 }
 
 int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, const std::vector<long long> &offs,
@@ -938,7 +976,7 @@ int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, co
   split_batch_destroy(b);
   std::vector<FormTcArgs> fd;
   std::vector<EvalTcArgs> ed;
-  // one work item per chunk, grouped by kernel variant: form_variant for
+  // the plans' work items (chunks, or chunk passes), grouped by kernel variant: form_variant for
   // form; density packing (nd > 1) and the column-tile count of H for eval
   // (variant = nnt + 16 pack); within a group the plans keep their order
   std::vector<std::vector<int2>> fw(3), ew(32);
@@ -949,7 +987,7 @@ int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, co
     ed.push_back(eval_args(dp, offs[i]));
     if (dp.precision != BFGT_PREC_SPLIT || dp.direct_only) continue;
     const int fv = form_variant(dp), ev = (dp.hh + 3) / 4 + 16 * (dp.nd > 1 ? 1 : 0);
-    for (int c = 0; c < dp.split.nchunks; c++) {
+    for (int c = 0; c < split_ctas(dp); c++) {
       fw[fv].push_back(make_int2((int)i, c));
       ew[ev].push_back(make_int2((int)i, c));
     }

@@ -37,6 +37,11 @@ constexpr uint32_t kWaitIters = 1u << 26;  // bounded spin on an mbarrier
 // dynamic shared memory opt-in: the 227 KB per-block limit minus room for the
 // kernels' static shared variables
 constexpr int kMaxDynSmem = 227 * 1024 - 1024;
+// resident form CTAs per SM (registers and TMEM of the unpacked variants), and
+// the shortest step range a long chunk is cut into
+constexpr int kFormCtasPerSm = 4;
+constexpr int kLongChunkSteps = 32;
+constexpr int kMinPieceSteps = 16;
 // dynamic shared memory of an eval CTA that still lets two CTAs share an SM
 // (228 KB per SM, 1 KB reserved per CTA, the kernel's static variables)
 constexpr int kEvalSmemTwoPerSm = 112 * 1024;
@@ -760,6 +765,38 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     }
     step_begin.push_back((int)(steps.size() / (1 + sp.cpc)));
     c = e;
+  }
+  // A plan with few, long chunks (a coarse cutoff level: one cutoff box at
+  // delta = 1e-2 on an order-16 tree gives 35 chunks of up to 256 steps)
+  // would leave most SMs idle.  When the chunks fill less than a quarter of
+  // the form kernel's CTA slots, chunks of more than kLongChunkSteps steps
+  // are cut into step ranges of about (total steps) / (slots), at least
+  // kMinPieceSteps: each piece is a chunk of the same columns.  The form kernel's x contraction and the eval
+  // kernel's H are then done once per piece; the partial expansions of the
+  // pieces are summed by the same reduction as those of separate chunks.
+  {
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dp.device) != cudaSuccess || nsm <= 0) {
+      cudaGetLastError();
+      nsm = 148;
+    }
+    const int slots = kFormCtasPerSm * nsm;
+    const int nch = (int)chunks.size(), total = step_begin.back();
+    if (nch > 0 && 4 * nch <= slots) {
+      const int smax = std::max(kMinPieceSteps, (total + slots - 1) / slots);
+      std::vector<int4> pc;
+      std::vector<int> pb(1, 0);
+      for (int c = 0; c < nch; c++) {
+        const int s0 = step_begin[c], ns = step_begin[c + 1] - s0;
+        const int pieces = ns > kLongChunkSteps ? (ns + smax - 1) / smax : 1, per = (ns + pieces - 1) / pieces;
+        for (int q = s0; q < s0 + ns; q += per) {
+          pc.push_back(chunks[c]);
+          pb.push_back(std::min(q + per, s0 + ns));
+        }
+      }
+      chunks.swap(pc);
+      step_begin.swap(pb);
+    }
   }
   // per (level, offset) operand tables
   const long long tyt = 3LL * sp.NP * sp.KA, eyt = 3LL * sp.NB * sp.KE;

@@ -108,10 +108,13 @@ __global__ void __launch_bounds__(kTrThreads) k_translate(const __grid_constant_
   const int icut = (int)(idx / per);
   const size_t r = idx - (size_t)icut * per;
   const int e = (int)(r % nexp);
-  double2 s = a.M[idx];
-  for (int j = a.pw_begin[icut]; j < a.pw_begin[icut + 1]; j++) {
-    const double2 m = a.M[(size_t)a.pw_src[j] * per + r];
-    const double2 w = a.W[(size_t)a.pw_ind[j] * nexp + e];
+  double2 s = __ldg(&a.M[idx]);
+  const int j0 = a.pw_begin[icut], j1 = a.pw_begin[icut + 1];
+  // unrolled so that several neighbours' loads are in flight at once
+#pragma unroll 4
+  for (int j = j0; j < j1; j++) {
+    const double2 m = __ldg(&a.M[(size_t)a.pw_src[j] * per + r]);
+    const double2 w = __ldg(&a.W[(size_t)a.pw_ind[j] * nexp + e]);
     s.x += m.x * w.x - m.y * w.y;
     s.y += m.x * w.y + m.y * w.x;
   }

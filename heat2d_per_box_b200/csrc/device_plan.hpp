@@ -43,6 +43,9 @@ struct DevicePlan {
   int4 *leaves = nullptr;       // {box, ox, oy, level}
   int4 *chunks = nullptr;       // {column begin, column end, icut, level}
   int4 *columns = nullptr;      // {leaf begin, leaf end, ox, -}
+  // the FP64 kernels' columns: the same, with a column of more than 64 leaves
+  // cut into sub-columns of up to 64 (dp.chunks index into these)
+  int4 *columns64 = nullptr;
   int ncolumns = 0;
   int form_tile[3] = {0, 0, 0}, eval_tile[3] = {0, 0, 0};
   int *cut_chunk_begin = nullptr, *cut_pw_begin = nullptr, *cut_pw_src = nullptr, *cut_pw_ind = nullptr;

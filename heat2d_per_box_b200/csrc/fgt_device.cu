@@ -52,6 +52,8 @@ __device__ __forceinline__ void cfma(double2 &acc, double2 a, double2 b) {
 }
 
 constexpr int kWarps = 4;
+// longest column (in leaves) an FP64 chunk keeps whole
+constexpr int kFp64ColumnLeaves = 64;
 
 struct FormArgs {
   const double *fvals;
@@ -674,13 +676,13 @@ int device_plan_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::st
   const std::vector<TileChoice> fc = valid_tiles(dp.npw, dp.hh, kFormTiles, kNFormTiles);
   const std::vector<TileChoice> ec = valid_tiles(dp.n, dp.hh, kEvalTiles, kNEvalTiles);
   for (const TileChoice &t : fc) {
-    FormArgs fa{f, dp.leaves, dp.columns, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, reduce_args(dp), dp.nd, dp.n,
+    FormArgs fa{f, dp.leaves, dp.columns64, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, reduce_args(dp), dp.nd, dp.n,
                 dp.npw, dp.hh, dp.nexp};
     const double ms = time_ms([&] { launch_form_fp64(t, dp.nchunks, dp.smem_form, s, fa); });
     if (ms < tf) tf = ms, bf = t;
   }
   for (const TileChoice &t : ec) {
-    EvalArgs ea{p, dp.leaves, dp.columns, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n,
+    EvalArgs ea{p, dp.leaves, dp.columns64, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n,
                 dp.npw, dp.hh, dp.nexp};
     const double ms = time_ms([&] { launch_eval_fp64(t, dp.nchunks, dp.smem_eval, s, ea); });
     if (ms < te) te = ms, be = t;
@@ -743,13 +745,41 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     chk(upload(dp.W, W, msg));
     std::vector<long long> po(hp.phase_off.begin(), hp.phase_off.end());
     chk(upload(dp.ph_off, po, msg));
-    std::vector<int4> lv(hp.leaves.size()), cv(hp.chunks.size()), colv(hp.columns.size());
+    std::vector<int4> lv(hp.leaves.size()), colv(hp.columns.size());
     for (size_t i = 0; i < lv.size(); i++) lv[i] = make_int4(hp.leaves[i].box, hp.leaves[i].ox, hp.leaves[i].oy, hp.leaves[i].level);
-    for (size_t i = 0; i < cv.size(); i++) cv[i] = make_int4(hp.chunks[i].begin, hp.chunks[i].end, hp.chunks[i].icut, hp.chunks[i].level);
     for (size_t i = 0; i < colv.size(); i++) colv[i] = make_int4(hp.columns[i].begin, hp.columns[i].end, hp.columns[i].ox, 0);
+    // FP64 chunks: the host's chunks, except that a column of more than
+    // kFp64ColumnLeaves leaves (alone in its chunk: a coarse cutoff level gives
+    // columns of 256 leaves) is cut into sub-columns of kFp64ColumnLeaves /
+    // kWarps leaves, kWarps to a chunk (the kernels give each warp a column),
+    // so that such a tree still keeps every SM and warp busy.  The kernels
+    // treat a sub-column like a column; the partial sums meet in the warp and
+    // chunk reductions.
+    std::vector<int4> cv, colv64;
+    std::vector<int> cut_of_chunk;
+    for (const Chunk &ch : hp.chunks) {
+      const Column &c0 = hp.columns[ch.begin];
+      if (ch.end - ch.begin == 1 && c0.end - c0.begin > kFp64ColumnLeaves) {
+        const int sub = kFp64ColumnLeaves / kWarps;
+        for (int b = c0.begin; b < c0.end; b += kFp64ColumnLeaves) {
+          const int first = (int)colv64.size();
+          for (int q = b; q < std::min(b + kFp64ColumnLeaves, c0.end); q += sub)
+            colv64.push_back(make_int4(q, std::min(q + sub, c0.end), c0.ox, 0));
+          cv.push_back(make_int4(first, (int)colv64.size(), ch.icut, ch.level));
+          cut_of_chunk.push_back(ch.icut);
+        }
+      } else {
+        cv.push_back(make_int4((int)colv64.size(), (int)colv64.size() + (ch.end - ch.begin), ch.icut, ch.level));
+        for (int c = ch.begin; c < ch.end; c++)
+          colv64.push_back(make_int4(hp.columns[c].begin, hp.columns[c].end, hp.columns[c].ox, 0));
+        cut_of_chunk.push_back(ch.icut);
+      }
+    }
+    dp.nchunks = (int)cv.size();
     chk(upload(dp.leaves, lv, msg));
     chk(upload(dp.chunks, cv, msg));
     chk(upload(dp.columns, colv, msg));
+    chk(upload(dp.columns64, colv64, msg));
     dp.ncolumns = (int)colv.size();
     chk(upload(dp.cut_chunk_begin, hp.cut_chunk_begin, msg));
     chk(upload(dp.cut_pw_begin, hp.cut_pw_begin, msg));
@@ -762,11 +792,7 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     chk(alloc_bytes((void **)&dp.M, ex * dp.ncut, msg));
     chk(alloc_bytes((void **)&dp.L, ex * dp.ncut, msg));
     if (rc == BFGT_OK) cudaMemset(dp.M, 0, ex * dp.ncut);  // boxes without PW leaves keep zero
-    {
-      std::vector<int> cut_of_chunk(hp.chunks.size());
-      for (size_t c = 0; c < hp.chunks.size(); c++) cut_of_chunk[c] = hp.chunks[c].icut;
-      chk(build_reduce_groups(dp, cut_of_chunk, msg));
-    }
+    chk(build_reduce_groups(dp, cut_of_chunk, msg));
     const int npb = n * n;
     dp.smem_form = sizeof(double2) * ((size_t)n * dp.npw + (size_t)dp.npw * dp.hh +
                                       (size_t)kWarps * ((size_t)n * dp.hh + dp.npw + dp.hh + (npb + 1) / 2));
@@ -820,7 +846,7 @@ void device_plan_destroy(DevicePlan &dp) {
   if (dp.graph_exec) cudaGraphExecDestroy(dp.graph_exec);
   if (dp.graph) cudaGraphDestroy(dp.graph);
   split_plan_destroy(dp);
-  void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.columns, dp.cut_chunk_begin, dp.cut_pw_begin,
+  void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.columns, dp.columns64, dp.cut_chunk_begin, dp.cut_pw_begin,
                   dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.kscale, dp.dfac, dp.Ld, dp.tab3_loc, dp.t_nchild, dp.t_ichild, dp.t_level, dp.t_centers, dp.t_boxsize, dp.t_umat, dp.t_has, dp.t_coefs, dp.t_leaf, dp.Mpart, dp.M, dp.L, dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups, dp.nf_target,
                   dp.nf_begin, dp.nf_src, dp.nf_ixy, dp.tab_loc, dp.ind_loc, dp.d_stage_f, dp.d_stage_p, dp.d_stage_gh};
   for (void *p : ptrs)
@@ -882,7 +908,7 @@ void plan_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
   if (dp.precision == BFGT_PREC_SPLIT) {
     split_form(dp, d_fvals, s);
   } else {
-    FormArgs fa{d_fvals, dp.leaves, dp.columns, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, reduce_args(dp),
+    FormArgs fa{d_fvals, dp.leaves, dp.columns64, dp.chunks, dp.T, dp.PH, dp.ph_off, dp.Mpart, reduce_args(dp),
                 dp.nd, dp.n, dp.npw, dp.hh, dp.nexp};
     launch_form_fp64(TileChoice{dp.form_tile[0], dp.form_tile[1], dp.form_tile[2]}, dp.nchunks, dp.smem_form, s, fa);
   }
@@ -893,7 +919,7 @@ void plan_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
   if (dp.precision == BFGT_PREC_SPLIT) {
     split_eval(dp, d_pot, s);
   } else {
-    EvalArgs ea{d_pot, dp.leaves, dp.columns, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n,
+    EvalArgs ea{d_pot, dp.leaves, dp.columns64, dp.chunks, dp.E, dp.PH, dp.ph_off, dp.L, dp.pw_weight, dp.nd, dp.n,
                 dp.npw, dp.hh, dp.nexp};
     launch_eval_fp64(TileChoice{dp.eval_tile[0], dp.eval_tile[1], dp.eval_tile[2]}, dp.nchunks, dp.smem_eval, s, ea);
   }

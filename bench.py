@@ -533,6 +533,16 @@ def main():
         line["fp64_value"] = F["job_points"] / (F["ms"] * 1e-3)
         line["split_over_fp64"] = value / line["fp64_value"]
         line["fp64_stage_ms"] = {k: round(v, 5) for k, v in F["stage"].items()}
+        # accuracy of the measured split transform against the FP64 one on this
+        # tree (one more execute of each, outside the timed regions; non-leaf
+        # boxes hold zeros in both)
+        outs = []
+        for prec in (main_prec, hb.BFGT_PREC_FP64):
+            p1 = torch.zeros_like(f)
+            results[prec]["plan"].execute(f, p1, stream)
+            outs.append(p1)
+        torch.cuda.synchronize()
+        line["split_rel_l2_err_vs_fp64"] = ((outs[0] - outs[1]).norm() / outs[1].norm()).item()
     for r in results.values():
         r["plan"].close()
     if rank == 0:

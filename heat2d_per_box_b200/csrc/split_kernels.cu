@@ -359,6 +359,7 @@ struct EvalTcArgs {
   int *err;
   int nd, n, npw, hh, nexp, cpc, NB, KE, KH;
   int lslots;              // densities whose L the shared memory holds at once
+  int ebatch;              // steps per tensor-core group (8, or 4 when shared memory is short)
   uint32_t wait_iters;
   long long elem_off;      // start of this plan's leaf arrays in the (packed) pot
   const int2 *items;       // {chunk, pass} per CTA; null: CTA b = chunk b, all passes
@@ -372,8 +373,10 @@ struct EvalTcLaunch {
 };
 
 // Steps of a chunk per tensor-core group in the eval kernel: the group's B
-// operand is the step tiles side by side, N = 16 x steps <= 128.
-constexpr int kEvalBatch = 8;
+// operand is the step tiles side by side, N = 16 x steps <= 128 (the TMEM
+// accumulators hold 128 columns each).  A plan uses 4 instead where that is
+// what keeps two CTAs per SM (large npw).
+constexpr int kEvalBatchMax = 8;
 constexpr int kEvalThreads = 256;
 
 // H rows of kT 8-row tiles that share one density's L, on the FP64 tensor
@@ -442,7 +445,7 @@ __device__ __forceinline__ void h_to_operand(unsigned char *sA, int r, const dou
 // two CTAs per SM.  H(k1,m2) = sum_m1 E(m1,k1) phase_ox(m1) L(m1,m2) is formed
 // in FP64 once per chunk and density, on 8-row tiles of one density each, and
 // split into the A operand (row (slot n + k1) dpc + dl, K = re/im x m2).  The
-// steps are then taken kEvalBatch at a time: their Ey tiles are copied side by
+// steps are then taken a.ebatch at a time: their Ey tiles are copied side by
 // side into one B operand (cp.async, issued while the previous group is read
 // out), 18 MMAs with N = 16 x steps produce the values of every leaf of the
 // group, and the readout adds 2 (D0 + D1) into pot.  Warps w and w+4 share
@@ -470,7 +473,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
   const int pitem = (kPack && a.items) ? a.items[item].y : -1;
   const int pbeg = pitem < 0 ? 0 : pitem, pend = pitem < 0 ? pk.npass : pitem + 1;
   const int nl = npw * hh;  // L entries per density
-  const int abytes = 3 * kRows * KE * 2, bbytes = 3 * (16 * kEvalBatch) * KE * 2;
+  const int eb = a.ebatch;
+  const int abytes = 3 * kRows * KE * 2, bbytes = 3 * (16 * eb) * KE * 2;
   unsigned char *sA = smem + 128;
   unsigned char *sB = sA + ((abytes + 127) / 128) * 128;
   double2 *sE = reinterpret_cast<double2 *>(sB + ((bbytes + 127) / 128) * 128);  // [m1][k1]
@@ -486,7 +490,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
   const int sb = a.step_begin[chunk], se = a.step_begin[chunk + 1], nsteps = se - sb;
   const int stride = 1 + cpc;
   const uint16_t *eyb = a.EyB + a.eyb_off[ch.w];
-  const int nbatch = (nsteps + kEvalBatch - 1) / kEvalBatch;
+  const int nbatch = (nsteps + eb - 1) / eb;
   // Ey tiles of steps [s0, s0+S) -> B rows 16 s .. 16 s + 15 (K-major core layout, N = 16 S)
   auto load_batch = [&](int s0, int S) {
     const int N = 16 * S, KG = KE / 8, U = 3 * KG * 16;
@@ -500,7 +504,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
     }
     tc::cp_async_commit();
   };
-  if (nbatch > 0) load_batch(0, min(kEvalBatch, nsteps));
+  if (nbatch > 0) load_batch(0, min(eb, nsteps));
   // E(m1,k1) of this level and the x phases of the chunk's columns (FP64)
   for (int i = tid; i < npw * n; i += kEvalThreads) {
     const int m = i % npw, k = i / npw;
@@ -580,7 +584,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
       }
     }
     for (int j = 0; j < nbatch; j++, g++) {
-      const int s0 = j * kEvalBatch, S = min(kEvalBatch, nsteps - s0), N = 16 * S;
+      const int s0 = j * eb, S = min(eb, nsteps - s0), N = 16 * S;
       tc::cp_async_wait_all();
       tc::fence_async_smem();
       tc::fence_before_sync();
@@ -614,8 +618,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
       }
       tc::fence_after_sync();
       // the B buffer is free again: fetch the next group's tiles during the readout
-      if (j + 1 < nbatch) load_batch(s0 + kEvalBatch, min(kEvalBatch, nsteps - s0 - kEvalBatch));
-      else if (pass + 1 < pend) load_batch(0, min(kEvalBatch, nsteps));
+      if (j + 1 < nbatch) load_batch(s0 + eb, min(eb, nsteps - s0 - eb));
+      else if (pass + 1 < pend) load_batch(0, min(eb, nsteps));
       // readout: warp w covers TMEM lanes 32 (w%4)..; warps 0-3 take even steps, 4-7 odd steps
       {
         const int qw = warp & 3, r = 32 * qw + lane, rdl = r % pk.dpc, rsk = r / pk.dpc;
@@ -900,13 +904,22 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     const int ybytes = kRows * (hh | 1) * 16;
     const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 127) / 128) * 128;
     sp.smem_form = 128 + ubytes + sizeof(double2) * (size_t)n * npw;
-    // eval: operands, E, the chunk's phases and lslots densities' L.  As many
-    // L slots as keep two CTAs per SM (up to the densities a pass can pack:
-    // cpc, and 3 nd for the gradient and Hessian views), at least one.
-    const int eab = 3 * kRows * sp.KE * 2, ebb = 3 * (16 * kEvalBatch) * sp.KE * 2;
-    const size_t ebase = 128 + ((eab + 127) / 128) * 128 + ((ebb + 127) / 128) * 128 +
-                         sizeof(double2) * ((size_t)npw * n + (size_t)sp.cpc * npw);
+    // eval: operands, E, the chunk's phases and lslots densities' L.  Groups
+    // of 8 steps, or of 4 if only that keeps two CTAs per SM with one L slot;
+    // then as many L slots as keep two CTAs per SM (up to the densities a pass
+    // can pack: cpc, and 3 nd for the gradient and Hessian views), at least one.
     const size_t lbytes = sizeof(double2) * (size_t)npw * hh;
+    const int eab = 3 * kRows * sp.KE * 2;
+    auto eval_base = [&](int eb) {
+      const int ebb = 3 * (16 * eb) * sp.KE * 2;
+      return 128 + ((eab + 127) / 128) * 128 + ((ebb + 127) / 128) * 128 +
+             sizeof(double2) * ((size_t)npw * n + (size_t)sp.cpc * npw);
+    };
+    sp.ebatch = kEvalBatchMax;
+    if (eval_base(kEvalBatchMax) + lbytes > (size_t)kEvalSmemTwoPerSm &&
+        eval_base(kEvalBatchMax / 2) + lbytes <= (size_t)kEvalSmemTwoPerSm)
+      sp.ebatch = kEvalBatchMax / 2;
+    const size_t ebase = eval_base(sp.ebatch);
     const int lcap = std::min(sp.cpc, 3 * hp.nd);
     sp.lslots = 1;
     while (sp.lslots < lcap && ebase + (sp.lslots + 1) * lbytes <= (size_t)kEvalSmemTwoPerSm) sp.lslots++;
@@ -956,7 +969,7 @@ EvalTcArgs eval_args(const DevicePlan &dp, long long elem_off) {
   const SplitPlan &sp = dp.split;
   return EvalTcArgs{sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, dp.E, dp.PH,
                     dp.ph_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
-                    sp.lslots, sp.wait_iters, elem_off, split_items(dp)};
+                    sp.lslots, sp.ebatch, sp.wait_iters, elem_off, split_items(dp)};
 }
 
 // variant: 0, 1 = unpacked with 1, 2 x-contraction tiles per thread; 2 = packed

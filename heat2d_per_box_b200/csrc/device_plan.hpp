@@ -16,6 +16,7 @@ struct SplitPlan {
   int cpc = 0, KA = 0, NP = 0, KH = 0, KE = 0, NB = 0, nt = 0, nchunks = 0;
   int lslots = 1;  // densities whose L the eval kernel holds in shared memory at once
   int ebatch = 8;  // steps per tensor-core group of the eval kernel (8, or 4)
+  bool yfloat = false;  // the form kernel stages Y as float2 (exact: an FP32 sum)
   // work items {chunk, pass} when densities are packed (nd > 1): one CTA per
   // pass of a chunk; null: one CTA per chunk running all its passes
   int2 *items = nullptr;

@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/bfgt.h"
@@ -117,8 +118,8 @@ __device__ __forceinline__ DensityPass density_pass(int ncol, int n, int nd) {
 // memory) instead of the launch's own parameter block.  kPack: densities are
 // packed into the rows (plans with nd > 1); without it one density per pass,
 // with the row arithmetic folded at compile time, and NT x-contraction tiles
-// per thread (1 or 2; unused when packed).
-template <bool kBatch, bool kPack, int NT>
+// per thread (1 or 2; unused when packed).  kYF: Y staged as float2 (see sY).
+template <bool kBatch, bool kPack, int NT, bool kYF>
 __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ FormTcLaunch lp) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ FormTcArgs s_desc;
@@ -138,13 +139,18 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
   const int pitem = (kPack && a.items) ? a.items[item].y : -1;
   const int pbeg = pitem < 0 ? 0 : pitem, pend = pitem < 0 ? pk.npass : pitem + 1;
   const int abytes = 3 * kRows * KA * 2, bbytes = 3 * NP * KA * 2, bufbytes = abytes + bbytes;
-  // Y rows padded to an odd number of double2 so that the readout's per-row
-  // stores fall in distinct banks
+  // Y = D0 + D1 is an FP32 sum, held exactly as (re, im) in YT: float2 where
+  // a double2 Y would be the largest user of this shared area (large npw,
+  // unpacked: less shared memory and traffic, measured faster), else double2
+  // (no conversions in the x contraction, measured faster).  Rows padded to
+  // an odd number of elements so that the readout's per-row stores spread
+  // over the banks.
+  using YT = typename std::conditional<kYF, float2, double2>::type;
   const int ys = hh | 1;
-  const int ybytes = kRows * ys * 16;
+  const int ybytes = kRows * ys * (int)sizeof(YT);
   const int ubytes = ((std::max(2 * bufbytes, ybytes) + 127) / 128) * 128;
   unsigned char *U = smem + 128;
-  double2 *sY = reinterpret_cast<double2 *>(U);  // after the tensor-core loop: [row][k2], row stride ys
+  YT *sY = reinterpret_cast<YT *>(U);  // after the tensor-core loop: [row][k2], row stride ys
   double2 *sT = reinterpret_cast<double2 *>(U + ubytes);  // [m][k] n x npw
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, 128);
@@ -261,7 +267,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
       }
     }
     tc::fence_after_sync();
-    // read the two accumulators of this thread's row and sum them in FP64
+    // read the two accumulators of this thread's row and sum them
     {
       const uint32_t lanebase = (uint32_t)(32 * warp) << 16;
       for (int j0 = 0; j0 < NP; j0 += 16) {
@@ -273,8 +279,8 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
         for (int i = 0; i < 16; i++) {
           const int j = j0 + i;
           // D0 + D1 in FP32 (one more rounding of 2^-24, below the accumulated
-          // error), then one conversion
-          const double y = ok ? (double)(v0[i] + v1[i]) : 0.0;
+          // error); the x contraction converts it to FP64 exactly
+          const float y = ok ? v0[i] + v1[i] : 0.0f;  // stored exactly in YT
           if (j < hh) sY[r * ys + j].x = y;
           else if (j < 2 * hh) sY[r * ys + (j - hh)].y = y;
         }
@@ -294,7 +300,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
         if (tile >= ntiles) break;
         const int dl = kPack ? tile / ntd : 0, tt = tile - dl * ntd;
         const int k1b = (tt % ntm) * 2, k2b = (tt / ntm) * 4;
-        const double2 *Yd = sY + (size_t)dl * ys;
+        const YT *Yd = sY + (size_t)dl * ys;
         double2 acc[2][4];
 #pragma unroll
         for (int i = 0; i < 2; i++)
@@ -313,7 +319,10 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
 #pragma unroll
             for (int i = 0; i < 2; i++) av[i] = zmul((k1b + i < npw) ? sT[m1 * npw + k1b + i] : make_double2(0, 0), ph[i]);
 #pragma unroll
-            for (int j = 0; j < 4; j++) bv[j] = (k2b + j < hh) ? Yd[(slot * n + m1) * yst + k2b + j] : make_double2(0, 0);
+            for (int j = 0; j < 4; j++) {
+              const YT y = (k2b + j < hh) ? Yd[(slot * n + m1) * yst + k2b + j] : YT{0, 0};
+              bv[j] = make_double2(y.x, y.y);
+            }
 #pragma unroll
             for (int i = 0; i < 2; i++)
 #pragma unroll
@@ -668,9 +677,11 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
 // cheap to repeat).
 void set_split_smem_attrs() {
 #define SMEM_ATTR(K) cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  SMEM_ATTR((k_form_tc<false, false, 1>)) SMEM_ATTR((k_form_tc<true, false, 1>))
-  SMEM_ATTR((k_form_tc<false, false, 2>)) SMEM_ATTR((k_form_tc<true, false, 2>))
-  SMEM_ATTR((k_form_tc<false, true, 1>)) SMEM_ATTR((k_form_tc<true, true, 1>))
+  SMEM_ATTR((k_form_tc<false, false, 1, false>)) SMEM_ATTR((k_form_tc<true, false, 1, false>))
+  SMEM_ATTR((k_form_tc<false, false, 2, false>)) SMEM_ATTR((k_form_tc<true, false, 2, false>))
+  SMEM_ATTR((k_form_tc<false, false, 1, true>)) SMEM_ATTR((k_form_tc<true, false, 1, true>))
+  SMEM_ATTR((k_form_tc<false, false, 2, true>)) SMEM_ATTR((k_form_tc<true, false, 2, true>))
+  SMEM_ATTR((k_form_tc<false, true, 1, false>)) SMEM_ATTR((k_form_tc<true, true, 1, false>))
 #define SMEM_EVAL(X)                                                             \
   SMEM_ATTR((k_eval_tc<X, false, false>)) SMEM_ATTR((k_eval_tc<X, true, false>)) \
   SMEM_ATTR((k_eval_tc<X, false, true>)) SMEM_ATTR((k_eval_tc<X, true, true>))
@@ -901,7 +912,11 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   // shared memory
   {
     const int abytes = 3 * kRows * sp.KA * 2, bbytes = 3 * sp.NP * sp.KA * 2;
-    const int ybytes = kRows * (hh | 1) * 16;
+    // Y as float2 when, as double2, it would be the largest user of the area
+    // (unpacked plans; the packed kernel keeps double2)
+    const int ybytes_d = kRows * (hh | 1) * 16;
+    sp.yfloat = hp.nd == 1 && ybytes_d > 2 * (abytes + bbytes);
+    const int ybytes = sp.yfloat ? ybytes_d / 2 : ybytes_d;
     const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 127) / 128) * 128;
     sp.smem_form = 128 + ubytes + sizeof(double2) * (size_t)n * npw;
     // eval: operands, E, the chunk's phases and lslots densities' L.  Groups
@@ -972,22 +987,25 @@ EvalTcArgs eval_args(const DevicePlan &dp, long long elem_off) {
                     sp.lslots, sp.ebatch, sp.wait_iters, elem_off, split_items(dp)};
 }
 
-// variant: 0, 1 = unpacked with 1, 2 x-contraction tiles per thread; 2 = packed
-int form_variant(const DevicePlan &dp) { return dp.nd > 1 ? 2 : dp.split.nt - 1; }
+// variant: 0, 1 = unpacked with 1, 2 x-contraction tiles per thread (+2 with
+// Y as float2); 4 = packed
+int form_variant(const DevicePlan &dp) {
+  return dp.nd > 1 ? 4 : dp.split.nt - 1 + (dp.split.yfloat ? 2 : 0);
+}
 
 void launch_form(int variant, int grid, size_t smem, cudaStream_t s, const FormTcLaunch &lp) {
   if (grid <= 0) return;
   const bool b = lp.descs != nullptr;
-  if (variant == 2) {
-    if (b) k_form_tc<true, true, 1><<<grid, kThreads, smem, s>>>(lp);
-    else k_form_tc<false, true, 1><<<grid, kThreads, smem, s>>>(lp);
-  } else if (variant == 1) {
-    if (b) k_form_tc<true, false, 2><<<grid, kThreads, smem, s>>>(lp);
-    else k_form_tc<false, false, 2><<<grid, kThreads, smem, s>>>(lp);
-  } else {
-    if (b) k_form_tc<true, false, 1><<<grid, kThreads, smem, s>>>(lp);
-    else k_form_tc<false, false, 1><<<grid, kThreads, smem, s>>>(lp);
+#define FORM_V(V, P, NT, YF)                                                    \
+  case V:                                                                       \
+    if (b) k_form_tc<true, P, NT, YF><<<grid, kThreads, smem, s>>>(lp);        \
+    else k_form_tc<false, P, NT, YF><<<grid, kThreads, smem, s>>>(lp);         \
+    break;
+  switch (variant) {
+    FORM_V(0, false, 1, false) FORM_V(1, false, 2, false) FORM_V(2, false, 1, true) FORM_V(3, false, 2, true)
+    FORM_V(4, true, 1, false)
   }
+#undef FORM_V
 }
 
 void launch_eval(int nnt, bool pack, int grid, size_t smem, cudaStream_t s, const EvalTcLaunch &lp) {
@@ -1029,8 +1047,8 @@ int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, co
   // the plans' work items (chunks, or chunk passes), grouped by kernel variant: form_variant for
   // form; density packing (nd > 1) and the column-tile count of H for eval
   // (variant = nnt + 16 pack); within a group the plans keep their order
-  std::vector<std::vector<int2>> fw(3), ew(32);
-  std::vector<size_t> fsm(3, 0), esm(32, 0);
+  std::vector<std::vector<int2>> fw(5), ew(32);
+  std::vector<size_t> fsm(5, 0), esm(32, 0);
   for (size_t i = 0; i < plans.size(); i++) {
     DevicePlan &dp = *plans[i];
     fd.push_back(form_args(dp, offs[i]));
@@ -1045,7 +1063,7 @@ int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, co
     esm[ev] = std::max(esm[ev], dp.split.smem_eval);
   }
   std::vector<int2> fall, eall;
-  for (int v = 0; v < 3; v++)
+  for (int v = 0; v < 5; v++)
     if (!fw[v].empty()) {
       b.form_groups.push_back(SplitBatch::Group{v, (int)fall.size(), (int)fw[v].size(), fsm[v]});
       fall.insert(fall.end(), fw[v].begin(), fw[v].end());

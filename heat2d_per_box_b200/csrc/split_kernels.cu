@@ -119,7 +119,8 @@ __device__ __forceinline__ DensityPass density_pass(int ncol, int n, int nd) {
 // packed into the rows (plans with nd > 1); without it one density per pass,
 // with the row arithmetic folded at compile time, and NT x-contraction tiles
 // per thread (1 or 2; unused when packed).  kYF: Y staged as float2 (see sY).
-template <bool kBatch, bool kPack, int NT, bool kYF>
+// kN: the leaf order n (8 or 16), so that per-thread arrays hold n values.
+template <bool kBatch, bool kPack, int NT, bool kYF, int kN>
 __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ FormTcLaunch lp) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ FormTcArgs s_desc;
@@ -187,14 +188,15 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
     const bool rowok = rdl < dcnt && rsk < pk.rpd;
     // software pipeline: the leaf values and the B tile of step s+1 are
     // loaded into registers while step s is converted and multiplied
-    double fnext[16];
+    double fnext[kN];
     uint4 bnext[kMaxPieces];
     auto load_step = [&](int s2) {
       const int *st2 = a.steps + (size_t)(sb + s2) * stride;
       const int box = rowok ? st2[1 + rslot] : -1;
       const double *fv = fvals + (size_t)(box < 0 ? 0 : box) * nd * npb + (d0 + rdl) + (size_t)nd * rm1;
 #pragma unroll
-      for (int k = 0; k < 16; k++) fnext[k] = (box >= 0 && k < n) ? fv[(size_t)nd * n * k] : 0.0;
+      for (int k = 0; k < kN; k++)
+        fnext[k] = (box >= 0 && (kN == 8 || k < n)) ? fv[(size_t)nd * (kN == 8 ? kN : n) * k] : 0.0;
       const uint4 *src = reinterpret_cast<const uint4 *>(tyb + (size_t)st2[0] * a.tyb_tile);
 #pragma unroll
       for (int q = 0; q < kMaxPieces; q++) {
@@ -205,10 +207,10 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
     if (nsteps > 0) load_step(0);
     for (int s = 0; s < nsteps; s++) {
       const int g = (pass - pbeg) * nsteps + s, b = g & 1;  // operand buffer uses so far
-      double fcur[16];
+      double fcur[kN];
       uint4 bcur[kMaxPieces];
 #pragma unroll
-      for (int k = 0; k < 16; k++) fcur[k] = fnext[k];
+      for (int k = 0; k < kN; k++) fcur[k] = fnext[k];
 #pragma unroll
       for (int q = 0; q < kMaxPieces; q++) bcur[q] = bnext[q];
       if (s + 1 < nsteps) load_step(s + 1);
@@ -223,7 +225,11 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
         if (h >= KA / 8) break;
         uint32_t s0[4], s1[4], s2[4];
 #pragma unroll
-        for (int q = 0; q < 4; q++) tc::split3_bf16x2(fcur[8 * h + 2 * q], fcur[8 * h + 2 * q + 1], s0[q], s1[q], s2[q]);
+        for (int q = 0; q < 4; q++) {
+          const int k = 8 * h + 2 * q;  // K columns past n are zero
+          tc::split3_bf16x2(k < kN ? fcur[k < kN ? k : 0] : 0.0, k + 1 < kN ? fcur[k + 1 < kN ? k + 1 : 0] : 0.0, s0[q],
+                            s1[q], s2[q]);
+        }
         const uint32_t off = tc::kmajor_off(r, 8 * h, kRows);
         *reinterpret_cast<uint4 *>(Ab + off) = *reinterpret_cast<uint4 *>(s0);
         *reinterpret_cast<uint4 *>(Ab + kRows * KA * 2 + off) = *reinterpret_cast<uint4 *>(s1);
@@ -462,7 +468,7 @@ __device__ __forceinline__ void h_to_operand(unsigned char *sA, int r, const dou
 // a.lslots densities at a time (their L in shared memory), so the packing of
 // densities into rows does not depend on the shared-memory size.
 // Shared memory: [A][B][E (npw x n)][phases (cpc x npw)][L (lslots x npw x hh)].
-template <int NNT, bool kBatch, bool kPack>
+template <int NNT, bool kBatch, bool kPack, int kN>
 __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_constant__ EvalTcLaunch lp) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ EvalTcArgs s_desc;
@@ -635,29 +641,35 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
         const int rslot = rsk / n, rk1 = rsk - rslot * n;
         const bool rowok = rdl < dcnt && rsk < pk.rpd;
         const uint32_t lb = (uint32_t)(32 * qw) << 16;
-        double pv[16];
+        double pv[kN];
         double *pb = nullptr;
         auto load_pot = [&](int st) {
           const int box = (rowok && st < S) ? a.steps[(size_t)(sb + s0 + st) * stride + 1 + rslot] : -1;
           pb = box >= 0 ? pot + (size_t)box * nd * npb + (d0 + rdl) + (size_t)nd * rk1 : nullptr;
 #pragma unroll
-          for (int k2 = 0; k2 < 16; k2++) pv[k2] = (pb && k2 < n) ? pb[(size_t)nd * n * k2] : 0.0;
+          for (int k2 = 0; k2 < kN; k2++)  // (n = 16: the same code as before kN existed)
+            pv[k2] = (pb && (kN == 8 || k2 < n)) ? pb[(size_t)nd * (kN == 8 ? kN : n) * k2] : 0.0;
         };
         load_pot(warp >> 2);
         for (int st = warp >> 2; st < S; st += 2) {
-          double pc[16];
+          double pc[kN];
 #pragma unroll
-          for (int k2 = 0; k2 < 16; k2++) pc[k2] = pv[k2];
+          for (int k2 = 0; k2 < kN; k2++) pc[k2] = pv[k2];
           double *pbc = pb;
           if (st + 2 < S) load_pot(st + 2);
-          float v0[16], v1[16];
-          tc::tmem_ld16(tmem + lb + (uint32_t)(16 * st), v0);
-          tc::tmem_ld16(tmem + lb + 128u + (uint32_t)(16 * st), v1);
+          float v0[kN], v1[kN];  // columns 16 st .. 16 st + n - 1 of the step
+          if constexpr (kN == 16) {
+            tc::tmem_ld16(tmem + lb + (uint32_t)(16 * st), v0);
+            tc::tmem_ld16(tmem + lb + 128u + (uint32_t)(16 * st), v1);
+          } else {
+            tc::tmem_ld8(tmem + lb + (uint32_t)(16 * st), v0);
+            tc::tmem_ld8(tmem + lb + 128u + (uint32_t)(16 * st), v1);
+          }
           tc::tmem_ld_wait();
           if (ok && pbc) {
 #pragma unroll
-            for (int k2 = 0; k2 < 16; k2++)
-              if (k2 < n) pbc[(size_t)nd * n * k2] = pc[k2] + 2.0 * (double)(v0[k2] + v1[k2]);
+            for (int k2 = 0; k2 < kN; k2++)
+              if (kN == 8 || k2 < n) pbc[(size_t)nd * (kN == 8 ? kN : n) * k2] = pc[k2] + 2.0 * (double)(v0[k2] + v1[k2]);
           }
         }
       }
@@ -677,15 +689,22 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
 // cheap to repeat).
 void set_split_smem_attrs() {
 #define SMEM_ATTR(K) cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-  SMEM_ATTR((k_form_tc<false, false, 1, false>)) SMEM_ATTR((k_form_tc<true, false, 1, false>))
-  SMEM_ATTR((k_form_tc<false, false, 2, false>)) SMEM_ATTR((k_form_tc<true, false, 2, false>))
-  SMEM_ATTR((k_form_tc<false, false, 1, true>)) SMEM_ATTR((k_form_tc<true, false, 1, true>))
-  SMEM_ATTR((k_form_tc<false, false, 2, true>)) SMEM_ATTR((k_form_tc<true, false, 2, true>))
-  SMEM_ATTR((k_form_tc<false, true, 1, false>)) SMEM_ATTR((k_form_tc<true, true, 1, false>))
-#define SMEM_EVAL(X)                                                             \
-  SMEM_ATTR((k_eval_tc<X, false, false>)) SMEM_ATTR((k_eval_tc<X, true, false>)) \
-  SMEM_ATTR((k_eval_tc<X, false, true>)) SMEM_ATTR((k_eval_tc<X, true, true>))
-  SMEM_EVAL(1) SMEM_EVAL(2) SMEM_EVAL(3) SMEM_EVAL(4) SMEM_EVAL(5) SMEM_EVAL(6) SMEM_EVAL(7) SMEM_EVAL(8)
+#define SMEM_FORM(N)                                                                         \
+  SMEM_ATTR((k_form_tc<false, false, 1, false, N>)) SMEM_ATTR((k_form_tc<true, false, 1, false, N>)) \
+  SMEM_ATTR((k_form_tc<false, false, 2, false, N>)) SMEM_ATTR((k_form_tc<true, false, 2, false, N>)) \
+  SMEM_ATTR((k_form_tc<false, false, 1, true, N>)) SMEM_ATTR((k_form_tc<true, false, 1, true, N>))   \
+  SMEM_ATTR((k_form_tc<false, false, 2, true, N>)) SMEM_ATTR((k_form_tc<true, false, 2, true, N>))   \
+  SMEM_ATTR((k_form_tc<false, true, 1, false, N>)) SMEM_ATTR((k_form_tc<true, true, 1, false, N>))
+  SMEM_FORM(8) SMEM_FORM(16)
+#undef SMEM_FORM
+#define SMEM_EVAL(X, N)                                                                    \
+  SMEM_ATTR((k_eval_tc<X, false, false, N>)) SMEM_ATTR((k_eval_tc<X, true, false, N>)) \
+  SMEM_ATTR((k_eval_tc<X, false, true, N>)) SMEM_ATTR((k_eval_tc<X, true, true, N>))
+#define SMEM_EVAL_N(N)                                                                                 \
+  SMEM_EVAL(1, N) SMEM_EVAL(2, N) SMEM_EVAL(3, N) SMEM_EVAL(4, N) SMEM_EVAL(5, N) SMEM_EVAL(6, N) \
+  SMEM_EVAL(7, N) SMEM_EVAL(8, N)
+  SMEM_EVAL_N(8) SMEM_EVAL_N(16)
+#undef SMEM_EVAL_N
 #undef SMEM_EVAL
 #undef SMEM_ATTR
 }
@@ -988,38 +1007,50 @@ EvalTcArgs eval_args(const DevicePlan &dp, long long elem_off) {
 }
 
 // variant: 0, 1 = unpacked with 1, 2 x-contraction tiles per thread (+2 with
-// Y as float2); 4 = packed
+// Y as float2); 4 = packed; +5 for n = 16
 int form_variant(const DevicePlan &dp) {
-  return dp.nd > 1 ? 4 : dp.split.nt - 1 + (dp.split.yfloat ? 2 : 0);
+  return (dp.nd > 1 ? 4 : dp.split.nt - 1 + (dp.split.yfloat ? 2 : 0)) + (dp.n == 16 ? 5 : 0);
 }
 
 void launch_form(int variant, int grid, size_t smem, cudaStream_t s, const FormTcLaunch &lp) {
   if (grid <= 0) return;
   const bool b = lp.descs != nullptr;
-#define FORM_V(V, P, NT, YF)                                                    \
+#define FORM_V(V, P, NT, YF, N)                                                 \
   case V:                                                                       \
-    if (b) k_form_tc<true, P, NT, YF><<<grid, kThreads, smem, s>>>(lp);        \
-    else k_form_tc<false, P, NT, YF><<<grid, kThreads, smem, s>>>(lp);         \
+    if (b) k_form_tc<true, P, NT, YF, N><<<grid, kThreads, smem, s>>>(lp);     \
+    else k_form_tc<false, P, NT, YF, N><<<grid, kThreads, smem, s>>>(lp);      \
     break;
   switch (variant) {
-    FORM_V(0, false, 1, false) FORM_V(1, false, 2, false) FORM_V(2, false, 1, true) FORM_V(3, false, 2, true)
-    FORM_V(4, true, 1, false)
+    FORM_V(0, false, 1, false, 8) FORM_V(1, false, 2, false, 8) FORM_V(2, false, 1, true, 8)
+    FORM_V(3, false, 2, true, 8) FORM_V(4, true, 1, false, 8)
+    FORM_V(5, false, 1, false, 16) FORM_V(6, false, 2, false, 16) FORM_V(7, false, 1, true, 16)
+    FORM_V(8, false, 2, true, 16) FORM_V(9, true, 1, false, 16)
   }
 #undef FORM_V
 }
 
-void launch_eval(int nnt, bool pack, int grid, size_t smem, cudaStream_t s, const EvalTcLaunch &lp) {
+void launch_eval(int nnt, bool pack, bool n16, int grid, size_t smem, cudaStream_t s, const EvalTcLaunch &lp) {
   if (grid <= 0) return;
   const bool b = lp.descs != nullptr;
   switch (nnt) {
 #define EVAL_NNT(X)                                                         \
   case X:                                                                   \
-    if (pack) {                                                              \
-      if (b) k_eval_tc<X, true, true><<<grid, kEvalThreads, smem, s>>>(lp);  \
-      else k_eval_tc<X, false, true><<<grid, kEvalThreads, smem, s>>>(lp);  \
+    if (n16) {                                                               \
+      if (pack) {                                                            \
+        if (b) k_eval_tc<X, true, true, 16><<<grid, kEvalThreads, smem, s>>>(lp);  \
+        else k_eval_tc<X, false, true, 16><<<grid, kEvalThreads, smem, s>>>(lp);  \
+      } else {                                                               \
+        if (b) k_eval_tc<X, true, false, 16><<<grid, kEvalThreads, smem, s>>>(lp); \
+        else k_eval_tc<X, false, false, 16><<<grid, kEvalThreads, smem, s>>>(lp); \
+      }                                                                      \
     } else {                                                                 \
-      if (b) k_eval_tc<X, true, false><<<grid, kEvalThreads, smem, s>>>(lp); \
-      else k_eval_tc<X, false, false><<<grid, kEvalThreads, smem, s>>>(lp); \
+      if (pack) {                                                            \
+        if (b) k_eval_tc<X, true, true, 8><<<grid, kEvalThreads, smem, s>>>(lp);   \
+        else k_eval_tc<X, false, true, 8><<<grid, kEvalThreads, smem, s>>>(lp);   \
+      } else {                                                               \
+        if (b) k_eval_tc<X, true, false, 8><<<grid, kEvalThreads, smem, s>>>(lp);  \
+        else k_eval_tc<X, false, false, 8><<<grid, kEvalThreads, smem, s>>>(lp);  \
+      }                                                                      \
     }                                                                        \
     break;
     EVAL_NNT(1) EVAL_NNT(2) EVAL_NNT(3) EVAL_NNT(4) EVAL_NNT(5) EVAL_NNT(6) EVAL_NNT(7) EVAL_NNT(8)
@@ -1036,7 +1067,7 @@ void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
 
 void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
   EvalTcLaunch lp{eval_args(dp, 0), nullptr, nullptr, d_pot};
-  launch_eval((dp.hh + 3) / 4, dp.nd > 1, split_ctas(dp), dp.split.smem_eval, s, lp);
+  launch_eval((dp.hh + 3) / 4, dp.nd > 1, dp.n == 16, split_ctas(dp), dp.split.smem_eval, s, lp);
 }
 
 int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, const std::vector<long long> &offs,
@@ -1045,16 +1076,17 @@ int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, co
   std::vector<FormTcArgs> fd;
   std::vector<EvalTcArgs> ed;
   // the plans' work items (chunks, or chunk passes), grouped by kernel variant: form_variant for
-  // form; density packing (nd > 1) and the column-tile count of H for eval
-  // (variant = nnt + 16 pack); within a group the plans keep their order
-  std::vector<std::vector<int2>> fw(5), ew(32);
-  std::vector<size_t> fsm(5, 0), esm(32, 0);
+  // form; density packing (nd > 1), the column-tile count of H and the leaf
+  // order for eval (variant = nnt + 16 pack + 32 (n = 16)); within a group the
+  // plans keep their order
+  std::vector<std::vector<int2>> fw(10), ew(64);
+  std::vector<size_t> fsm(10, 0), esm(64, 0);
   for (size_t i = 0; i < plans.size(); i++) {
     DevicePlan &dp = *plans[i];
     fd.push_back(form_args(dp, offs[i]));
     ed.push_back(eval_args(dp, offs[i]));
     if (dp.precision != BFGT_PREC_SPLIT || dp.direct_only) continue;
-    const int fv = form_variant(dp), ev = (dp.hh + 3) / 4 + 16 * (dp.nd > 1 ? 1 : 0);
+    const int fv = form_variant(dp), ev = (dp.hh + 3) / 4 + 16 * (dp.nd > 1 ? 1 : 0) + 32 * (dp.n == 16 ? 1 : 0);
     for (int c = 0; c < split_ctas(dp); c++) {
       fw[fv].push_back(make_int2((int)i, c));
       ew[ev].push_back(make_int2((int)i, c));
@@ -1063,12 +1095,12 @@ int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, co
     esm[ev] = std::max(esm[ev], dp.split.smem_eval);
   }
   std::vector<int2> fall, eall;
-  for (int v = 0; v < 5; v++)
+  for (int v = 0; v < 10; v++)
     if (!fw[v].empty()) {
       b.form_groups.push_back(SplitBatch::Group{v, (int)fall.size(), (int)fw[v].size(), fsm[v]});
       fall.insert(fall.end(), fw[v].begin(), fw[v].end());
     }
-  for (int v = 0; v < 32; v++)
+  for (int v = 0; v < 64; v++)
     if (!ew[v].empty()) {
       b.eval_groups.push_back(SplitBatch::Group{v, (int)eall.size(), (int)ew[v].size(), esm[v]});
       eall.insert(eall.end(), ew[v].begin(), ew[v].end());
@@ -1104,7 +1136,7 @@ void split_batch_eval(const SplitBatch &b, double *pbase, cudaStream_t s) {
     lp.descs = static_cast<const EvalTcArgs *>(b.eval_descs);
     lp.work = b.eval_work + g.begin;
     lp.pbase = pbase;
-    launch_eval(g.variant & 15, g.variant >= 16, g.count, g.smem, s, lp);
+    launch_eval(g.variant & 15, (g.variant & 16) != 0, g.variant >= 32, g.count, g.smem, s, lp);
   }
 }
 

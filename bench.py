@@ -325,6 +325,63 @@ def run_uniform5(args):
     print(json.dumps(line), flush=True)
 
 
+def run_heat5(args):
+    """The transforms of one time step of the reaction-diffusion / heat solvers
+    (hpots2dadap.f:79, 329-346): the initial-value transform with delta = 4 dt
+    and one volume transform per Gauss-Legendre node s_q of [t_n, t_n + dt]
+    with delta = 4 (t_n + dt - s_q), 4 nodes, dt = 1e-3.  A uniform level-6
+    periodic order-8 tree (4096 leaves), nd = 1, eps = 1e-6, split precision;
+    the 5 plans in one batch, the step replayed as one CUDA graph, and the
+    same 5 plans in FP64 executed one after another for comparison."""
+    import torch
+    import heat2d_per_box_b200 as hb
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(5)
+    ng = 10
+    g = hb.gauss_params(rng.uniform(-0.5, 0.5, (ng, 2)), np.full(ng, 0.02), rng.standard_normal(ng))
+    t = hb.build_uniform(6, g, norder=8, ipoly=0, iperiod=1)
+    dt, eps = 1e-3, 1e-6
+    xq = (np.polynomial.legendre.leggauss(4)[0] + 1) / 2
+    deltas = [4 * dt] + [4 * (1 - x) * dt for x in xq]
+    npts = len(t.leaves()) * t.npbox * len(deltas)
+    stream = torch.cuda.current_stream()
+    res = {}
+    for prec in (hb.BFGT_PREC_SPLIT, hb.BFGT_PREC_FP64):
+        plans = [hb.Plan(t, d, eps if prec == hb.BFGT_PREC_SPLIT else 1e-9, precision=prec) for d in deltas]
+        batch = hb.Batch(plans)
+        off = batch.offsets
+        F = torch.from_numpy(np.tile(t.fvals.reshape(-1), len(deltas))).cuda()
+        P = torch.zeros_like(F)
+        assert F.numel() == off[-1]
+        batch.graph_capture(F, P, stream)
+        for _ in range(args.warmup):
+            batch.graph_launch(stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            batch.graph_launch(stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        batch.check()
+        res[prec] = (e0.elapsed_time(e1) / args.steps, batch.info())
+        batch.close()
+        for pl in plans:
+            pl.close()
+    ms, info = res[hb.BFGT_PREC_SPLIT]
+    line = {"metric": METRIC, "value": npts / (ms * 1e-3), "unit": "leaf points/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f16-split/f32acc/f64", "data": "synthetic",
+            "config": {"workload": "one heat/reaction-diffusion time step: 5 transforms (delta = 4 dt and 4 dt (1 - x_q), "
+                                   "4 Gauss-Legendre nodes, dt = 1e-3) on a uniform level-6 periodic order-8 tree, "
+                                   "nd=1, eps=1e-6, one batch replayed as one CUDA graph",
+                       "leaves": int(len(t.leaves())), "transforms": len(deltas), "points_x_transforms": int(npts),
+                       "deltas": deltas, "launches_per_step": info["launches"]},
+            "fp64_value": npts / (res[hb.BFGT_PREC_FP64][0] * 1e-3),
+            "fp64_ms_per_step": res[hb.BFGT_PREC_FP64][0]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -336,10 +393,10 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "split"])
     ap.add_argument("--small", action="store_true", help="level-6 base tree (for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="adaptive16", choices=["adaptive16", "uneven64", "uniform5"],
+    ap.add_argument("--workload", default="adaptive16", choices=["adaptive16", "uneven64", "uniform5", "heat5"],
                     help="adaptive16: one adaptive order-16 tree (default); uneven64: 64 uneven order-8 trees, "
                          "nd=8, batched in one graph; uniform5: the plain FP64 case on a uniform level-5 order-8 "
-                         "tree")
+                         "tree; heat5: the 5 transforms of one heat-solver time step, batched in one graph")
     ap.add_argument("--trees", type=int, default=64,
                     help="uneven64: use only the first N of the 64 trees (for profiler captures)")
     args = ap.parse_args()
@@ -357,6 +414,9 @@ def main():
         return
     if args.workload == "uniform5":
         run_uniform5(args)
+        return
+    if args.workload == "heat5":
+        run_heat5(args)
         return
 
     import torch

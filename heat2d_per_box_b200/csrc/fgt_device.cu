@@ -52,7 +52,7 @@ __device__ __forceinline__ void cfma(double2 &acc, double2 a, double2 b) {
 }
 
 constexpr int kWarps = 4;
-// longest column (in leaves) an FP64 chunk keeps whole
+// leaves of an FP64 chunk made of sub-columns (kFp64ColumnLeaves / kWarps each)
 constexpr int kFp64ColumnLeaves = 64;
 
 struct FormArgs {
@@ -748,23 +748,30 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     std::vector<int4> lv(hp.leaves.size()), colv(hp.columns.size());
     for (size_t i = 0; i < lv.size(); i++) lv[i] = make_int4(hp.leaves[i].box, hp.leaves[i].ox, hp.leaves[i].oy, hp.leaves[i].level);
     for (size_t i = 0; i < colv.size(); i++) colv[i] = make_int4(hp.columns[i].begin, hp.columns[i].end, hp.columns[i].ox, 0);
-    // FP64 chunks: the host's chunks, except that a column of more than
-    // kFp64ColumnLeaves leaves (alone in its chunk: a coarse cutoff level gives
-    // columns of 256 leaves) is cut into sub-columns of kFp64ColumnLeaves /
-    // kWarps leaves, kWarps to a chunk (the kernels give each warp a column),
-    // so that such a tree still keeps every SM and warp busy.  The kernels
-    // treat a sub-column like a column; the partial sums meet in the warp and
-    // chunk reductions.
+    // FP64 chunks: the host's chunks, except that a chunk with fewer columns
+    // than warps (the kernels give each warp a column) has its columns cut
+    // into sub-columns of at most kFp64ColumnLeaves / kWarps leaves, regrouped
+    // kWarps to a chunk.  A coarse cutoff level gives such chunks: two columns
+    // of 32 leaves, or one of 64 or 256; cut, they keep every warp and SM busy.
+    // The kernels treat a sub-column like a column; the partial sums meet in
+    // the warp and chunk reductions.
     std::vector<int4> cv, colv64;
     std::vector<int> cut_of_chunk;
+    const int sub = kFp64ColumnLeaves / kWarps;
     for (const Chunk &ch : hp.chunks) {
-      const Column &c0 = hp.columns[ch.begin];
-      if (ch.end - ch.begin == 1 && c0.end - c0.begin > kFp64ColumnLeaves) {
-        const int sub = kFp64ColumnLeaves / kWarps;
-        for (int b = c0.begin; b < c0.end; b += kFp64ColumnLeaves) {
+      bool cut = ch.end - ch.begin < kWarps;
+      if (cut) {
+        cut = false;
+        for (int c = ch.begin; c < ch.end; c++) cut = cut || hp.columns[c].end - hp.columns[c].begin > sub;
+      }
+      if (cut) {
+        std::vector<int4> subs;
+        for (int c = ch.begin; c < ch.end; c++)
+          for (int q = hp.columns[c].begin; q < hp.columns[c].end; q += sub)
+            subs.push_back(make_int4(q, std::min(q + sub, hp.columns[c].end), hp.columns[c].ox, 0));
+        for (size_t i = 0; i < subs.size(); i += kWarps) {
           const int first = (int)colv64.size();
-          for (int q = b; q < std::min(b + kFp64ColumnLeaves, c0.end); q += sub)
-            colv64.push_back(make_int4(q, std::min(q + sub, c0.end), c0.ox, 0));
+          for (size_t j = i; j < std::min(i + kWarps, subs.size()); j++) colv64.push_back(subs[j]);
           cv.push_back(make_int4(first, (int)colv64.size(), ch.icut, ch.level));
           cut_of_chunk.push_back(ch.icut);
         }

@@ -42,6 +42,7 @@ constexpr int kMaxDynSmem = 227 * 1024 - 1024;
 // the shortest step range a long chunk is cut into
 constexpr int kFormCtasPerSm = 4;
 constexpr int kLongChunkSteps = 32;
+constexpr int kPieceCols = 4;  // columns of a group split off a short, wide group
 constexpr int kMinPieceSteps = 16;
 // dynamic shared memory of an eval CTA that still lets two CTAs share an SM
 // (228 KB per SM, 1 KB reserved per CTA, the kernel's static variables)
@@ -771,13 +772,47 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   sp.KH = ((hh + 7) / 8) * 8;
   sp.KE = ((2 * sp.KH + 15) / 16) * 16;
   sp.NB = 16;
-  // chunks of up to cpc columns of one (icut, level), and their oy steps
-  std::vector<int4> chunks;
-  std::vector<int> step_begin(1, 0), steps;
+  int nsm = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dp.device) != cudaSuccess || nsm <= 0) {
+    cudaGetLastError();
+    nsm = 148;
+  }
+  const int slots = kFormCtasPerSm * nsm;  // resident form CTAs on the GPU
+  // column groups: up to cpc columns of one (icut, level)
   const std::vector<Column> &cols = hp.columns;
+  std::vector<std::pair<size_t, size_t>> groups;
   for (size_t c = 0; c < cols.size();) {
     size_t e = c;
     while (e < cols.size() && cols[e].icut == cols[c].icut && cols[e].level == cols[c].level && (int)(e - c) < sp.cpc) e++;
+    groups.emplace_back(c, e);
+    c = e;
+  }
+  // A plan whose groups fill less than a quarter of the form kernel's CTA
+  // slots (a small tree, or a coarse cutoff level) splits its short, wide
+  // groups (at most kLongChunkSteps steps, more than kPieceCols columns) into
+  // groups of kPieceCols columns: each column is still contracted once, the
+  // work spreads over more SMs.  Long groups are cut into step ranges below.
+  if (!groups.empty() && 4 * (int)groups.size() <= slots) {
+    std::vector<std::pair<size_t, size_t>> g2;
+    for (const auto &gr : groups) {
+      std::vector<int> oys;
+      for (size_t q = gr.first; q < gr.second; q++)
+        for (int i = cols[q].begin; i < cols[q].end; i++) oys.push_back(hp.leaves[i].oy);
+      std::sort(oys.begin(), oys.end());
+      const int nsteps = (int)(std::unique(oys.begin(), oys.end()) - oys.begin());
+      if ((int)(gr.second - gr.first) > kPieceCols && nsteps <= kLongChunkSteps) {
+        for (size_t q = gr.first; q < gr.second; q += kPieceCols) g2.emplace_back(q, std::min(q + kPieceCols, gr.second));
+      } else {
+        g2.push_back(gr);
+      }
+    }
+    groups.swap(g2);
+  }
+  // chunks (one per group) and their oy steps
+  std::vector<int4> chunks;
+  std::vector<int> step_begin(1, 0), steps;
+  for (const auto &gr : groups) {
+    const size_t c = gr.first, e = gr.second;
     chunks.push_back(make_int4((int)c, (int)e, cols[c].icut, cols[c].level));
     std::vector<size_t> ptr(e - c);
     for (size_t q = c; q < e; q++) ptr[q - c] = cols[q].begin;
@@ -798,7 +833,6 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
       }
     }
     step_begin.push_back((int)(steps.size() / (1 + sp.cpc)));
-    c = e;
   }
   // A plan with few, long chunks (a coarse cutoff level: one cutoff box at
   // delta = 1e-2 on an order-16 tree gives 35 chunks of up to 256 steps)
@@ -809,12 +843,6 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   // kernel's H are then done once per piece; the partial expansions of the
   // pieces are summed by the same reduction as those of separate chunks.
   {
-    int nsm = 0;
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dp.device) != cudaSuccess || nsm <= 0) {
-      cudaGetLastError();
-      nsm = 148;
-    }
-    const int slots = kFormCtasPerSm * nsm;
     const int nch = (int)chunks.size(), total = step_begin.back();
     if (nch > 0 && 4 * nch <= slots) {
       const int smax = std::max(kMinPieceSteps, (total + slots - 1) / slots);

@@ -79,7 +79,7 @@ struct FormArgs {
 // accumulators of a warp stay in registers (NT tiles of TM x TN per lane)
 // across its columns; warps are then summed in a fixed order.
 // L(icut) = M(icut) + sum over its plane-wave list of M(src) * W(shift)
-// (mp -> loc at the cutoff level, boxfgt.f:805-822), one thread per element.
+// (mp -> loc at the cutoff level, boxfgt.f:805-822), one thread per element and group of densities.
 // kscale (hh entries, may be null) multiplies element (k1,k2) by kscale[k2];
 // the transposed transform uses it for the half-spectrum weight.
 struct TrArgs {
@@ -100,32 +100,70 @@ struct TrLaunch {
 
 constexpr int kTrThreads = 256;
 
+// One thread per (cutoff box, group of kTrDens densities, element e): the
+// shift W of each plane-wave-list neighbour is loaded once for the group's
+// densities, and the group's M loads of a neighbour are independent.
+constexpr int kTrDens = 4;
+__host__ __device__ inline size_t tr_threads(int ncut, int nd, int nexp) {
+  return (size_t)ncut * ((nd + kTrDens - 1) / kTrDens) * nexp;
+}
+
 __global__ void __launch_bounds__(kTrThreads) k_translate(const __grid_constant__ TrLaunch lp) {
   const TrArgs &a = lp.descs ? lp.descs[lp.work[blockIdx.x].x] : lp.one;
   const int blk = lp.descs ? lp.work[blockIdx.x].y : (int)blockIdx.x;
-  const int nexp = a.nexp;
-  const size_t per = (size_t)a.nd * nexp;
+  const int nexp = a.nexp, nd = a.nd, ng = (nd + kTrDens - 1) / kTrDens;
+  const size_t per = (size_t)nd * nexp;
   const size_t idx = (size_t)blk * blockDim.x + threadIdx.x;
-  if (idx >= per * a.ncut) return;
-  const int icut = (int)(idx / per);
-  const size_t r = idx - (size_t)icut * per;
-  const int e = (int)(r % nexp);
-  double2 s = __ldg(&a.M[idx]);
-  const int j0 = a.pw_begin[icut], j1 = a.pw_begin[icut + 1];
-  // unrolled so that several neighbours' loads are in flight at once
+  if (idx >= (size_t)a.ncut * ng * nexp) return;
+  if (nd == 1) {
+    // one density: one element per thread, neighbour loop unrolled by 4 (the
+    // group loop below measured slower here)
+    const int icut = (int)(idx / nexp), e = (int)(idx - (size_t)icut * nexp);
+    double2 s = __ldg(&a.M[idx]);
+    const int j0 = a.pw_begin[icut], j1 = a.pw_begin[icut + 1];
 #pragma unroll 4
+    for (int j = j0; j < j1; j++) {
+      const double2 m = __ldg(&a.M[(size_t)a.pw_src[j] * nexp + e]);
+      const double2 w = __ldg(&a.W[(size_t)a.pw_ind[j] * nexp + e]);
+      s.x += m.x * w.x - m.y * w.y;
+      s.y += m.x * w.y + m.y * w.x;
+    }
+    if (a.kscale) {
+      const double f = a.kscale[e / a.npw];
+      s.x *= f;
+      s.y *= f;
+    }
+    a.L[idx] = s;
+    return;
+  }
+  const int icut = (int)(idx / ((size_t)ng * nexp));
+  const int rem = (int)(idx - (size_t)icut * ng * nexp);
+  const int g = rem / nexp, e = rem - g * nexp;
+  const int d0 = g * kTrDens, dn = min(kTrDens, nd - d0);
+  const size_t r = (size_t)d0 * nexp + e;  // element (d0, e) within a box's expansions
+  double2 s[kTrDens];
+#pragma unroll
+  for (int u = 0; u < kTrDens; u++)
+    s[u] = u < dn ? __ldg(&a.M[(size_t)icut * per + r + (size_t)u * nexp]) : make_double2(0, 0);
+  const int j0 = a.pw_begin[icut], j1 = a.pw_begin[icut + 1];
+#pragma unroll 2
   for (int j = j0; j < j1; j++) {
-    const double2 m = __ldg(&a.M[(size_t)a.pw_src[j] * per + r]);
     const double2 w = __ldg(&a.W[(size_t)a.pw_ind[j] * nexp + e]);
-    s.x += m.x * w.x - m.y * w.y;
-    s.y += m.x * w.y + m.y * w.x;
+    const double2 *Ms = a.M + (size_t)a.pw_src[j] * per + r;
+#pragma unroll
+    for (int u = 0; u < kTrDens; u++) {
+      if (u >= dn) break;
+      const double2 m = __ldg(&Ms[(size_t)u * nexp]);
+      s[u].x += m.x * w.x - m.y * w.y;
+      s[u].y += m.x * w.y + m.y * w.x;
+    }
   }
-  if (a.kscale) {
-    const double f = a.kscale[e / a.npw];
-    s.x *= f;
-    s.y *= f;
+  const double f = a.kscale ? a.kscale[e / a.npw] : 1.0;
+#pragma unroll
+  for (int u = 0; u < kTrDens; u++) {
+    if (u >= dn) break;
+    a.L[(size_t)icut * per + r + (size_t)u * nexp] = a.kscale ? make_double2(s[u].x * f, s[u].y * f) : s[u];
   }
-  a.L[idx] = s;
 }
 
 // Ld(icut, c*nd + ind, e) = L(icut, ind, e) * fac(c, e) for nc components:
@@ -958,7 +996,7 @@ int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cu
     // the merge to the cutoff level finishes inside the form kernels
     if (ev) cudaEventRecord(ev[1], s);
     if (ev) cudaEventRecord(ev[2], s);
-    const size_t tot = (size_t)dp.ncut * dp.nd * dp.nexp;
+    const size_t tot = tr_threads(dp.ncut, dp.nd, dp.nexp);
     k_translate<<<(unsigned)((tot + kTrThreads - 1) / kTrThreads), kTrThreads, 0, s>>>(
         TrLaunch{tr_args(dp), nullptr, nullptr});
     if (ev) cudaEventRecord(ev[3], s);
@@ -1267,7 +1305,7 @@ int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, 
     tr.push_back(tr_args(dp));
     nf.push_back(near_args(dp, b.offs[i]));
     if (has_pw(dp)) {
-      const size_t tot = (size_t)dp.ncut * dp.nd * dp.nexp;
+      const size_t tot = tr_threads(dp.ncut, dp.nd, dp.nexp);
       for (size_t k = 0; k < (tot + kTrThreads - 1) / kTrThreads; k++) trw.push_back(make_int2((int)i, (int)k));
     }
     for (int t = 0; t < dp.nnf; t += kWarps) nfw.push_back(make_int2((int)i, t));

@@ -54,6 +54,17 @@ def make_tree(seed, small=False):
     return hb.build_adaptive(g, norder=16, ipoly=0, iperiod=1, eps=1e-10, eta=1.0, minlev=minlev, maxlev=12)
 
 
+def workload_config(tree, delta, eps, world):
+    """The config of the adaptive order-16 workload, identical in both arms."""
+    npts = len(tree.leaves()) * tree.npbox
+    return {"workload": "adaptive order-16 periodic tree, 20 Gaussians (w log-U[1e-3,1e-2], a~N(0,1)), "
+                        "uniform to level 8 then tail<1e-10, max level 12; nd=1",
+            "leaves": int(len(tree.leaves())), "points_per_gpu": int(npts), "nd": 1, "delta": delta, "eps": eps,
+            "norder": 16,
+            "l2": "inputs larger than L2 (leaf fvals + pot = %.0f MB per step)" % (npts * 24 / 1e6),
+            "parallelism": f"replicas x{world} (independent trees)"}
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -156,8 +167,7 @@ def run_reference(args, rank, world):
     line = {"metric": METRIC, "value": v, "unit": "leaf points/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": steps, "warmup": args.warmup, "ms_per_step": el / steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "adaptive order-16 periodic tree, 20 Gaussians, delta=1e-4, eps=1e-6",
-                       "leaves": int(len(t.leaves())), "points": int(npts), "nd": 1, "delta": delta, "eps": eps},
+            "config": workload_config(t, delta, eps, world),
             "cpu_baseline": {"value": v, "unit": "leaf points/s", "cores": threads, "kind": "port",
                              "sample": f"{steps} full transforms of the workload tree (oracle, OpenMP "
                                        f"{threads} threads; bfgt/boxfgt.f restated in C)"},
@@ -562,7 +572,15 @@ def main():
         from oracle import oracle
         threads = os.cpu_count() or 1
         oracle.set_threads(threads)
-        oracle.boxfgt(tree, tree.fvals, args.delta, args.eps)
+        ref = oracle.boxfgt(tree, tree.fvals, args.delta, args.eps).reshape(tree.nboxes, -1)[leaves]
+        # accuracy of each measured GPU path against the oracle on this tree
+        # (one more execute, outside the timed regions)
+        for prec, r in results.items():
+            p1 = torch.zeros_like(f)
+            r["plan"].execute(f, p1, stream)
+            r["plan"].check()
+            got = p1.cpu().numpy().reshape(tree.nboxes, -1)[leaves]
+            r["err_vs_oracle"] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
         reps = 0
         t0 = time.perf_counter()
         while True:
@@ -581,13 +599,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if main_prec == hb.BFGT_PREC_FP64 else "f16-split/f32acc/f64",
         "data": "synthetic",
-        "config": {"workload": "adaptive order-16 periodic tree, 20 Gaussians (w log-U[1e-3,1e-2], a~N(0,1)), "
-                               "uniform to level 8 then tail<1e-10, max level 12; nd=1, delta=1e-4, eps=1e-6",
-                   "leaves": int(len(leaves)), "points_per_gpu": int(npts), "nd": 1, "delta": args.delta,
-                   "eps": args.eps, "norder": 16, "npw": R["info"]["npw"], "npwlevel": R["info"]["npwlevel"],
-                   "precision": "split" if main_prec == hb.BFGT_PREC_SPLIT else "fp64",
-                   "l2": "inputs larger than L2 (leaf fvals + pot = %.0f MB per step)" % (npts * 24 / 1e6),
-                   "parallelism": f"replicas x{world} (independent trees)"},
+        "config": workload_config(tree, args.delta, args.eps, world),
+        "plan": {"npw": R["info"]["npw"], "npwlevel": R["info"]["npwlevel"],
+                 "precision": "split" if main_prec == hb.BFGT_PREC_SPLIT else "fp64"},
         "roofline": roof,
         "stage_ms": {k: round(v, 5) for k, v in stg.items()},
         "clocks": clocks,
@@ -596,6 +610,10 @@ def main():
     }
     if cpu:
         line["cpu_baseline"] = cpu
+    for prec, r in results.items():
+        if "err_vs_oracle" in r:
+            key = "split" if prec == hb.BFGT_PREC_SPLIT else "fp64"
+            line[f"{key}_rel_l2_err_vs_oracle"] = r["err_vs_oracle"]
     if hb.BFGT_PREC_FP64 in results and main_prec != hb.BFGT_PREC_FP64:
         F = results[hb.BFGT_PREC_FP64]
         line["fp64_value"] = F["job_points"] / (F["ms"] * 1e-3)

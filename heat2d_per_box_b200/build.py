@@ -10,6 +10,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -23,7 +24,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["fgt_device.cu", "split_kernels.cu", "noalloc.cu"]
+CU_SOURCES = ["fgt_device.cu", "split_kernels.cu", "split_fix.cu", "noalloc.cu"]
 CPP_SOURCES = ["host_plan.cpp", "tree_build.cpp", "capi.cpp"]
 
 
@@ -57,21 +58,25 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         return LIB
     BUILD.mkdir(exist_ok=True)
     LIBDIR.mkdir(exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for s in CU_SOURCES:
         o = BUILD / (s + ".o")
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE,
                "--expt-relaxed-constexpr", "-c", CSRC / s, "-o", o]
         if ptxas_verbose:
             cmd.insert(1, "-Xptxas=-v")
-        _run(cmd, verbose or ptxas_verbose)
+        cmds.append(cmd)
         objs.append(o)
     for s in CPP_SOURCES:
         o = BUILD / (s + ".o")
         cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
                "-I", os.path.join(CUDA_HOME, "include"), "-I", INCLUDE, "-c", CSRC / s, "-o", o]
-        _run(cmd, verbose)
+        cmds.append(cmd)
         objs.append(o)
+    # the translation units compile independently: in parallel
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(_run, c, verbose or ptxas_verbose) for c in cmds]:
+            f.result()
     tmp = LIB.with_suffix(".so.tmp")
     _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs, "-Xcompiler", "-fopenmp", "-lgomp"],
          verbose)

@@ -17,6 +17,10 @@ struct SplitPlan {
   int lslots = 1;  // densities whose L the eval kernel holds in shared memory at once
   int ebatch = 8;  // steps per tensor-core group of the eval kernel (8, or 4)
   bool yfloat = false;  // the form kernel stages Y as float2 (exact: an FP32 sum)
+  // operand slices: three floating ones, or S fixed-point digits (eps < 1e-7)
+  bool fixed = false;
+  int S = 3;
+  double *csc = nullptr, *esc = nullptr;  // fixed-point column scales of Ty, Ey per level
   // work items {chunk, pass} when densities are packed (nd > 1): one CTA per
   // pass of a chunk; null: one CTA per chunk running all its passes
   int2 *items = nullptr;

@@ -73,9 +73,9 @@ def test_pgh_split_precision(trees, name, delta, eps):
     t = trees[name]
     p, g, h = run_pgh(t, delta, eps, 3, precision=hb.BFGT_PREC_SPLIT)
     rp, rg, rh = oracle.boxfgt_pgh(t, t.fvals, delta, eps, 3)
-    assert rel_l2(leaf(t, p), leaf(t, rp)) < 1e-6
-    assert rel_l2(leaf(t, g), leaf(t, rg)) < 2e-6
-    assert rel_l2(leaf(t, h), leaf(t, rh)) < 2e-6
+    assert rel_l2(leaf(t, p), leaf(t, rp)) < min(1e-6, 10 * eps)
+    assert rel_l2(leaf(t, g), leaf(t, rg)) < min(2e-6, 20 * eps)
+    assert rel_l2(leaf(t, h), leaf(t, rh)) < min(2e-6, 20 * eps)
 
 
 def test_boxfgt_entry_ifpgh3_host_arrays(trees):

@@ -1,7 +1,9 @@
-"""Split-precision tensor-core path (tcgen05, BF16x3 slices) vs the FP64 oracle.
+"""Split-precision tensor-core path (tcgen05, BF16 slices) vs the FP64 oracle.
 
-Specified bar: relative L2 error over leaf values <= 1e-6 against the FP64
-oracle (and <= 10*eps where eps >= 1e-7)."""
+Specified bar: relative L2 error over leaf values <= min(1e-6, 10*eps)
+against the FP64 oracle.  eps >= 1e-7 runs three floating slices (about
+1e-6); smaller eps runs fixed-point (Ozaki) slices, 4 of them down to
+eps = 1e-9 and 5 down to 1e-11; below that a split plan is refused."""
 import numpy as np
 import pytest
 
@@ -13,6 +15,10 @@ from conftest import gauss_sum
 pytestmark = pytest.mark.gpu
 
 SPLIT_TOL = 1e-6
+
+
+def split_bar(eps):
+    return min(SPLIT_TOL, 10 * eps)
 
 
 def rel_l2(a, b):
@@ -35,7 +41,10 @@ def run_split(t, delta, eps, fvals=None, nd=1, pot0=None):
 
 CASES = [("ad16_leg_per", 1e-4, 1e-6), ("ad16_leg_per", 1e-3, 1e-9), ("ad16_leg_per", 1e-2, 1e-6),
          ("ad_leg_per", 1e-4, 1e-6), ("ad_cheb_free", 1e-4, 1e-9), ("uni3_leg_per", 1e-3, 1e-9),
-         ("uni3_cheb_per", 1e-2, 1e-6)]
+         ("uni3_cheb_per", 1e-2, 1e-6),
+         # fixed-point slices: 4 digits (eps 1e-8, 1e-9), 5 digits (1e-10, 1e-11)
+         ("ad16_leg_per", 1e-4, 1e-8), ("ad16_leg_per", 1e-2, 1e-9), ("ad_leg_per", 1e-4, 1e-10),
+         ("ad16_leg_per", 1e-4, 1e-11), ("ad16_leg_per", 1e-2, 1e-11), ("uni3_cheb_per", 1e-2, 1e-10), ("lev1_leaf_per", 1e-3, 1e-9)]
 
 
 @pytest.mark.parametrize("name,delta,eps", CASES)
@@ -45,8 +54,16 @@ def test_split_matches_oracle(trees, name, delta, eps):
     ref = oracle.boxfgt(t, t.fvals, delta, eps)
     lv = t.leaves()
     err = rel_l2(got.reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv])
-    tol = SPLIT_TOL if eps < 1e-7 else min(SPLIT_TOL, 10 * eps)
-    assert err < tol, (err, info)
+    assert err < split_bar(eps), (err, info)
+
+
+def test_split_refuses_eps_it_cannot_reach(trees):
+    """Below eps = 1e-11 the fixed-point slices cannot promise 10*eps: plan
+    creation fails with BFGT_ERR_CAPACITY and names the FP64 mode."""
+    with pytest.raises(hb.BfgtError) as e:
+        hb.Plan(trees["ad16_leg_per"], 1e-4, 1e-12, precision=hb.BFGT_PREC_SPLIT)
+    assert e.value.code == 3
+    assert "FP64" in str(e.value)
 
 
 def test_split_benchmark_statistics_tree():
@@ -55,33 +72,37 @@ def test_split_benchmark_statistics_tree():
     g = hb.gauss_params(rng.uniform(-0.5, 0.5, (20, 2)), np.exp(rng.uniform(np.log(1e-3), np.log(1e-2), 20)),
                         rng.standard_normal(20))
     t = hb.build_adaptive(g, norder=16, ipoly=0, iperiod=1, eps=1e-10, eta=1.0, minlev=6, maxlev=12)
-    for delta, eps in [(1e-4, 1e-6), (1e-2, 1e-6), (1e-4, 1e-9)]:
+    for delta, eps in [(1e-4, 1e-6), (1e-2, 1e-6), (1e-4, 1e-9), (1e-2, 1e-9)]:
         got, info = run_split(t, delta, eps)
         ref = oracle.boxfgt(t, t.fvals, delta, eps)
         lv = t.leaves()
         err = rel_l2(got.reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv])
-        assert err < SPLIT_TOL, (delta, eps, err, info)
+        assert err < split_bar(eps), (delta, eps, err, info)
 
 
-def test_split_multiple_densities_and_accumulate(trees):
-    t = trees["ad16_leg_per"]
-    nd = 2
+@pytest.mark.parametrize("name,eps,nd", [("ad16_leg_per", 1e-6, 2), ("ad16_leg_per", 1e-9, 2),
+                                         ("ad_leg_per", 1e-9, 5)])
+def test_split_multiple_densities_and_accumulate(trees, name, eps, nd):
+    t = trees[name]
     rng = np.random.default_rng(3)
-    fv = np.stack([t.fvals, rng.standard_normal(t.fvals.shape)], axis=2)
+    fv = np.stack([t.fvals] + [rng.standard_normal(t.fvals.shape) for _ in range(nd - 1)], axis=2)
+    fv[t.nchild() > 0] = 0.0
+    fv = np.ascontiguousarray(fv)
     pot0 = rng.standard_normal(t.nboxes * t.npbox * nd)
-    got, _ = run_split(t, 1e-4, 1e-6, fvals=fv, nd=nd, pot0=pot0)
-    ref = oracle.boxfgt(t, fv, 1e-4, 1e-6, nd=nd)
+    got, _ = run_split(t, 1e-4, eps, fvals=fv, nd=nd, pot0=pot0)
+    ref = oracle.boxfgt(t, fv, 1e-4, eps, nd=nd)
     lv = t.leaves()
     g = (got - pot0).reshape(t.nboxes, -1)[lv]
-    assert rel_l2(g, ref.reshape(t.nboxes, -1)[lv]) < SPLIT_TOL
+    assert rel_l2(g, ref.reshape(t.nboxes, -1)[lv]) < split_bar(eps)
     nonleaf = np.nonzero(t.nchild() > 0)[0]
     np.testing.assert_array_equal(got.reshape(t.nboxes, -1)[nonleaf], pot0.reshape(t.nboxes, -1)[nonleaf])
 
 
-def test_split_deterministic(trees):
+@pytest.mark.parametrize("eps", [1e-6, 1e-9])
+def test_split_deterministic(trees, eps):
     t = trees["ad16_leg_per"]
-    a, _ = run_split(t, 1e-4, 1e-6)
-    b, _ = run_split(t, 1e-4, 1e-6)
+    a, _ = run_split(t, 1e-4, eps)
+    b, _ = run_split(t, 1e-4, eps)
     np.testing.assert_array_equal(a, b)
 
 

@@ -700,6 +700,12 @@ int bfgt_batch_create(bfgt_batch *batch, int nplans, const bfgt_plan *plans) {
   for (int i = 0; i < nplans; i++) {
     if (!plans[i]) return fail(BFGT_ERR_ARG, "plan " + std::to_string(i) + " is NULL");
     if (plans[i]->dp.device != dev) return fail(BFGT_ERR_ARG, "plan " + std::to_string(i) + " is on another device");
+    // a plan owns its expansion scratch and arrival counters: two entries of
+    // one plan in a launch would mix their partial sums
+    for (int j = 0; j < i; j++)
+      if (plans[j] == plans[i])
+        return fail(BFGT_ERR_ARG, "plan " + std::to_string(i) + " repeats plan " + std::to_string(j) +
+                                      " (each entry of a batch needs its own plan)");
     b->plans.push_back(plans[i]);
     dps.push_back(&plans[i]->dp);
   }

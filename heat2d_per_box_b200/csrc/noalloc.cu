@@ -1,10 +1,11 @@
 // Allocation-free execution of a planned transform.
 //
-// Some callers cannot call cudaMalloc while they run the transform: code that
-// records its time step into its own CUDA graph, or that runs under a memory
-// manager which owns all device memory (a caching allocator, a solver that
-// reserves its pools at start-up), must not have the library allocate during
-// the stepping loop.  bfgt_plan_execute_noalloc runs the same kernels as
+// Some callers cannot call cudaMalloc while they run the transform.  A solver
+// whose memory manager owns all device memory (a caching allocator, or pools
+// reserved at start-up and handed out by the solver itself) must not have a
+// library allocate behind its back, and cudaMalloc/cudaFree can also stall
+// the device, which a time-stepping loop that keeps the GPU busy cannot
+// afford.  bfgt_plan_execute_noalloc runs the same kernels as
 // bfgt_plan_execute, but takes the plane-wave scratch it needs (the partial
 // expansions of every chunk of leaves, their group sums and the expansions of
 // the cutoff boxes) from one file-scope device array of fixed size instead of
@@ -13,11 +14,17 @@
 // The array holds kNoallocScratchBytes on every GPU that loads this library,
 // until the process exits.  On the first call on a device this file resolves
 // the array's device address with cudaGetSymbolAddress (with that device
-// current); make that first call before any stream capture.  Every call shares
-// the array: calls that overlap on the GPU (other streams, other threads)
-// race on it.  Each call writes every element it later reads, except the
-// expansions of cutoff boxes that hold no plane-wave leaf, which no kernel
-// reads; nothing has to be cleared between calls.
+// current); make that first call before any stream capture.  The address is
+// kept per device ordinal for the life of the process: after cudaDeviceReset
+// it no longer names the array of the new context, so do not use this entry
+// point in a process that resets its device.  Every call shares the array:
+// calls that overlap on the GPU (other streams, other threads) race on it.
+// Each call writes every partial and group expansion it reads, and the
+// expansion of every cutoff box that holds plane-wave leaves.  The cutoff
+// translation also reads the expansion of a cutoff box without plane-wave
+// leaves (its own term), which then holds whatever an earlier call left there;
+// the local expansion computed from it is never read, so no result depends on
+// it and nothing has to be cleared between calls.
 #include <cuda_runtime.h>
 
 #include <mutex>

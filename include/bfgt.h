@@ -140,12 +140,16 @@ int bfgt_plan_execute_adjoint_host(bfgt_plan plan, const double *potbar, double 
    without allocating anything: the plane-wave scratch (partial expansions of
    the leaf chunks and the cutoff-box expansions) comes from one static device
    array of bfgt_noalloc_scratch_bytes() (32 MiB) per GPU, held until exit.
-   For callers that may not allocate device memory while they step, e.g.
-   inside their own graph capture or under an allocator that owns the device.
-   Plans whose scratch need (bfgt_plan_noalloc_need) exceeds the array are
-   rejected with BFGT_ERR_CAPACITY.  The first call on a device looks up the
-   array's address (cudaGetSymbolAddress) and should come before any stream
-   capture; calls that overlap on the GPU share, and race on, the array. */
+   For callers that may not allocate device memory while they step: a solver
+   whose own memory manager owns the device (a caching allocator, pools
+   reserved at start-up), or a stepping loop that cannot afford the device
+   stalls of cudaMalloc/cudaFree.  Plans whose scratch need
+   (bfgt_plan_noalloc_need) exceeds the array are rejected with
+   BFGT_ERR_CAPACITY.  The first call on a device looks up the array's address
+   (cudaGetSymbolAddress) and should come before any stream capture; the
+   address is kept for the life of the process, so a process that calls
+   cudaDeviceReset must not use this entry point afterwards.  Calls that
+   overlap on the GPU share, and race on, the array. */
 int bfgt_plan_execute_noalloc(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream);
 int bfgt_noalloc_scratch_bytes(size_t *bytes);
 int bfgt_plan_noalloc_need(bfgt_plan plan, size_t *bytes);

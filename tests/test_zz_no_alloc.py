@@ -1,7 +1,8 @@
 """bfgt_plan_execute_noalloc: the planned transform without any device
-allocation, for callers that may not allocate while they step (their own
-graph capture, or an allocator that owns the device).  Its plane-wave scratch
-lives in a static array inside the library.  Checked through the C ABI
+allocation, for callers that may not allocate while they step (a solver whose
+memory manager owns the device, or a loop that cannot afford the stalls of
+cudaMalloc/cudaFree).  Its plane-wave scratch lives in a static array inside
+the library.  Checked through the C ABI
 against bfgt_plan_execute on two calls in a row, with the tolerances of the
 other GPU tests (FP64: 1e-11 relative L2; split precision: 1e-6)."""
 import ctypes as C

@@ -57,6 +57,12 @@ def lib():
     L.bfgt_boxfgt.restype = C.c_int
     L.bfgt_boxfgt.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                               _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, C.c_void_p, C.c_int]
+    L.bfgt_set_default_precision.restype = C.c_int
+    L.bfgt_set_default_precision.argtypes = [C.c_int]
+    L.bfgt_plan_cache_clear.restype = C.c_int
+    L.bfgt_plan_cache_clear.argtypes = []
+    L.bfgt_plan_cache_info.restype = C.c_int
+    L.bfgt_plan_cache_info.argtypes = [C.c_void_p]
     L.bfgt_plan_create.restype = C.c_int
     L.bfgt_plan_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
                                    C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, C.c_int]

@@ -56,6 +56,23 @@ def boxfgt(nd, ndim, delta, eps, ipoly, iperiod, norder, npbox, nboxes, nlevels,
     return pot
 
 
+def set_default_precision(precision):
+    """Precision mode of the drop-in boxfgt (BFGT_PREC_FP64 or BFGT_PREC_SPLIT)."""
+    _lib.check(_lib.lib().bfgt_set_default_precision(int(precision)))
+
+
+def plan_cache_info():
+    """The drop-in entry points' plan cache: entries, capacity, hits, misses."""
+    out = np.zeros(4, np.int64)
+    _lib.check(_lib.lib().bfgt_plan_cache_info(out.ctypes.data))
+    return {"entries": int(out[0]), "capacity": int(out[1]), "hits": int(out[2]), "misses": int(out[3])}
+
+
+def plan_cache_clear():
+    """Frees the plans the drop-in entry points keep."""
+    _lib.check(_lib.lib().bfgt_plan_cache_clear())
+
+
 class Plan:
     """Device-resident boxfgt for one tree / delta / eps / norder / nd.
 

@@ -6,7 +6,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <cstdint>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -485,17 +487,158 @@ int bfgt_plan_destroy(bfgt_plan plan) {
 
 namespace {
 
+// ---- plan cache behind boxfgt_ / bfgt_boxfgt ---------------------------------
+// The reference's solvers call boxfgt several times per time step on an
+// unchanged tree (hpots/hpots2dadap.f:103, 343), each call paying the step-0
+// precomputation (boxfgt.f:472-703).  The drop-in entry points keep the plans
+// of the last few (tree, delta, eps, order, nd, precision) combinations.  The
+// key is a 64-bit hash of the tree arrays that define the lists and tables
+// (itree up to its colleague arrays, centers, boxsize) and of the scalar
+// arguments; the colleague arrays are left out because every call rewrites
+// them (boxfgt.f:516-528) and a hit writes back what a fresh plan would.
+struct CacheEntry {
+  uint64_t key = 0;
+  int device = 0;
+  std::vector<int> coll;  // itree's colleague arrays as the plan left them
+  bfgt_plan plan = nullptr;
+  uint64_t last = 0;
+};
+
+std::mutex g_cache_mu;
+std::vector<CacheEntry> g_cache;
+uint64_t g_cache_clock = 0, g_cache_hits = 0, g_cache_misses = 0;
+int g_default_precision = -1;  // -1: from BFGT_PRECISION at first use
+
+int cache_capacity() {
+  const char *e = std::getenv("BFGT_PLAN_CACHE");
+  if (!e || !*e) return 4;
+  return std::max(0, std::atoi(e));
+}
+
+int default_precision() {
+  if (g_default_precision < 0) {
+    const char *e = std::getenv("BFGT_PRECISION");
+    g_default_precision = (e && std::strcmp(e, "split") == 0) ? BFGT_PREC_SPLIT : BFGT_PREC_FP64;
+  }
+  return g_default_precision;
+}
+
+inline uint64_t mix(uint64_t h, uint64_t w) {
+  h ^= w + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+  h *= 0xBF58476D1CE4E5B9ull;
+  return h ^ (h >> 31);
+}
+uint64_t hash_block(uint64_t h, const unsigned char *c, size_t bytes) {
+  size_t i = 0;
+  for (; i + 8 <= bytes; i += 8) {
+    uint64_t w;
+    std::memcpy(&w, c + i, 8);
+    h = mix(h, w);
+  }
+  uint64_t w = 0;
+  std::memcpy(&w, c + i, bytes - i);
+  return mix(h, w ^ bytes);
+}
+// Blocks of 256 KB hashed on the host threads, then combined in block order
+// (the same value for any thread count).
+uint64_t hash_bytes(uint64_t h, const void *p, size_t bytes) {
+  constexpr size_t kBlock = 256 * 1024;
+  const unsigned char *c = static_cast<const unsigned char *>(p);
+  const long nb = (long)((bytes + kBlock - 1) / kBlock);
+  if (nb <= 1) return hash_block(h, c, bytes);
+  std::vector<uint64_t> part(nb);
+#pragma omp parallel for schedule(static)
+  for (long b = 0; b < nb; b++) {
+    const size_t o = (size_t)b * kBlock;
+    part[b] = hash_block(0x9E3779B97F4A7C15ull + (uint64_t)b, c + o, std::min(kBlock, bytes - o));
+  }
+  for (long b = 0; b < nb; b++) h = mix(h, part[b]);
+  return mix(h, bytes);
+}
+
+uint64_t plan_key(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
+                  int ltree, const int *itree, const int *iptr, const double *centers, const double *boxsize,
+                  int precision) {
+  uint64_t h = 0x243F6A8885A308D3ull;
+  const int ints[] = {nd, ipoly, iperiod, norder, nboxes, nlevels, ltree, precision};
+  h = hash_bytes(h, ints, sizeof(ints));
+  h = hash_bytes(h, &delta, sizeof(double));
+  h = hash_bytes(h, &eps, sizeof(double));
+  h = hash_bytes(h, iptr, 8 * sizeof(int));
+  h = hash_bytes(h, itree, sizeof(int) * (size_t)(iptr[5] - 1));  // laddr, ilevel, iparent, nchild, ichild
+  h = hash_bytes(h, centers, sizeof(double) * 2 * (size_t)nboxes);
+  return hash_bytes(h, boxsize, sizeof(double) * (size_t)(nlevels + 1));
+}
+
+// A plan for these arguments: from the cache (writing the colleague arrays
+// back into itree) or newly created (and cached).  *cached tells the caller
+// not to destroy it.  Called with g_cache_mu held when caching is on.
+int get_plan(bfgt_plan *out, bool *cached, double *precompute_s, int nd, double delta, double eps, int ipoly,
+             int iperiod, int norder, int nboxes, int nlevels, int ltree, int *itree, const int *iptr,
+             const double *centers, const double *boxsize, int precision) {
+  const double t0 = now_s();
+  *cached = false;
+  const int cap = cache_capacity();
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
+  const bool arrays_ok = itree && iptr && centers && boxsize && iptr[5] >= 1 && iptr[6] >= iptr[5] &&
+                         (long)iptr[6] - 1 + 9L * nboxes <= ltree;
+  uint64_t key = 0;
+  if (cap > 0 && arrays_ok) {
+    key = plan_key(nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree, iptr, centers, boxsize,
+                   precision);
+    for (CacheEntry &e : g_cache)
+      if (e.key == key && e.device == dev) {
+        std::memcpy(itree + iptr[5] - 1, e.coll.data(), sizeof(int) * e.coll.size());
+        e.last = ++g_cache_clock;
+        g_cache_hits++;
+        *out = e.plan;
+        *cached = true;
+        *precompute_s = now_s() - t0;
+        return BFGT_OK;
+      }
+  }
+  int rc = bfgt_plan_create(out, nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree, iptr, centers,
+                            boxsize, precision);
+  if (rc != BFGT_OK) return rc;
+  *precompute_s = now_s() - t0;
+  if (cap > 0 && arrays_ok) {
+    g_cache_misses++;
+    if ((int)g_cache.size() >= cap) {
+      auto victim = std::min_element(g_cache.begin(), g_cache.end(),
+                                     [](const CacheEntry &a, const CacheEntry &b) { return a.last < b.last; });
+      bfgt_plan_destroy(victim->plan);
+      g_cache.erase(victim);
+    }
+    CacheEntry e;
+    e.key = key;
+    e.device = dev;
+    e.coll.assign(itree + iptr[5] - 1, itree + iptr[6] - 1 + 9 * (size_t)nboxes);
+    e.plan = *out;
+    e.last = ++g_cache_clock;
+    g_cache.push_back(std::move(e));
+    *cached = true;
+  }
+  return BFGT_OK;
+}
+
 int boxfgt_impl(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
                 int ltree, int *itree, const int *iptr, const double *centers, const double *boxsize,
                 const double *fvals, int ifpgh, double *pot, double *grad, double *hess, double *timeinfo,
                 int precision, int ntarg = 0, const double *targs = nullptr, int ifpghtarg = 0,
                 double *pote = nullptr, double *grade = nullptr, double *hesse = nullptr) {
-  double t0 = now_s();
+  std::unique_lock<std::mutex> lk(g_cache_mu, std::defer_lock);
+  if (cache_capacity() > 0) lk.lock();  // cached plans are shared: one drop-in call at a time
   bfgt_plan plan = nullptr;
-  int rc = bfgt_plan_create(&plan, nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree, iptr,
-                            centers, boxsize, precision);
+  bool cached = false;
+  double t_pre = 0;
+  int rc = get_plan(&plan, &cached, &t_pre, nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree,
+                    iptr, centers, boxsize, precision);
   if (rc != BFGT_OK) return rc;
-  double t1 = now_s();
+  {
+    double drop[8];
+    bfgt::device_plan_stage_ms(plan->dp, drop);  // stage times of earlier calls on a cached plan
+  }
   // as boxfgt.f:207-276: when the targets ask for more derivatives than the
   // boxes, the transform computes them into zeroed internal arrays
   const int ifpgh2 = std::max(ifpgh, ifpghtarg);
@@ -511,7 +654,7 @@ int boxfgt_impl(int nd, double delta, double eps, int ipoly, int iperiod, int no
     hp = h2.data();
   }
   rc = bfgt_plan_execute_pgh_host(plan, ifpgh2, fvals, pot, gp, hp, nullptr);
-  double t2 = now_s();
+  const double t2 = now_s();
   if (rc == BFGT_OK && ifpghtarg > 0) rc = targets_host_on(plan->dp, ifpghtarg, ntarg, targs, pote, grade, hesse, nullptr);
   const double t_targ = now_s() - t2;
   if (rc == BFGT_OK) rc = bfgt_plan_check(plan);
@@ -519,7 +662,7 @@ int boxfgt_impl(int nd, double delta, double eps, int ipoly, int iperiod, int no
     double st[8];
     bfgt::device_plan_stage_ms(plan->dp, st);
     for (int i = 0; i < 20; i++) timeinfo[i] = 0;
-    timeinfo[0] = t1 - t0;           // step 0: precomputation
+    timeinfo[0] = t_pre;             // step 0: precomputation (near zero on a cached plan)
     timeinfo[1] = st[0] * 1e-3;      // steps 1+2: leaf -> cutoff expansions
     timeinfo[2] = st[1] * 1e-3;      // fixed-order partial-sum reduction
     timeinfo[3] = st[2] * 1e-3;      // step 3: cutoff translations
@@ -528,9 +671,11 @@ int boxfgt_impl(int nd, double delta, double eps, int ipoly, int iperiod, int no
     timeinfo[6] = st[4] * 1e-3;      // step 6: near field
     timeinfo[11] = ifpghtarg > 0 ? t_targ : 0;  // step 11: extra targets
   }
-  std::string keep = g_err;
-  bfgt_plan_destroy(plan);
-  g_err = keep;
+  if (!cached) {
+    std::string keep = g_err;
+    bfgt_plan_destroy(plan);
+    g_err = keep;
+  }
   return rc;
 }
 
@@ -578,9 +723,47 @@ void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *
     return;
   }
   double ti[20];
-  boxfgt_impl(*nd, *delta, *eps, *ipoly, *iperiod, *norder, *nboxes, *nlevels, *ltree, itree, iptr, centers, boxsize,
-              fvals, *ifpgh, pot, grad, hess, timeinfo ? timeinfo : ti, BFGT_PREC_FP64, *ntarg, targs, *ifpghtarg,
-              pote, grade, hesse);
+  int prec = BFGT_PREC_FP64;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    prec = default_precision();
+  }
+  int rc = boxfgt_impl(*nd, *delta, *eps, *ipoly, *iperiod, *norder, *nboxes, *nlevels, *ltree, itree, iptr, centers,
+                       boxsize, fvals, *ifpgh, pot, grad, hess, timeinfo ? timeinfo : ti, prec, *ntarg, targs,
+                       *ifpghtarg, pote, grade, hesse);
+  // split precision serves norder 8 and 16, npw <= 64 and eps >= 1e-11; other
+  // calls run in FP64, which meets every eps
+  if (rc == BFGT_ERR_CAPACITY && prec == BFGT_PREC_SPLIT)
+    boxfgt_impl(*nd, *delta, *eps, *ipoly, *iperiod, *norder, *nboxes, *nlevels, *ltree, itree, iptr, centers, boxsize,
+                fvals, *ifpgh, pot, grad, hess, timeinfo ? timeinfo : ti, BFGT_PREC_FP64, *ntarg, targs, *ifpghtarg,
+                pote, grade, hesse);
+}
+
+int bfgt_set_default_precision(int precision) {
+  g_err.clear();
+  if (precision != BFGT_PREC_FP64 && precision != BFGT_PREC_SPLIT) return fail(BFGT_ERR_ARG, "unknown precision mode");
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  g_default_precision = precision;
+  return BFGT_OK;
+}
+
+int bfgt_plan_cache_clear(void) {
+  g_err.clear();
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  for (CacheEntry &e : g_cache) bfgt_plan_destroy(e.plan);
+  g_cache.clear();
+  return BFGT_OK;
+}
+
+int bfgt_plan_cache_info(int64_t *out) {
+  g_err.clear();
+  if (!out) return fail(BFGT_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  out[0] = (int64_t)g_cache.size();
+  out[1] = (int64_t)cache_capacity();
+  out[2] = (int64_t)g_cache_hits;
+  out[3] = (int64_t)g_cache_misses;
+  return BFGT_OK;
 }
 
 int bfgt_host_plan_dump(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes,

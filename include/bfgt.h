@@ -45,7 +45,10 @@ extern "C" {
 #define BFGT_PREC_SPLIT 1       /* tensor-core split-FP16 slices, FP32 accum.,
                                    FP64 phases and FP64 cross-leaf accumulation */
 
-/* Replaces bfgt/boxfgt.f:5-286 (boxfgt).  Supported: ndim=2, ifpgh=1, 2, 3,
+/* Replaces bfgt/boxfgt.f:5-286 (boxfgt).  Runs in the precision set by
+   bfgt_set_default_precision (FP64 unless chosen otherwise), on a cached plan
+   when the tree and arguments repeat (bfgt_plan_cache_info).  Supported:
+   ndim=2, ifpgh=1, 2, 3,
    ifpghtarg=0..3, ifnewtree=0 (ifpgh=1, ifpghtarg=0 is what every solver in
    the reference uses, hpots/hpots2dadap.f:79-106).  pot (and
    grad(nd,2,npbox,nboxes), hess(nd,3,npbox,nboxes) as ifpgh asks) are
@@ -61,6 +64,26 @@ void boxfgt_(const int *nd, const int *ndim, const double *delta, const double *
              double *pot, double *grad, double *hess, const int *ifnewtree, const int *ntarg,
              const double *targs, const int *ifpghtarg, double *pote, double *grade, double *hesse,
              double *timeinfo);
+
+/* No counterpart in the reference.  Precision mode of boxfgt_ (which has no
+   precision argument): BFGT_PREC_FP64 (the default) or BFGT_PREC_SPLIT.  The
+   environment variable BFGT_PRECISION=split selects split before the first
+   call.  A call that split precision cannot serve (norder other than 8 and 16,
+   npw > 64, eps < 1e-11) runs in FP64. */
+int bfgt_set_default_precision(int precision);
+
+/* No counterpart in the reference.  boxfgt_ and bfgt_boxfgt keep the plans
+   (step-0 precomputation and device tables) of their last few argument sets,
+   4 by default or BFGT_PLAN_CACHE (0 turns the cache off).  A plan is found
+   again by a 64-bit hash of nd, delta, eps, ipoly, iperiod, norder, precision,
+   nboxes, nlevels, ltree, iptr, itree up to its colleague arrays, centers and
+   boxsize; on a hit the colleague arrays are written back as a fresh plan
+   would leave them and timeinfo(1) is the lookup time.  Calls into the cache
+   are serialised by a mutex.  bfgt_plan_cache_clear frees the cached plans;
+   bfgt_plan_cache_info gives out[0] entries, out[1] capacity, out[2] hits,
+   out[3] misses (out must hold 4). */
+int bfgt_plan_cache_clear(void);
+int bfgt_plan_cache_info(int64_t *out);
 
 /* Last error message of this thread ("" when the last call succeeded). */
 const char *bfgt_last_error(void);

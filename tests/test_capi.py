@@ -65,3 +65,14 @@ def test_boxfgt_rejects_unsupported_flags():
         hb.boxfgt(1, 2, 1e-3, 1e-9, 0, 1, 8, 64, t.nboxes, t.nlevels, t.ltree, t.itree.copy(), t.iptr, t.centers,
                   t.boxsize, t.fvals, 1, pot, None, None, 1, 0, None, 0, None, None, None, ti)
     assert not pot.any()
+
+
+def test_default_precision_and_plan_cache_api():
+    """The drop-in's precision selector and plan-cache queries need no device."""
+    hb.set_default_precision(hb.BFGT_PREC_SPLIT)
+    hb.set_default_precision(hb.BFGT_PREC_FP64)
+    with pytest.raises(hb.BfgtError):
+        hb.set_default_precision(7)
+    hb.plan_cache_clear()
+    info = hb.plan_cache_info()
+    assert info["entries"] == 0 and info["capacity"] >= 0

@@ -133,6 +133,65 @@ def _c4_tree():
     return hb.build_adaptive(g, norder=16, ipoly=0, iperiod=1, eps=1e-10, minlev=5, maxlev=9)
 
 
+def _c2_bench_tree():
+    """The benchmark's adaptive order-16 tree statistics at full size: 20
+    Gaussians (widths log-uniform in [1e-3, 1e-2], N(0,1) amplitudes), uniform
+    to level 8, refined to a 1e-10 Legendre tail, max level 12 (~65k leaves)."""
+    g = gauss_sum(2, 20, 1e-3, 1e-2, amp="normal", log_width=True)
+    return hb.build_adaptive(g, norder=16, ipoly=0, iperiod=1, eps=1e-10, minlev=8, maxlev=12)
+
+
+def _gradient_check(t, precision, tol, ndir=100):
+    """dJ/df through autograd (backward = the adjoint) vs central differences of
+    the FP64 transform, h = 1e-6, ndir random leaf directions drawn on the
+    device (seed 7)."""
+    import torch
+    from fgt_autograd import boxfgt, gauss_at_points, misfit
+
+    delta, eps = 1e-3, 1e-9
+    lv = t.leaves()
+    gpar = gauss_sum(3, 20, 1e-3, 1e-2, amp="normal", log_width=True)
+    gt = np.zeros((t.nboxes, t.npbox))
+    gt[lv] = gauss_at_points(t.grid_points(lv), gpar)
+    f0 = np.zeros((t.nboxes, t.npbox))
+    f0[lv] = t.fvals[lv]
+    dev = torch.device("cuda")
+    g = torch.from_numpy(gt.reshape(-1)).to(dev)
+    plan = hb.Plan(t, delta, eps, precision=precision)
+    f = torch.from_numpy(f0.reshape(-1)).to(dev).requires_grad_(True)
+    J = misfit(f, plan, g)
+    J.backward()
+    plan.check()
+    grad = f.grad.detach()
+    ref = hb.Plan(t, delta, eps, precision=hb.BFGT_PREC_FP64)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(7)
+    mask = torch.zeros(t.nboxes, t.npbox, dtype=torch.float64, device=dev)
+    mask[torch.from_numpy(lv).to(dev)] = 1.0
+    mask = mask.reshape(-1)
+    h = 1e-6
+    fd, an = [], []
+    with torch.no_grad():
+        for _ in range(ndir):
+            vt = torch.randn(mask.shape, generator=gen, dtype=torch.float64, device=dev) * mask
+            rp = boxfgt(f.detach() + h * vt, ref) - g
+            rm = boxfgt(f.detach() - h * vt, ref) - g
+            fd.append((0.5 * torch.sum((rp - rm) * (rp + rm))).item() / (2 * h))
+            an.append(torch.dot(grad, vt).item())
+    plan.close()
+    ref.close()
+    fd, an = np.array(fd), np.array(an)
+    err = np.linalg.norm(fd - an) / np.linalg.norm(fd)
+    assert err <= tol, err
+
+
+@pytest.mark.parametrize("precision,tol", [(hb.BFGT_PREC_FP64, 1e-7), (hb.BFGT_PREC_SPLIT, 1e-6)])
+def test_gradient_on_the_benchmark_tree(precision, tol):
+    """Configuration C4 at its size: the gradient check on the benchmark's
+    adaptive order-16 tree (65k leaves, 16.8 M leaf values), delta = 1e-3."""
+    _gradient_check(_c2_bench_tree(), precision, tol)
+
+
 @pytest.mark.parametrize("precision,tol", [(hb.BFGT_PREC_FP64, 1e-7), (hb.BFGT_PREC_SPLIT, 1e-6)])
 def test_gradient_matches_central_differences(precision, tol):
     """dJ/df through autograd (backward = the adjoint) vs central differences of

@@ -368,7 +368,8 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
             fix_digits(k < kN ? fcur[k < kN ? k : 0] * rinv : 0.0, S, v0);
             fix_digits(k + 1 < kN ? fcur[k + 1 < kN ? k + 1 : 0] * rinv : 0.0, S, v1);
 #pragma unroll
-            for (int c = 0; c < kMaxSlices; c++) p[c][q] = tc::bf162_bits(__floats2bfloat162_rn(v0[c], v1[c]));
+            for (int c = 0; c < kMaxSlices; c++)  // (exact BF16 values: their top 16 bits)
+              p[c][q] = __byte_perm(__float_as_uint(v0[c]), __float_as_uint(v1[c]), 0x7632);
           }
 #pragma unroll
           for (int c = 0; c < kMaxSlices; c++)
@@ -602,8 +603,9 @@ __device__ __forceinline__ void h_to_operand(unsigned char *sA, int r, const dou
 #pragma unroll
       for (int cc = 0; cc < kMaxSlices; cc++) {
         if (cc >= S) break;
-        *reinterpret_cast<__nv_bfloat16 *>(sA + cc * kRows * KE * 2 + ore) = __float2bfloat16_rn(vr[cc]);
-        *reinterpret_cast<__nv_bfloat16 *>(sA + cc * kRows * KE * 2 + oim) = __float2bfloat16_rn(vi[cc]);
+        // (exact BF16 values: their top 16 bits)
+        *reinterpret_cast<uint16_t *>(sA + cc * kRows * KE * 2 + ore) = (uint16_t)(__float_as_uint(vr[cc]) >> 16);
+        *reinterpret_cast<uint16_t *>(sA + cc * kRows * KE * 2 + oim) = (uint16_t)(__float_as_uint(vi[cc]) >> 16);
       }
     }
   } else {

@@ -119,16 +119,20 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
+// FP32 -> its leading BF16 part by truncation: the top 16 bits of the FP32
+// encoding (sign, exponent, 7 mantissa bits) are a BF16 number, and
+// x - hi(x) is exact in FP32.  Integer operations only (no conversion
+// instructions).
+__device__ __forceinline__ float bf16_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFF0000u); }
+
 // FP64 value -> three BF16 slices through FP32 (see split3_bf16x2)
 __device__ __forceinline__ void split3_bf16x1(double v, uint16_t &s0, uint16_t &s1, uint16_t &s2) {
   const float a = __double2float_rn(v);
-  const __nv_bfloat16 h = __float2bfloat16_rn(a);
-  const float r = a - __bfloat162float(h);
-  const __nv_bfloat16 m = __float2bfloat16_rn(r);
-  const __nv_bfloat16 l = __float2bfloat16_rn(r - __bfloat162float(m));
-  s0 = __bfloat16_as_ushort(h);
-  s1 = __bfloat16_as_ushort(m);
-  s2 = __bfloat16_as_ushort(l);
+  const float h = bf16_hi(a), r = a - h;
+  const float m = bf16_hi(r), l = r - m;
+  s0 = (uint16_t)(__float_as_uint(h) >> 16);
+  s1 = (uint16_t)(__float_as_uint(m) >> 16);
+  s2 = (uint16_t)(__float_as_uint(l) >> 16);
 }
 
 // 16-byte global -> shared copy that bypasses registers (completion: cp_async_wait_all)
@@ -141,22 +145,24 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 __device__ __forceinline__ uint32_t bf162_bits(__nv_bfloat162 h) { return *reinterpret_cast<uint32_t *>(&h); }
 
 // Two FP64 values -> three packed BF16x2 slices.  The values are rounded to
-// FP32 first (relative error 2^-24); the FP32 value is then split exactly:
-// each difference below is exact in FP32 (the operands agree in their leading
-// bits), and the last remainder has at most 6 significant bits, so
-// s0 + s1 + s2 reproduces the FP32 value.  Element v0 goes to the low half
+// FP32 first (relative error 2^-24); the FP32 value is then cut exactly by
+// truncation: s0 = the top 8 significant bits, the remainder (exact in FP32)
+// has at most 16, s1 = its top 8, and what is left (exact) has at most 8
+// significant bits, so it is a BF16 number s2 and s0 + s1 + s2 reproduces the
+// FP32 value (FP32 values below the normal range aside, which lose their low
+// bits: an absolute error below 2^-133).  One conversion per value; the cuts
+// and the packing are integer operations.  Element v0 goes to the low half
 // (the lower address of a packed pair).
 __device__ __forceinline__ void split3_bf16x2(double v0, double v1, uint32_t &p0, uint32_t &p1, uint32_t &p2) {
   const float a0 = __double2float_rn(v0), a1 = __double2float_rn(v1);
-  const __nv_bfloat162 h = __floats2bfloat162_rn(a0, a1);
-  const float2 hf = __bfloat1622float2(h);
-  const float r0 = a0 - hf.x, r1 = a1 - hf.y;
-  const __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
-  const float2 mf = __bfloat1622float2(m);
-  const __nv_bfloat162 l = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
-  p0 = bf162_bits(h);
-  p1 = bf162_bits(m);
-  p2 = bf162_bits(l);
+  const float h0 = bf16_hi(a0), h1 = bf16_hi(a1);
+  const float r0 = a0 - h0, r1 = a1 - h1;
+  const float m0 = bf16_hi(r0), m1 = bf16_hi(r1);
+  const float l0 = r0 - m0, l1 = r1 - m1;
+  // bytes 2, 3 of the first word, then bytes 2, 3 (6, 7) of the second
+  p0 = __byte_perm(__float_as_uint(h0), __float_as_uint(h1), 0x7632);
+  p1 = __byte_perm(__float_as_uint(m0), __float_as_uint(m1), 0x7632);
+  p2 = __byte_perm(__float_as_uint(l0), __float_as_uint(l1), 0x7632);
 }
 
 }  // namespace tc

@@ -165,3 +165,17 @@ def test_batch_adjoint_matches_single_plan_adjoints(trees):
     batch.close()
     for pl in plans:
         pl.close()
+
+
+def test_batch_refuses_a_repeated_plan(trees):
+    """A plan owns its expansion scratch and arrival counters, so one plan
+    listed twice in a batch would mix two transforms' partial sums:
+    bfgt_batch_create refuses it (BFGT_ERR_ARG) and creates nothing."""
+    a = hb.Plan(trees["ad_leg_per"], 1e-4, 1e-6, precision=hb.BFGT_PREC_SPLIT)
+    b = hb.Plan(trees["uni3_leg_per"], 1e-3, 1e-9)
+    with pytest.raises(hb.BfgtError, match="repeats plan"):
+        hb.Batch([a, b, a])
+    batch = hb.Batch([a, b])  # the same plans once each are fine
+    batch.close()
+    a.close()
+    b.close()

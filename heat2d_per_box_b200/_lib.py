@@ -63,6 +63,8 @@ def lib():
     L.bfgt_plan_cache_clear.argtypes = []
     L.bfgt_plan_cache_info.restype = C.c_int
     L.bfgt_plan_cache_info.argtypes = [C.c_void_p]
+    L.bfgt_boxfgt_last_bytes.restype = C.c_int
+    L.bfgt_boxfgt_last_bytes.argtypes = [C.c_void_p]
     L.bfgt_plan_create.restype = C.c_int
     L.bfgt_plan_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
                                    C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, C.c_int]

@@ -68,6 +68,15 @@ def plan_cache_info():
     return {"entries": int(out[0]), "capacity": int(out[1]), "hits": int(out[2]), "misses": int(out[3])}
 
 
+def last_call_bytes():
+    """Host-to-device and device-to-host bytes of the last boxfgt_ call (pot
+    runs that were all zero on the host are cleared on the device, not
+    uploaded)."""
+    out = np.zeros(2, np.float64)
+    _lib.check(_lib.lib().bfgt_boxfgt_last_bytes(out.ctypes.data))
+    return {"h2d": int(out[0]), "d2h": int(out[1])}
+
+
 def plan_cache_clear():
     """Frees the plans the drop-in entry points keep."""
     _lib.check(_lib.lib().bfgt_plan_cache_clear())
@@ -176,8 +185,11 @@ class Plan:
         _lib.check(self._L.bfgt_plan_set_wait_limit(self._h, 0xFFFFFFFF if polls is None else int(polls)))
 
     def autotune(self, stream=None):
-        """Times the FP64 kernels' tile shapes on this plan and keeps the fastest
-        (see bfgt_plan_autotune); returns (form ms, eval ms, shapes timed)."""
+        """Times the plan's compiled kernel shapes on its own work and keeps the
+        fastest (see bfgt_plan_autotune): FP64 tile shapes, or the split
+        kernels' Y staging, x tiles and eval step groups.  Tune a plan before
+        putting it in a Batch (a batch keeps the shapes its plans had when it
+        was created).  Returns (form ms, eval ms, shapes timed)."""
         s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         rep = np.zeros(4)
         _lib.check(self._L.bfgt_plan_autotune(self._h, s, rep))
@@ -200,7 +212,8 @@ class Plan:
         out = np.zeros(16, np.int32)
         _lib.check(self._L.bfgt_plan_info(self._h, out))
         keys = ["npwlevel", "npw", "nlevstart", "nlevend", "regime", "nleafbox", "npwleaves", "nnear_targets",
-                "nnear_pairs", "mnlist1", "iperiod_int", "nchunks", "launches", "form_tile", "eval_tile"]
+                "nnear_pairs", "mnlist1", "iperiod_int", "nchunks", "launches", "form_tile", "eval_tile",
+                "split_shape"]
         return {k: int(out[i]) for i, k in enumerate(keys)}
 
     def work(self):
@@ -269,14 +282,6 @@ class Batch:
         _lib.check(self._L.bfgt_batch_info(self._h, out))
         keys = ["plans", "launches", "form_items", "eval_items", "translate_blocks", "near_blocks"]
         return {k: int(out[i]) for i, k in enumerate(keys)}
-
-    def autotune(self, stream=None):
-        """Times the FP64 kernels' tile shapes on this plan and keeps the fastest
-        (see bfgt_plan_autotune); returns (form ms, eval ms, shapes timed)."""
-        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
-        rep = np.zeros(4)
-        _lib.check(self._L.bfgt_plan_autotune(self._h, s, rep))
-        return float(rep[0]), float(rep[1]), int(rep[2] + rep[3])
 
     def check(self):
         _lib.check(self._L.bfgt_batch_check(self._h))

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -131,9 +132,33 @@ int bfgt_plan_execute(bfgt_plan plan, const double *d_fvals, double *d_pot, void
 
 namespace {
 
+// True when the n doubles at p are all +0.0 (every bit clear), tested in
+// blocks on the host threads.  Only +0.0 counts: -0.0 + x and +0.0 + x differ
+// when x is -0.0, so a run holding -0.0 is uploaded like any other.
+bool all_zero_bits(const double *p, size_t n) {
+  constexpr size_t kBlock = 1 << 16;
+  const long nb = (long)((n + kBlock - 1) / kBlock);
+  std::atomic<bool> nonzero{false};
+#pragma omp parallel for schedule(dynamic, 4) if (nb > 4)
+  for (long b = 0; b < nb; b++) {
+    if (nonzero.load(std::memory_order_relaxed)) continue;
+    const uint64_t *w = reinterpret_cast<const uint64_t *>(p) + (size_t)b * kBlock;
+    const size_t m = std::min(kBlock, n - (size_t)b * kBlock);
+    uint64_t acc = 0;
+    for (size_t i = 0; i < m; i++) acc |= w[i];
+    if (acc) nonzero.store(true, std::memory_order_relaxed);
+  }
+  return !nonzero.load();
+}
+
 // Host-array form of one transform on dp: uploads the leaf runs of the input
 // and of the accumulators, runs, and copies the accumulators' leaf runs back.
 // With ifpgh >= 2 grad(nd,2,..) and, for 3, hess(nd,3,..) are accumulated too.
+// The reference's callers zero pot before every call (hpots2dadap.f:97-101,
+// 321-325): an accumulator run that is all +0.0 on the host is cleared on the
+// device instead of uploaded, which gives the same sums bit for bit.  The
+// zero test runs on the host while the input's upload is in flight (pinned
+// input; a pageable one is staged by the copy call first).
 int execute_host_on(bfgt_plan plan, bfgt::DevicePlan &dp, const double *in, double *acc, cudaStream_t s,
                     int ifpgh = 1, double *grad = nullptr, double *hess = nullptr) {
   const size_t elems = (size_t)dp.nd * dp.n * dp.n * dp.nboxes;
@@ -170,24 +195,41 @@ int execute_host_on(bfgt_plan plan, bfgt::DevicePlan &dp, const double *in, doub
   std::vector<Acc> accs = {{acc, dp.d_stage_p, 1}};
   if (dg) accs.push_back({grad, dg, 2});
   if (dh) accs.push_back({hess, dh, 3});
+  double up = 0;
   for (const auto &r : plan->leaf_runs) {
     const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
     if (cudaMemcpyAsync(dp.d_stage_f + o, in + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess)
       return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
-    for (const Acc &a : accs)
-      if (cudaMemcpyAsync(a.d + a.k * o, a.h + a.k * o, a.k * c, cudaMemcpyHostToDevice, s) != cudaSuccess)
-        return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
+    up += (double)c;
   }
+  for (const auto &r : plan->leaf_runs) {
+    const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
+    for (const Acc &a : accs) {
+      if (all_zero_bits(a.h + a.k * o, a.k * c / sizeof(double))) {
+        if (cudaMemsetAsync(a.d + a.k * o, 0, a.k * c, s) != cudaSuccess)
+          return fail(BFGT_ERR_CUDA, "device clear failed");
+      } else {
+        if (cudaMemcpyAsync(a.d + a.k * o, a.h + a.k * o, a.k * c, cudaMemcpyHostToDevice, s) != cudaSuccess)
+          return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
+        up += (double)(a.k * c);
+      }
+    }
+  }
+  plan->last_h2d_bytes = up;
   std::string msg;
   int rc = ifpgh >= 2 ? bfgt::device_plan_execute_pgh(dp, ifpgh, dp.d_stage_f, dp.d_stage_p, dg, dh, s, msg)
                       : bfgt::device_plan_execute(dp, dp.d_stage_f, dp.d_stage_p, s, msg);
   if (rc != BFGT_OK) return fail(rc, msg);
+  double down = 0;
   for (const auto &r : plan->leaf_runs) {
     const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
-    for (const Acc &a : accs)
+    for (const Acc &a : accs) {
       if (cudaMemcpyAsync(a.h + a.k * o, a.d + a.k * o, a.k * c, cudaMemcpyDeviceToHost, s) != cudaSuccess)
         return fail(BFGT_ERR_CUDA, "device-to-host copy failed");
+      down += (double)(a.k * c);
+    }
   }
+  plan->last_d2h_bytes = down;
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(BFGT_ERR_CUDA, std::string("transform failed: ") + cudaGetErrorString(cudaGetLastError()));
   return BFGT_OK;
 }
@@ -418,6 +460,10 @@ int bfgt_plan_info(bfgt_plan plan, int *out) {
   out[13] = f64 ? 100 * plan->dp.form_tile[0] + 10 * plan->dp.form_tile[1] + plan->dp.form_tile[2] : 0;
   out[14] = f64 ? 100 * plan->dp.eval_tile[0] + 10 * plan->dp.eval_tile[1] + plan->dp.eval_tile[2] : 0;
   out[12] = (!plan->dp.direct_only && plan->dp.nchunks > 0 ? 3 : 0) + (plan->dp.nnf > 0 ? 1 : 0);
+  // split kernels' shapes in use (100 eval step group + 10 x tiles per form
+  // thread + 1 if the form kernel stages Y as float2), 0 for FP64 plans
+  const bfgt::SplitPlan &sp = plan->dp.split;
+  out[15] = f64 ? 0 : 100 * sp.ebatch + 10 * sp.nt + (sp.yfloat ? 1 : 0);
   return BFGT_OK;
 }
 
@@ -442,6 +488,7 @@ int bfgt_plan_work(bfgt_plan plan, double *out) {
   for (const auto &r : plan->leaf_runs) run_bytes += 8.0 * plan->dp.nd * plan->dp.n * plan->dp.n * (r.second - r.first);
   out[13] = 2 * run_bytes;  // bfgt_plan_execute_host: fvals and pot up
   out[14] = run_bytes;      // and pot down
+  out[15] = plan->last_h2d_bytes;  // bytes the last host execute uploaded
   return BFGT_OK;
 }
 
@@ -492,13 +539,21 @@ namespace {
 // unchanged tree (hpots/hpots2dadap.f:103, 343), each call paying the step-0
 // precomputation (boxfgt.f:472-703).  The drop-in entry points keep the plans
 // of the last few (tree, delta, eps, order, nd, precision) combinations.  The
-// key is a 64-bit hash of the tree arrays that define the lists and tables
-// (itree up to its colleague arrays, centers, boxsize) and of the scalar
-// arguments; the colleague arrays are left out because every call rewrites
-// them (boxfgt.f:516-528) and a hit writes back what a fresh plan would.
-struct CacheEntry {
-  uint64_t key = 0;
+// key is the scalar arguments and a copy of the tree arrays that define the
+// lists and tables (itree up to its colleague arrays, iptr, centers,
+// boxsize), compared exactly; the colleague arrays are left out because every
+// call rewrites them (boxfgt.f:516-528) and a hit writes back what a fresh
+// plan would.
+struct CacheKey {
+  int ints[8] = {0};  // nd, ipoly, iperiod, norder, nboxes, nlevels, ltree, precision
+  double delta = 0, eps = 0;
   int device = 0;
+  std::vector<int> iptr, itree;
+  std::vector<double> centers, boxsize;
+};
+
+struct CacheEntry {
+  CacheKey key;
   std::vector<int> coll;  // itree's colleague arrays as the plan left them
   bfgt_plan plan = nullptr;
   uint64_t last = 0;
@@ -507,6 +562,7 @@ struct CacheEntry {
 std::mutex g_cache_mu;
 std::vector<CacheEntry> g_cache;
 uint64_t g_cache_clock = 0, g_cache_hits = 0, g_cache_misses = 0;
+double g_last_bytes[2] = {0, 0};  // host<->device bytes of the last drop-in call
 int g_default_precision = -1;  // -1: from BFGT_PRECISION at first use
 
 int cache_capacity() {
@@ -523,51 +579,54 @@ int default_precision() {
   return g_default_precision;
 }
 
-inline uint64_t mix(uint64_t h, uint64_t w) {
-  h ^= w + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
-  h *= 0xBF58476D1CE4E5B9ull;
-  return h ^ (h >> 31);
-}
-uint64_t hash_block(uint64_t h, const unsigned char *c, size_t bytes) {
-  size_t i = 0;
-  for (; i + 8 <= bytes; i += 8) {
-    uint64_t w;
-    std::memcpy(&w, c + i, 8);
-    h = mix(h, w);
-  }
-  uint64_t w = 0;
-  std::memcpy(&w, c + i, bytes - i);
-  return mix(h, w ^ bytes);
-}
-// Blocks of 256 KB hashed on the host threads, then combined in block order
-// (the same value for any thread count).
-uint64_t hash_bytes(uint64_t h, const void *p, size_t bytes) {
+// Byte-wise equality of two arrays, compared in 256 KB blocks on the host
+// threads (the tree arrays of a large tree are several MB).
+bool same_bytes(const void *a, const void *b, size_t bytes) {
   constexpr size_t kBlock = 256 * 1024;
-  const unsigned char *c = static_cast<const unsigned char *>(p);
   const long nb = (long)((bytes + kBlock - 1) / kBlock);
-  if (nb <= 1) return hash_block(h, c, bytes);
-  std::vector<uint64_t> part(nb);
+  if (nb <= 1) return std::memcmp(a, b, bytes) == 0;
+  const unsigned char *x = static_cast<const unsigned char *>(a), *y = static_cast<const unsigned char *>(b);
+  std::atomic<bool> differ{false};
 #pragma omp parallel for schedule(static)
-  for (long b = 0; b < nb; b++) {
-    const size_t o = (size_t)b * kBlock;
-    part[b] = hash_block(0x9E3779B97F4A7C15ull + (uint64_t)b, c + o, std::min(kBlock, bytes - o));
+  for (long k = 0; k < nb; k++) {
+    if (differ.load(std::memory_order_relaxed)) continue;
+    const size_t o = (size_t)k * kBlock;
+    if (std::memcmp(x + o, y + o, std::min(kBlock, bytes - o)) != 0) differ.store(true, std::memory_order_relaxed);
   }
-  for (long b = 0; b < nb; b++) h = mix(h, part[b]);
-  return mix(h, bytes);
+  return !differ.load();
 }
 
-uint64_t plan_key(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
+template <class T>
+bool same_array(const std::vector<T> &v, const T *p, size_t n) {
+  return v.size() == n && same_bytes(v.data(), p, n * sizeof(T));
+}
+
+CacheKey make_key(int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes, int nlevels,
                   int ltree, const int *itree, const int *iptr, const double *centers, const double *boxsize,
-                  int precision) {
-  uint64_t h = 0x243F6A8885A308D3ull;
-  const int ints[] = {nd, ipoly, iperiod, norder, nboxes, nlevels, ltree, precision};
-  h = hash_bytes(h, ints, sizeof(ints));
-  h = hash_bytes(h, &delta, sizeof(double));
-  h = hash_bytes(h, &eps, sizeof(double));
-  h = hash_bytes(h, iptr, 8 * sizeof(int));
-  h = hash_bytes(h, itree, sizeof(int) * (size_t)(iptr[5] - 1));  // laddr, ilevel, iparent, nchild, ichild
-  h = hash_bytes(h, centers, sizeof(double) * 2 * (size_t)nboxes);
-  return hash_bytes(h, boxsize, sizeof(double) * (size_t)(nlevels + 1));
+                  int precision, int device) {
+  CacheKey k;
+  const int ints[8] = {nd, ipoly, iperiod, norder, nboxes, nlevels, ltree, precision};
+  std::memcpy(k.ints, ints, sizeof(ints));
+  k.delta = delta;
+  k.eps = eps;
+  k.device = device;
+  k.iptr.assign(iptr, iptr + 8);
+  k.itree.assign(itree, itree + (iptr[5] - 1));  // laddr, ilevel, iparent, nchild, ichild
+  k.centers.assign(centers, centers + 2 * (size_t)nboxes);
+  k.boxsize.assign(boxsize, boxsize + nlevels + 1);
+  return k;
+}
+
+// The cheap scalar comparison first, then the arrays.
+bool key_matches(const CacheKey &k, int nd, double delta, double eps, int ipoly, int iperiod, int norder, int nboxes,
+                 int nlevels, int ltree, const int *itree, const int *iptr, const double *centers,
+                 const double *boxsize, int precision, int device) {
+  const int ints[8] = {nd, ipoly, iperiod, norder, nboxes, nlevels, ltree, precision};
+  if (std::memcmp(k.ints, ints, sizeof(ints)) != 0 || device != k.device) return false;
+  if (std::memcmp(&k.delta, &delta, sizeof(double)) != 0 || std::memcmp(&k.eps, &eps, sizeof(double)) != 0)
+    return false;
+  return same_array(k.iptr, iptr, 8) && same_array(k.boxsize, boxsize, (size_t)nlevels + 1) &&
+         same_array(k.itree, itree, (size_t)(iptr[5] - 1)) && same_array(k.centers, centers, 2 * (size_t)nboxes);
 }
 
 // A plan for these arguments: from the cache (writing the colleague arrays
@@ -583,12 +642,10 @@ int get_plan(bfgt_plan *out, bool *cached, double *precompute_s, int nd, double 
   if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
   const bool arrays_ok = itree && iptr && centers && boxsize && iptr[5] >= 1 && iptr[6] >= iptr[5] &&
                          (long)iptr[6] - 1 + 9L * nboxes <= ltree;
-  uint64_t key = 0;
   if (cap > 0 && arrays_ok) {
-    key = plan_key(nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree, iptr, centers, boxsize,
-                   precision);
     for (CacheEntry &e : g_cache)
-      if (e.key == key && e.device == dev) {
+      if (key_matches(e.key, nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree, iptr, centers,
+                      boxsize, precision, dev)) {
         std::memcpy(itree + iptr[5] - 1, e.coll.data(), sizeof(int) * e.coll.size());
         e.last = ++g_cache_clock;
         g_cache_hits++;
@@ -611,8 +668,8 @@ int get_plan(bfgt_plan *out, bool *cached, double *precompute_s, int nd, double 
       g_cache.erase(victim);
     }
     CacheEntry e;
-    e.key = key;
-    e.device = dev;
+    e.key = make_key(nd, delta, eps, ipoly, iperiod, norder, nboxes, nlevels, ltree, itree, iptr, centers, boxsize,
+                     precision, dev);
     e.coll.assign(itree + iptr[5] - 1, itree + iptr[6] - 1 + 9 * (size_t)nboxes);
     e.plan = *out;
     e.last = ++g_cache_clock;
@@ -654,6 +711,12 @@ int boxfgt_impl(int nd, double delta, double eps, int ipoly, int iperiod, int no
     hp = h2.data();
   }
   rc = bfgt_plan_execute_pgh_host(plan, ifpgh2, fvals, pot, gp, hp, nullptr);
+  {
+    std::unique_lock<std::mutex> lb(g_cache_mu, std::defer_lock);
+    if (!lk.owns_lock()) lb.lock();
+    g_last_bytes[0] = plan->last_h2d_bytes;
+    g_last_bytes[1] = plan->last_d2h_bytes;
+  }
   const double t2 = now_s();
   if (rc == BFGT_OK && ifpghtarg > 0) rc = targets_host_on(plan->dp, ifpghtarg, ntarg, targs, pote, grade, hesse, nullptr);
   const double t_targ = now_s() - t2;
@@ -752,6 +815,15 @@ int bfgt_plan_cache_clear(void) {
   std::lock_guard<std::mutex> lk(g_cache_mu);
   for (CacheEntry &e : g_cache) bfgt_plan_destroy(e.plan);
   g_cache.clear();
+  return BFGT_OK;
+}
+
+int bfgt_boxfgt_last_bytes(double *out) {
+  g_err.clear();
+  if (!out) return fail(BFGT_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  out[0] = g_last_bytes[0];
+  out[1] = g_last_bytes[1];
   return BFGT_OK;
 }
 

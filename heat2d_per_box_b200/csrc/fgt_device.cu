@@ -684,7 +684,8 @@ void tuned_tiles(int n, int npw, int nd, TileChoice &form, TileChoice &eval) {
 
 int device_plan_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::string &msg) {
   for (int i = 0; i < 4; i++) report[i] = 0;
-  if (dp.precision == BFGT_PREC_SPLIT || dp.direct_only || dp.nchunks == 0) return BFGT_OK;  // no tile choice to make
+  if (dp.precision == BFGT_PREC_SPLIT) return split_autotune(dp, s, report, msg);
+  if (dp.direct_only || dp.nchunks == 0) return BFGT_OK;  // no tile choice to make
   const size_t elems = (size_t)dp.nd * dp.n * dp.n * dp.nboxes;
   double *f = nullptr, *p = nullptr;
   if (alloc_bytes((void **)&f, sizeof(double) * elems, msg) != BFGT_OK) return BFGT_ERR_OOM;

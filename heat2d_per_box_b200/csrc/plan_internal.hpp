@@ -16,6 +16,9 @@ struct bfgt_plan_s {
   // merged, so a range may include some non-leaf boxes, which the transform
   // neither reads nor writes)
   std::vector<std::pair<int, int>> leaf_runs;
+  // bytes the last host-array execute copied host to device (accumulator runs
+  // that were all zero are cleared on the device instead)
+  double last_h2d_bytes = 0, last_d2h_bytes = 0;
   // the transposed transform (bfgt_plan_execute_adjoint), built on first use
   std::unique_ptr<bfgt::HostPlan> adj_hp;
   std::unique_ptr<bfgt::DevicePlan> adj_dp;

@@ -102,6 +102,44 @@ inline cplx cmulh(cplx a, cplx b) { return cplx{a.re * b.re - a.im * b.im, a.re 
 
 }  // namespace
 
+namespace {
+
+// Dynamic shared memory of the form kernel: the double-buffered A/B operand
+// slices, or Y (as float2 or double2) where that is larger, and T of the level.
+size_t form_smem(const SplitPlan &sp, int n, int npw, int hh, bool yfloat) {
+  const int abytes = sp.S * kRows * sp.KA * 2, bbytes = sp.S * sp.NP * sp.KA * 2;
+  const int ybytes_d = kRows * (hh | 1) * 16;
+  const int ybytes = yfloat ? ybytes_d / 2 : ybytes_d;
+  const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 127) / 128) * 128;
+  size_t sm = 128 + ubytes + sizeof(double2) * (size_t)n * npw;
+  if (sp.fixed) sm = std::max(sm, kFixFormSmemMin);
+  return sm;
+}
+
+// The eval kernel's shared memory without L: operands for step groups of eb,
+// E of the level and the chunk's column phases.
+size_t eval_base_smem(const SplitPlan &sp, int n, int npw, int eb) {
+  const int eab = sp.S * kRows * sp.KE * 2;
+  const int ebb = sp.S * (16 * eb) * sp.KE * 2;
+  return 128 + ((eab + 127) / 128) * 128 + ((ebb + 127) / 128) * 128 +
+         sizeof(double2) * ((size_t)npw * n + (size_t)sp.cpc * npw);
+}
+
+// Step groups of eb and as many L slots as keep two CTAs per SM (up to the
+// densities a pass can pack: cpc, and 3 nd for the gradient and Hessian
+// views), at least one.
+void set_eval_shape(SplitPlan &sp, int n, int npw, int hh, int nd, int eb) {
+  const size_t lbytes = sizeof(double2) * (size_t)npw * hh;
+  const size_t ebase = eval_base_smem(sp, n, npw, eb);
+  const int lcap = std::min(sp.cpc, 3 * nd);
+  sp.ebatch = eb;
+  sp.lslots = 1;
+  while (sp.lslots < lcap && ebase + (sp.lslots + 1) * lbytes <= (size_t)kEvalSmemTwoPerSm) sp.lslots++;
+  sp.smem_eval = ebase + sp.lslots * lbytes;
+}
+
+}  // namespace
+
 int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   const int n = hp.norder, npw = hp.npw, hh = hp.hh, nl = hp.nlevels, ls = hp.nlevstart;
   if (n != 8 && n != 16) {
@@ -381,39 +419,23 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     chk(build_reduce_groups(dp, cut_of_chunk, msg, arrivals));
   }
   dp.nchunks = (int)chunks.size();
-  // shared memory
+  // shared memory.  Y as float2 when, as double2, it would be the largest
+  // user of the form kernel's area (unpacked plans with floating slices; the
+  // packed kernel and fixed-point slices keep double2).  Eval: groups of ebmax
+  // steps (8 floating, 4 fixed-point: three accumulators), or of half that if
+  // only that keeps two CTAs per SM with one L slot.
   {
     const int abytes = S * kRows * sp.KA * 2, bbytes = S * sp.NP * sp.KA * 2;
-    // Y as float2 when, as double2, it would be the largest user of the area
-    // (unpacked plans with floating slices; the packed kernel and fixed-point
-    // slices keep double2)
     const int ybytes_d = kRows * (hh | 1) * 16;
     sp.yfloat = !sp.fixed && hp.nd == 1 && ybytes_d > 2 * (abytes + bbytes);
-    const int ybytes = sp.yfloat ? ybytes_d / 2 : ybytes_d;
-    const int ubytes = ((std::max(2 * (abytes + bbytes), ybytes) + 127) / 128) * 128;
-    sp.smem_form = 128 + ubytes + sizeof(double2) * (size_t)n * npw;
-    if (sp.fixed) sp.smem_form = std::max(sp.smem_form, kFixFormSmemMin);
-    // eval: operands, E, the chunk's phases and lslots densities' L.  Groups
-    // of ebmax steps (8 floating, 4 fixed-point: three accumulators), or of
-    // half that if only that keeps two CTAs per SM with one L slot; then as
-    // many L slots as keep two CTAs per SM (up to the densities a pass can
-    // pack: cpc, and 3 nd for the gradient and Hessian views), at least one.
+    sp.smem_form = form_smem(sp, n, npw, hh, sp.yfloat);
     const size_t lbytes = sizeof(double2) * (size_t)npw * hh;
-    const int eab = S * kRows * sp.KE * 2;
-    auto eval_base = [&](int eb) {
-      const int ebb = S * (16 * eb) * sp.KE * 2;
-      return 128 + ((eab + 127) / 128) * 128 + ((ebb + 127) / 128) * 128 +
-             sizeof(double2) * ((size_t)npw * n + (size_t)sp.cpc * npw);
-    };
     const int ebmax = sp.fixed ? kEvalBatchFix : kEvalBatchMax;
-    sp.ebatch = ebmax;
-    if (eval_base(ebmax) + lbytes > (size_t)kEvalSmemTwoPerSm && eval_base(ebmax / 2) + lbytes <= (size_t)kEvalSmemTwoPerSm)
-      sp.ebatch = ebmax / 2;
-    const size_t ebase = eval_base(sp.ebatch);
-    const int lcap = std::min(sp.cpc, 3 * hp.nd);
-    sp.lslots = 1;
-    while (sp.lslots < lcap && ebase + (sp.lslots + 1) * lbytes <= (size_t)kEvalSmemTwoPerSm) sp.lslots++;
-    sp.smem_eval = ebase + sp.lslots * lbytes;
+    int eb = ebmax;
+    if (eval_base_smem(sp, n, npw, ebmax) + lbytes > (size_t)kEvalSmemTwoPerSm &&
+        eval_base_smem(sp, n, npw, ebmax / 2) + lbytes <= (size_t)kEvalSmemTwoPerSm)
+      eb = ebmax / 2;
+    set_eval_shape(sp, n, npw, hh, hp.nd, eb);
   }
   // x-contraction tiles per form thread (npw <= 64: at most 256 tiles)
   sp.nt = ((((npw + 1) / 2) * ((hh + 3) / 4)) + kThreads - 1) / kThreads;
@@ -497,6 +519,99 @@ void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
 void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
   EvalTcLaunch lp{eval_args(dp, 0), nullptr, nullptr, d_pot};
   launch_eval_any(eval_variant(dp), split_ctas(dp), dp.split.smem_eval, s, lp);
+}
+
+int split_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::string &msg) {
+  for (int i = 0; i < 4; i++) report[i] = 0;
+  SplitPlan &sp = dp.split;
+  if (dp.precision != BFGT_PREC_SPLIT || dp.direct_only || sp.nchunks == 0) return BFGT_OK;
+  const size_t elems = (size_t)dp.nd * dp.n * dp.n * dp.nboxes;
+  double *f = nullptr, *p = nullptr;
+  if (cudaMalloc(&f, sizeof(double) * elems) != cudaSuccess || cudaMalloc(&p, sizeof(double) * elems) != cudaSuccess) {
+    cudaGetLastError();
+    if (f) cudaFree(f);
+    msg = "cudaMalloc failed (autotuner scratch)";
+    return BFGT_ERR_OOM;
+  }
+  cudaMemsetAsync(f, 0, sizeof(double) * elems, s);
+  cudaMemsetAsync(p, 0, sizeof(double) * elems, s);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto time_ms = [&](auto &&launch) {
+    launch();  // warm-up
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; r++) launch();
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms / 3.0;
+  };
+  // form: Y staged as float2 or double2 (unpacked floating-slice plans) and
+  // 1 or 2 x-contraction tiles per thread (unpacked plans; the minimum count
+  // is the only choice when it is 2)
+  struct FormShape {
+    bool yf;
+    int nt;
+  };
+  std::vector<FormShape> fc;
+  const bool packed = dp.nd > 1;
+  const int nt_min = sp.nt;
+  for (int yf = 0; yf < 2; yf++)
+    for (int nt = nt_min; nt <= 2; nt++) {
+      if ((yf && (sp.fixed || packed)) || (packed && nt != nt_min)) continue;
+      if (form_smem(sp, dp.n, dp.npw, dp.hh, yf != 0) > (size_t)kMaxDynSmem) continue;
+      fc.push_back(FormShape{yf != 0, nt});
+    }
+  const FormShape f0{sp.yfloat, sp.nt};
+  FormShape bf = f0;
+  double tf = 1e30;
+  for (const FormShape &c : fc) {
+    sp.yfloat = c.yf;
+    sp.nt = c.nt;
+    sp.smem_form = form_smem(sp, dp.n, dp.npw, dp.hh, c.yf);
+    const double ms = time_ms([&] { split_form(dp, f, s); });
+    if (ms < tf) tf = ms, bf = c;
+  }
+  sp.yfloat = bf.yf;
+  sp.nt = bf.nt;
+  sp.smem_form = form_smem(sp, dp.n, dp.npw, dp.hh, bf.yf);
+  // eval: step groups of 8, 4 or 2 (up to the slices' maximum), each with the
+  // L slots that keep two CTAs per SM
+  const int ebmax = sp.fixed ? kEvalBatchFix : kEvalBatchMax;
+  std::vector<int> ec;
+  for (int eb = ebmax; eb >= 2; eb /= 2) {
+    SplitPlan t = sp;
+    set_eval_shape(t, dp.n, dp.npw, dp.hh, dp.nd, eb);
+    if (t.smem_eval <= (size_t)kMaxDynSmem) ec.push_back(eb);
+  }
+  int be = sp.ebatch;
+  double te = 1e30;
+  for (int eb : ec) {
+    set_eval_shape(sp, dp.n, dp.npw, dp.hh, dp.nd, eb);
+    const double ms = time_ms([&] { split_eval(dp, p, s); });
+    if (ms < te) te = ms, be = eb;
+  }
+  set_eval_shape(sp, dp.n, dp.npw, dp.hh, dp.nd, be);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(s);
+  cudaFree(f);
+  cudaFree(p);
+  if (cudaGetLastError() != cudaSuccess) {
+    msg = "CUDA error while autotuning";
+    return BFGT_ERR_CUDA;
+  }
+  if (split_check(dp) != BFGT_OK) {
+    msg = "a bounded device-side wait gave up while autotuning";
+    return BFGT_ERR_TIMEOUT;
+  }
+  report[0] = tf;
+  report[1] = te;
+  report[2] = (double)fc.size();
+  report[3] = (double)ec.size();
+  return BFGT_OK;
 }
 
 int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, const std::vector<long long> &offs,

@@ -19,6 +19,12 @@ void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s);
 // cutoff expansions -> leaf values, accumulated into pot (same as k_eval_fp64)
 void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s);
 void split_plan_destroy(DevicePlan &dp);
+// Times the plan's compiled shape choices on its own work lists (scratch
+// arrays; synchronous) and keeps the fastest: form with Y as float2 or
+// double2 and 1 or 2 x-contraction tiles per thread, eval with step groups of
+// 8, 4 or 2.  Every choice gives the same bits.  report: best form and eval
+// ms per launch, and the numbers of choices timed.
+int split_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::string &msg);
 
 // Work lists of a batch of plans whose form and eval stages run as one launch
 // per kernel variant (all chunks of all split plans in the batch).

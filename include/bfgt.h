@@ -75,15 +75,23 @@ int bfgt_set_default_precision(int precision);
 /* No counterpart in the reference.  boxfgt_ and bfgt_boxfgt keep the plans
    (step-0 precomputation and device tables) of their last few argument sets,
    4 by default or BFGT_PLAN_CACHE (0 turns the cache off).  A plan is found
-   again by a 64-bit hash of nd, delta, eps, ipoly, iperiod, norder, precision,
-   nboxes, nlevels, ltree, iptr, itree up to its colleague arrays, centers and
-   boxsize; on a hit the colleague arrays are written back as a fresh plan
-   would leave them and timeinfo(1) is the lookup time.  Calls into the cache
+   again when nd, delta, eps, ipoly, iperiod, norder, precision, nboxes,
+   nlevels, ltree, the device, iptr, itree up to its colleague arrays, centers
+   and boxsize all equal, bit for bit, those it was built from (the cache keeps
+   a copy of them); on a hit the colleague arrays are written back as a fresh
+   plan would leave them and timeinfo(1) is the lookup time.  Calls into the cache
    are serialised by a mutex.  bfgt_plan_cache_clear frees the cached plans;
    bfgt_plan_cache_info gives out[0] entries, out[1] capacity, out[2] hits,
    out[3] misses (out must hold 4). */
 int bfgt_plan_cache_clear(void);
 int bfgt_plan_cache_info(int64_t *out);
+
+/* No counterpart in the reference.  Bytes the last boxfgt_ / bfgt_boxfgt call
+   copied host to device (out[0]) and device to host (out[1]).  pot, grad and
+   hess runs that are all +0.0 on the host (the reference's callers zero pot
+   before each call, hpots/hpots2dadap.f:97-101, 321-325) are cleared on the
+   device instead of uploaded, with the same result bit for bit. */
+int bfgt_boxfgt_last_bytes(double *out);
 
 /* Last error message of this thread ("" when the last call succeeded). */
 const char *bfgt_last_error(void);
@@ -200,8 +208,10 @@ int bfgt_plan_reserve_events(bfgt_plan plan, int n);
    interactions, out[9]=mnlist1, out[10]=internal iperiod, out[11]=number of
    plane-wave chunks (CTAs of the form and eval kernels), out[12]=kernel
    launches per execute, out[13]/out[14]=FP64 form/eval tile shape in use
-   (100 tm + 10 tn + tiles per lane; 0 for split plans).  out must hold 16
-   ints. */
+   (100 tm + 10 tn + tiles per lane; 0 for split plans), out[15]=split
+   kernel shapes in use (100 eval step group + 10 x-contraction tiles per form
+   thread + 1 when the form kernel stages Y as float2; 0 for FP64 plans).  out
+   must hold 16 ints. */
 int bfgt_plan_info(bfgt_plan plan, int *out);
 
 /* Algorithmic work of one execute (every real operation counted once, split
@@ -211,16 +221,24 @@ int bfgt_plan_info(bfgt_plan plan, int *out);
    eval, near-field and translation stages, out[8..10]=compulsory bytes of the
    form, eval and near-field stages, out[11..12]=tensor-core FLOP issued by the
    form and eval stages, out[13..14]=bytes bfgt_plan_execute_host moves host to
-   device and device to host (leaf boxes only).  out must hold 16. */
+   device and device to host (leaf boxes only), out[15]=bytes the last
+   host-array execute actually uploaded: accumulator runs (pot, grad, hess)
+   that are all +0.0 on the host are cleared on the device instead of copied,
+   as when the caller zeroes pot before each call.  out must hold 16. */
 int bfgt_plan_work(bfgt_plan plan, double *out);
 
-/* No counterpart in the reference.  Autotuner of the FP64 kernels' tile
-   shapes: times every compiled shape of the form and eval kernels on this
-   plan's work (on scratch arrays it allocates; synchronous), keeps the fastest
-   for this plan and remembers it for plans of the same (norder, npw, nd)
-   created later in the process.  report (may be NULL) receives the best form
-   and eval ms per launch and the numbers of shapes timed.  Split-precision
-   plans have fixed shapes: nothing is timed. */
+/* No counterpart in the reference.  Autotuner of the kernels' compiled
+   shapes: times every shape of the form and eval kernels that fits this plan
+   on its own work (on scratch arrays it allocates; synchronous) and keeps the
+   fastest.  FP64 plans: the tile shapes, remembered for plans of the same
+   (norder, npw, nd) created later in the process.  Split-precision plans: Y
+   staged as float2 or double2 and 1 or 2 x-contraction tiles per thread in
+   the form kernel, step groups of 8, 4 or 2 in the eval kernel (for this plan
+   only).  FP64 shapes give the same sums to rounding, split shapes the same
+   bits.  report (may be NULL) receives
+   the best form and eval ms per launch and the numbers of shapes timed.  A
+   batch or a captured graph keeps the shapes its plans had when it was made:
+   tune first. */
 int bfgt_plan_autotune(bfgt_plan plan, void *stream, double *report);
 
 /* Waits for the device and reports failures of earlier executes on this plan:

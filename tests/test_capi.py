@@ -76,3 +76,5 @@ def test_default_precision_and_plan_cache_api():
     hb.plan_cache_clear()
     info = hb.plan_cache_info()
     assert info["entries"] == 0 and info["capacity"] >= 0
+    b = hb.last_call_bytes()
+    assert set(b) == {"h2d", "d2h"} and min(b.values()) >= 0

@@ -1,8 +1,10 @@
-"""The tile-shape autotuner (bfgt_plan_autotune): it times the compiled FP64
-tile shapes on the plan's own work lists, keeps the fastest, and later plans
-of the same (norder, npw, nd) start with it.  Results must not change beyond
-FP64 rounding (every shape computes the same sums, 1e-11 against the oracle),
-the caller's arrays are untouched, and split plans have nothing to tune."""
+"""The shape autotuner (bfgt_plan_autotune): it times the compiled FP64 tile
+shapes on the plan's own work lists, keeps the fastest, and later plans of the
+same (norder, npw, nd) start with it.  Results must not change beyond FP64
+rounding (every shape computes the same sums, 1e-11 against the oracle), and
+the caller's arrays are untouched.  Split plans: the form kernel's Y staging
+and x tiles and the eval kernel's step groups are timed; every choice gives
+the same bits as the untuned plan."""
 import numpy as np
 import pytest
 
@@ -39,9 +41,34 @@ def test_autotune_keeps_results_and_caches(trees, name, delta, eps):
     plan.close()
 
 
-def test_autotune_split_plan_is_a_no_op(trees):
-    t = trees["ad16_leg_per"]
-    plan = hb.Plan(t, 1e-4, 1e-6, precision=hb.BFGT_PREC_SPLIT)
-    assert plan.autotune() == (0.0, 0.0, 0)
-    assert plan.info()["form_tile"] == 0
+@pytest.mark.parametrize("name,delta,eps,nd", [("ad16_leg_per", 1e-4, 1e-6, 1), ("ad16_leg_per", 1e-3, 1e-9, 1),
+                                               ("ad_leg_per", 1e-4, 1e-6, 3), ("uni3_leg_per", 1e-2, 1e-6, 1)])
+def test_autotune_split_plan_same_bits(trees, name, delta, eps, nd):
+    import torch
+    t = trees[name]
+    f0 = np.repeat(t.fvals[:, :, None], nd, axis=2) * np.linspace(1.0, 2.0, nd)[None, None, :]
+    f = torch.from_numpy(np.ascontiguousarray(f0).reshape(-1)).cuda()
+    base = hb.Plan(t, delta, eps, nd=nd, precision=hb.BFGT_PREC_SPLIT)
+    p0 = torch.zeros_like(f)
+    base.execute(f, p0)
+    base.check()
+    plan = hb.Plan(t, delta, eps, nd=nd, precision=hb.BFGT_PREC_SPLIT)
+    tf, te, ncand = plan.autotune()
+    assert tf > 0 and te > 0 and ncand >= 2
+    p = torch.zeros_like(f)
+    plan.execute(f, p)
+    plan.check()
+    np.testing.assert_array_equal(p.cpu().numpy(), p0.cpu().numpy())
+    ref = oracle.boxfgt(t, t.fvals, delta, eps).reshape(t.nboxes, -1)
+    lv = t.leaves()
+    got = p.cpu().numpy().reshape(t.nboxes, t.npbox, nd)[lv, :, 0]
+    assert rel_l2(got, ref[lv]) < min(1e-6, 10 * eps)
+    # a batch made after tuning runs the tuned shapes: same bits again
+    batch = hb.Batch([plan])
+    pb = torch.zeros_like(f)
+    batch.execute(f, pb)
+    batch.check()
+    np.testing.assert_array_equal(pb.cpu().numpy(), p0.cpu().numpy())
+    batch.close()
+    base.close()
     plan.close()

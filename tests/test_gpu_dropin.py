@@ -126,3 +126,37 @@ def test_split_selected_falls_back_to_fp64_where_split_cannot_serve(trees):
     p, _, _, _, _ = call(t, 1e-4, 1e-12)
     ref = oracle.boxfgt(t, t.fvals, 1e-4, 1e-12)
     assert rel_l2(p.reshape(t.nboxes, -1)[lv], ref.reshape(t.nboxes, -1)[lv]) < 1e-11
+
+
+def test_zero_pot_is_cleared_on_the_device_not_uploaded(trees):
+    """The reference's callers zero pot before each call (hpots2dadap.f:97-101,
+    321-325).  A zero pot is then not uploaded: the call moves fvals up and pot
+    down only, and gives the same bits as the upload path, which a single -0.0
+    in pot forces (-0.0 is not skipped, so sums of signed zeros stay as the
+    reference's)."""
+    t = trees["ad16_leg_per"]
+    lv = t.leaves()
+    p0, _, _, _, _ = call(t, 1e-4, 1e-6)
+    b0 = hb.last_call_bytes()
+    leaf_bytes = 8 * t.npbox * len(lv)
+    assert leaf_bytes <= b0["h2d"] < 2 * leaf_bytes  # fvals runs only
+    assert b0["d2h"] >= leaf_bytes
+    pot = np.zeros(t.npbox * t.nboxes)
+    pot.reshape(t.nboxes, -1)[lv[0], 0] = -0.0
+    ti = np.zeros(20)
+    hb.boxfgt(1, 2, 1e-4, 1e-6, t.ipoly, t.iperiod, t.norder, t.npbox, t.nboxes, t.nlevels, t.ltree, t.itree.copy(),
+              t.iptr, t.centers, t.boxsize, np.ascontiguousarray(t.fvals), 1, pot, None, None, 0, 0, None, 0, None,
+              None, None, ti)
+    b1 = hb.last_call_bytes()
+    assert b1["h2d"] == b0["h2d"] + b0["d2h"]  # pot uploaded too
+    np.testing.assert_array_equal(pot, p0)
+    # a nonzero pot is accumulated into
+    base = np.random.default_rng(5).standard_normal(t.npbox * t.nboxes)
+    pot2 = base.copy()
+    hb.boxfgt(1, 2, 1e-4, 1e-6, t.ipoly, t.iperiod, t.norder, t.npbox, t.nboxes, t.nlevels, t.ltree, t.itree.copy(),
+              t.iptr, t.centers, t.boxsize, np.ascontiguousarray(t.fvals), 1, pot2, None, None, 0, 0, None, 0, None,
+              None, None, ti)
+    np.testing.assert_allclose(pot2.reshape(t.nboxes, -1)[lv], (base + p0).reshape(t.nboxes, -1)[lv], rtol=0,
+                               atol=1e-14 * (np.abs(base).max() + np.abs(p0).max()))
+    nonleaf = t.nchild() > 0
+    np.testing.assert_array_equal(pot2.reshape(t.nboxes, -1)[nonleaf], base.reshape(t.nboxes, -1)[nonleaf])

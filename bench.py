@@ -367,6 +367,68 @@ def run_uniform5(args):
     print(json.dumps(line), flush=True)
 
 
+def run_near16(args):
+    """Regime C (near field only): a uniform level-8 periodic tree, Legendre
+    order 16 (65,536 leaves, 16.8 M points, as many as the adaptive tree), 20
+    Gaussians (seed 2, widths log-uniform in [1e-3, 1e-2], N(0,1)
+    amplitudes), nd=1, delta=1e-6, eps=1e-6: every leaf interacts with its 8
+    neighbours and itself through the near-field tables.  Device time of the
+    near-field stage against the FP64 peak (it is FP64 work in both
+    precisions) and against HBM."""
+    import torch
+    import heat2d_per_box_b200 as hb
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(2)
+    g = hb.gauss_params(rng.uniform(-0.5, 0.5, (20, 2)), np.exp(rng.uniform(np.log(1e-3), np.log(1e-2), 20)),
+                        rng.standard_normal(20))
+    t = hb.build_uniform(8, g, norder=16, ipoly=0, iperiod=1)
+    delta, eps = 1e-6, 1e-6
+    npts = len(t.leaves()) * t.npbox
+    f = torch.from_numpy(t.fvals.reshape(-1)).cuda()
+    stream = torch.cuda.current_stream()
+    res = {}
+    for prec in (hb.BFGT_PREC_FP64, hb.BFGT_PREC_SPLIT):
+        plan = hb.Plan(t, delta, eps, precision=prec)
+        plan.autotune(stream)
+        p = torch.zeros_like(f)
+        for _ in range(args.warmup):
+            plan.execute(f, p, stream)
+        plan.reserve_events(args.steps + 8)
+        plan.stage_ms()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.execute(f, p, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        st = plan.stage_ms()
+        res[prec] = (e0.elapsed_time(e1) / args.steps, st[4] / max(st[6], 1), plan.info(), plan.work(), p.clone())
+        plan.close()
+    ms64, near64, info, work, p64 = res[hb.BFGT_PREC_FP64]
+    mss, nears, _, _, ps = res[hb.BFGT_PREC_SPLIT]
+    lv = t.leaves()
+    a = ps.cpu().numpy().reshape(t.nboxes, -1)[lv]
+    b = p64.cpu().numpy().reshape(t.nboxes, -1)[lv]
+    hbm = peaks()[0]
+    line = {"metric": METRIC, "value": npts / (mss * 1e-3), "unit": "leaf points/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mss, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f16-split/f32acc/f64", "data": "synthetic",
+            "config": {"workload": "uniform level-8 periodic tree, Legendre order 16, 20 Gaussians (seed 2), nd=1, "
+                                   "delta=1e-6, eps=1e-6 (regime C: near field only)",
+                       "leaves": int(len(lv)), "points": int(npts), "regime": info["regime"],
+                       "near_pairs": info["nnear_pairs"]},
+            "fp64_value": npts / (ms64 * 1e-3), "fp64_ms_per_step": ms64,
+            "near_ms": {"split": nears, "fp64": near64},
+            "near_roofline": {"flop_per_launch": work["flops_near"], "bytes_per_launch": work["bytes_near"],
+                              "fp64_tflops": work["flops_near"] / (near64 * 1e-3) / 1e12,
+                              "frac_of_nominal_40tflops_fp64": work["flops_near"] / (near64 * 1e-3) / 40e12,
+                              "hbm_gbs": work["bytes_near"] / (near64 * 1e-3) / 1e9,
+                              "frac_of_hbm": work["bytes_near"] / (near64 * 1e-3) / 1e9 / hbm},
+            "split_rel_l2_err_vs_fp64": float(np.linalg.norm(a - b) / np.linalg.norm(b))}
+    print(json.dumps(line), flush=True)
+
+
 def run_heat5(args):
     """The transforms of one time step of the reaction-diffusion / heat solvers
     (hpots2dadap.f:79, 329-346): the initial-value transform with delta = 4 dt
@@ -443,10 +505,11 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "split"])
     ap.add_argument("--small", action="store_true", help="level-6 base tree (for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="adaptive16", choices=["adaptive16", "uneven64", "uniform5", "heat5"],
+    ap.add_argument("--workload", default="adaptive16", choices=["adaptive16", "uneven64", "uniform5", "heat5", "near16"],
                     help="adaptive16: one adaptive order-16 tree (default); uneven64: 64 uneven order-8 trees, "
                          "nd=8, batched in one graph; uniform5: the plain FP64 case on a uniform level-5 order-8 "
-                         "tree; heat5: the 5 transforms of one heat-solver time step, batched in one graph")
+                         "tree; heat5: the 5 transforms of one heat-solver time step, batched in one graph; "
+                         "near16: regime C (near field only) on a uniform level-8 order-16 tree")
     ap.add_argument("--trees", type=int, default=64,
                     help="uneven64: use only the first N of the 64 trees (for profiler captures)")
     args = ap.parse_args()
@@ -467,6 +530,9 @@ def main():
         return
     if args.workload == "heat5":
         run_heat5(args)
+        return
+    if args.workload == "near16":
+        run_near16(args)
         return
 
     import torch

@@ -24,7 +24,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["fgt_device.cu", "split_kernels.cu", "split_fix.cu", "noalloc.cu"]
+CU_SOURCES = ["fgt_device.cu", "split_kernels.cu", "split_fix.cu", "near_tc.cu", "noalloc.cu"]
 CPP_SOURCES = ["host_plan.cpp", "tree_build.cpp", "capi.cpp"]
 
 

@@ -21,6 +21,12 @@ struct DeviceBatch {
   int2 *tr_work = nullptr, *nf_work = nullptr;    // {plan, block of the plan}
   int tr_blocks = 0, nf_blocks = 0;
   size_t smem_near = 0;
+  // tensor-core near field of split plans: per-plan arguments, {plan, CTA}
+  // work of the order-8 and order-16 plans
+  void *ntc_descs = nullptr;
+  int2 *ntc_work[2] = {nullptr, nullptr};
+  int ntc_blocks[2] = {0, 0};
+  size_t smem_ntc[2] = {0, 0};
   std::vector<std::array<cudaEvent_t, 6>> evsets;
   int nrec = 0;
   bool events = false;

@@ -36,6 +36,17 @@ struct SplitPlan {
   double tc_flops_form = 0, tc_flops_eval = 0;
 };
 
+// Tensor-core near field of a split plan (near_tc.cuh); empty when the FP64
+// near-field kernel serves the plan.
+struct NearTcPlan {
+  int4 *ctas = nullptr, *tiles = nullptr;
+  int2 *pairs = nullptr;
+  int *targets = nullptr, *slot_q = nullptr;
+  uint16_t *tabB = nullptr;
+  int nctas = 0, maxslot = 0;
+  size_t smem = 0;
+};
+
 struct DevicePlan {
   int device = 0;
   int nd = 1, n = 0, npw = 0, hh = 0, nexp = 0, nlevels = 0, nboxes = 0, precision = 0;
@@ -72,6 +83,7 @@ struct DevicePlan {
   size_t t_coef_elems = 0;
   int t_leaf_cap = 0, ipoly = 0;
   bool targ_ready = false;
+  NearTcPlan ntc;
   double2 *Mpart = nullptr;     // (nchunks, nd, nexp) partial expansions per chunk
   double2 *M = nullptr;         // (ncut, nd, nexp) cutoff-box expansions
   double2 *L = nullptr;         // (ncut, nd, nexp) cutoff-box local expansions

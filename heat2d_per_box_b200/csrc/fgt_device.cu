@@ -35,6 +35,7 @@
 #include "batch.hpp"
 #include "device_plan.hpp"
 #include "fgt_common.cuh"
+#include "near_tc.cuh"
 #include "split_kernels.cuh"
 
 namespace bfgt {
@@ -868,6 +869,15 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     chk(upload(dp.tab_loc, hp.tab_loc, msg));
     chk(upload(dp.ind_loc, hp.ind_loc, msg));
     dp.smem_near = sizeof(double) * (size_t)kWarps * 3 * n * n;
+    // split plans with floating slices: the near field on the tensor cores
+    // (fixed-point plans keep the FP64 kernel, which meets their smaller eps)
+    if (rc == BFGT_OK && dp.precision == BFGT_PREC_SPLIT && hp.eps >= 1e-7 && !dp.split.fixed) {
+      if (!dp.split.err) {
+        std::vector<int> zero(4, 0);
+        chk(upload(dp.split.err, zero, msg));
+      }
+      chk(near_tc_create(dp, hp, msg));
+    }
   }
   // the 227 KB per-block limit minus room for the kernels' static shared variables
   const size_t smax = 227 * 1024 - 1024;
@@ -891,6 +901,7 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
 void device_plan_destroy(DevicePlan &dp) {
   if (dp.graph_exec) cudaGraphExecDestroy(dp.graph_exec);
   if (dp.graph) cudaGraphDestroy(dp.graph);
+  near_tc_destroy(dp);
   split_plan_destroy(dp);
   void *ptrs[] = {dp.T, dp.E, dp.PH, dp.ph_off, dp.leaves, dp.chunks, dp.columns, dp.columns64, dp.cut_chunk_begin, dp.cut_pw_begin,
                   dp.cut_pw_src, dp.cut_pw_ind, dp.W, dp.pw_weight, dp.kscale, dp.dfac, dp.Ld, dp.tab3_loc, dp.t_nchild, dp.t_ichild, dp.t_level, dp.t_centers, dp.t_boxsize, dp.t_umat, dp.t_has, dp.t_coefs, dp.t_leaf, dp.Mpart, dp.M, dp.L, dp.G, dp.gcnt, dp.bcnt, dp.chunk_group, dp.groups, dp.box_groups, dp.nf_target,
@@ -1006,7 +1017,9 @@ int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cu
   } else if (ev) {
     for (int i = 1; i <= 4; i++) cudaEventRecord(ev[i], s);
   }
-  if (dp.nnf > 0)
+  if (dp.ntc.nctas > 0)
+    near_tc_launch(dp.n, dp.ntc.nctas, dp.ntc.smem, s, NearTcLaunch{near_tc_args(dp, 0), nullptr, nullptr, d_fvals, d_pot});
+  else if (dp.nnf > 0)
     k_near_fp64<<<(dp.nnf + kWarps - 1) / kWarps, kWarps * 32, dp.smem_near, s>>>(
         NearLaunch{near_args(dp, 0), nullptr, nullptr, d_fvals, d_pot});
   if (ev) cudaEventRecord(ev[5], s);
@@ -1300,7 +1313,8 @@ int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, 
   if (rc != BFGT_OK) return rc;
   std::vector<TrArgs> tr;
   std::vector<NearArgs> nf;
-  std::vector<int2> trw, nfw;
+  std::vector<NearTcArgs> ntc;
+  std::vector<int2> trw, nfw, ntw[2];
   for (size_t i = 0; i < plans.size(); i++) {
     const DevicePlan &dp = *plans[i];
     tr.push_back(tr_args(dp));
@@ -1309,13 +1323,23 @@ int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, 
       const size_t tot = tr_threads(dp.ncut, dp.nd, dp.nexp);
       for (size_t k = 0; k < (tot + kTrThreads - 1) / kTrThreads; k++) trw.push_back(make_int2((int)i, (int)k));
     }
-    for (int t = 0; t < dp.nnf; t += kWarps) nfw.push_back(make_int2((int)i, t));
-    b.smem_near = std::max(b.smem_near, dp.smem_near);
+    ntc.push_back(near_tc_args(dp, b.offs[i]));
+    if (dp.ntc.nctas > 0) {
+      // the tensor-core near field: one launch per order (8, 16)
+      const int v = dp.n == 16 ? 1 : 0;
+      for (int c = 0; c < dp.ntc.nctas; c++) ntw[v].push_back(make_int2((int)i, c));
+      b.smem_ntc[v] = std::max(b.smem_ntc[v], dp.ntc.smem);
+    } else {
+      for (int t = 0; t < dp.nnf; t += kWarps) nfw.push_back(make_int2((int)i, t));
+      b.smem_near = std::max(b.smem_near, dp.smem_near);
+    }
   }
   b.tr_blocks = (int)trw.size();
   b.nf_blocks = (int)nfw.size();
+  for (int v = 0; v < 2; v++) b.ntc_blocks[v] = (int)ntw[v].size();
   TrArgs *dtr = nullptr;
   NearArgs *dnf = nullptr;
+  NearTcArgs *dnt = nullptr;
   auto chk = [&](int r) {
     if (rc == BFGT_OK && r != BFGT_OK) rc = r;
   };
@@ -1323,8 +1347,13 @@ int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, 
   chk(upload(dnf, nf, msg));
   chk(upload(b.tr_work, trw, msg));
   chk(upload(b.nf_work, nfw, msg));
+  if (b.ntc_blocks[0] + b.ntc_blocks[1] > 0) {
+    chk(upload(dnt, ntc, msg));
+    for (int v = 0; v < 2; v++) chk(upload(b.ntc_work[v], ntw[v], msg));
+  }
   b.tr_descs = dtr;
   b.nf_descs = dnf;
+  b.ntc_descs = dnt;
   if (rc == BFGT_OK) {
     b.events = true;
     reserve_event_sets(b.evsets, 8);
@@ -1333,7 +1362,8 @@ int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, 
 }
 
 int device_batch_launches(const DeviceBatch &b) {
-  int n = split_batch_launches(b.split) + (b.tr_blocks > 0) + (b.nf_blocks > 0);
+  int n = split_batch_launches(b.split) + (b.tr_blocks > 0) + (b.nf_blocks > 0) + (b.ntc_blocks[0] > 0) +
+          (b.ntc_blocks[1] > 0);
   for (const DevicePlan *dp : b.plans)
     if (dp->precision != BFGT_PREC_SPLIT && has_pw(*dp)) n += 2;
   return n;
@@ -1358,6 +1388,11 @@ int device_batch_execute(DeviceBatch &b, const double *d_fvals, double *d_pot, c
   if (b.nf_blocks > 0)
     k_near_fp64<<<b.nf_blocks, kWarps * 32, b.smem_near, s>>>(
         NearLaunch{NearArgs{}, static_cast<const NearArgs *>(b.nf_descs), b.nf_work, d_fvals, d_pot});
+  for (int v = 0; v < 2; v++)
+    if (b.ntc_blocks[v] > 0)
+      near_tc_launch(v ? 16 : 8, b.ntc_blocks[v], b.smem_ntc[v], s,
+                     NearTcLaunch{NearTcArgs{}, static_cast<const NearTcArgs *>(b.ntc_descs), b.ntc_work[v], d_fvals,
+                                  d_pot});
   if (ev) cudaEventRecord(ev[5], s);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -1373,7 +1408,7 @@ void device_batch_destroy(DeviceBatch &b) {
   if (b.graph_exec) cudaGraphExecDestroy(b.graph_exec);
   if (b.graph) cudaGraphDestroy(b.graph);
   split_batch_destroy(b.split);
-  void *ptrs[] = {b.tr_descs, b.nf_descs, b.tr_work, b.nf_work};
+  void *ptrs[] = {b.tr_descs, b.nf_descs, b.tr_work, b.nf_work, b.ntc_descs, b.ntc_work[0], b.ntc_work[1]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &es : b.evsets)

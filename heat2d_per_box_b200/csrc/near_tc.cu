@@ -1,0 +1,433 @@
+// Tensor-core near field of split-precision plans (see near_tc.cuh).
+#include "near_tc.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "../../include/bfgt.h"
+#include "tc_sm100.cuh"
+
+namespace bfgt {
+
+namespace {
+
+constexpr int kNtThreads = 128;                       // one thread per MMA row
+constexpr int kNtA = 128 * 16 * 2;                    // one BF16 slice of a 128 x 16 A operand
+constexpr int kNtB = 16 * 16 * 2;                     // one slice of a 16 x 16 B operand
+constexpr int kNtTab = 3 * kNtB / 2;                  // uint16 per table slot (3 slices)
+constexpr size_t kNtFixed = 3 * kNtA + 3 * kNtB;      // operand buffers
+constexpr size_t kNtMinSmem = 29 * 1024;              // at most 7 CTAs per SM: 7 x 64 TMEM columns fit
+constexpr uint32_t kNtWaitIters = 1u << 26;
+
+// host copy of tc::kmajor_off
+inline uint32_t kmajor_off_host(int r, int k, int R) {
+  return (uint32_t)((((k >> 3) * (R >> 3) + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+// FP64 -> FP32 -> three BF16 slices by truncation (as tc::split3_bf16x1)
+inline void split3_host(double v, uint16_t &s0, uint16_t &s1, uint16_t &s2) {
+  auto hi = [](float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u &= 0xFFFF0000u;
+    float y;
+    std::memcpy(&y, &u, 4);
+    return y;
+  };
+  auto top = [](float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    return (uint16_t)(u >> 16);
+  };
+  const float a = (float)v;
+  const float h = hi(a), r = a - h;
+  const float m = hi(r), l = r - m;
+  s0 = top(h);
+  s1 = top(m);
+  s2 = top(l);
+}
+
+template <typename T>
+int upload_nt(T *&d, const std::vector<T> &v, std::string &msg) {
+  d = nullptr;
+  if (v.empty()) return BFGT_OK;
+  if (cudaMalloc(&d, sizeof(T) * v.size()) != cudaSuccess) {
+    cudaGetLastError();
+    msg = "cudaMalloc failed (tensor-core near field)";
+    return BFGT_ERR_OOM;
+  }
+  if (cudaMemcpy(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    msg = "cudaMemcpy failed (tensor-core near field)";
+    return BFGT_ERR_CUDA;
+  }
+  return BFGT_OK;
+}
+
+// Stores the 16 K values v[0..15] of MMA row r as three BF16 slices (K-major
+// core layout, R = 128 rows).
+__device__ __forceinline__ void store_row16(unsigned char *sA, int r, const float (&v)[16]) {
+#pragma unroll
+  for (int k0 = 0; k0 < 16; k0 += 8) {
+    uint32_t p[3][4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const float a0 = v[k0 + 2 * q], a1 = v[k0 + 2 * q + 1];
+      const float h0 = tc::bf16_hi(a0), h1 = tc::bf16_hi(a1);
+      const float r0 = a0 - h0, r1 = a1 - h1;
+      const float m0 = tc::bf16_hi(r0), m1 = tc::bf16_hi(r1);
+      const float l0 = r0 - m0, l1 = r1 - m1;
+      p[0][q] = __byte_perm(__float_as_uint(h0), __float_as_uint(h1), 0x7632);
+      p[1][q] = __byte_perm(__float_as_uint(m0), __float_as_uint(m1), 0x7632);
+      p[2][q] = __byte_perm(__float_as_uint(l0), __float_as_uint(l1), 0x7632);
+    }
+    const uint32_t o = tc::kmajor_off(r, k0, 128);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      *reinterpret_cast<uint4 *>(sA + c * kNtA + o) = make_uint4(p[c][0], p[c][1], p[c][2], p[c][3]);
+  }
+}
+
+// The six slice products i + j <= 2 of one 128 x 16 x 16 MMA step: s0 s0 into
+// D0, the corrections into D1.
+__device__ __forceinline__ void near_mmas(uint32_t d0, uint32_t d1, uint32_t aA, uint32_t aB, uint32_t acc) {
+  constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 16);
+  uint64_t ad[3], bd[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    ad[c] = tc::smem_desc(aA + c * kNtA, (128 / 8) * 128, 128);
+    bd[c] = tc::smem_desc(aB + c * kNtB, (16 / 8) * 128, 128);
+  }
+  tc::mma_bf16(d0, ad[0], bd[0], idesc, acc);
+  tc::mma_bf16(d1, ad[0], bd[1], idesc, acc);
+  tc::mma_bf16(d1, ad[1], bd[0], idesc, 1u);
+  tc::mma_bf16(d1, ad[0], bd[2], idesc, 1u);
+  tc::mma_bf16(d1, ad[1], bd[1], idesc, 1u);
+  tc::mma_bf16(d1, ad[2], bd[0], idesc, 1u);
+}
+
+// One CTA: up to 128/kN targets; per density, stage A over the CTA's pair
+// tiles into Q (shared memory), then stage B over the slots into pot.
+// TMEM: D0, D1 of stage A in columns 0-31, of stage B in 32-63.
+template <int kN>
+__global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ NearTcLaunch lp) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar[2];  // MMA groups; the final drain
+  __shared__ uint32_t tmem_slot;
+  constexpr int kG = 128 / kN;  // pairs per stage-A tile, targets per CTA
+  const NearTcArgs &a = lp.descs ? lp.descs[lp.work[blockIdx.x].x] : lp.one;
+  const int cta = lp.descs ? lp.work[blockIdx.x].y : (int)blockIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int4 c = a.ctas[cta];
+  const int ntarget = c.w & 0xFF, nslot = c.w >> 8;
+  const int nd = a.nd, npb = kN * kN;
+  const double *fv = lp.fbase + a.elem_off;
+  double *pot = lp.pbase + a.elem_off;
+  unsigned char *sA = smem;
+  unsigned char *sB = smem + 3 * kNtA;
+  float *sQ = reinterpret_cast<float *>(smem + kNtFixed);  // [tl][slot][j1][k2]
+  const int qsz = kG * nslot * npb;
+
+  if (warp == 0) tc::tmem_alloc(&tmem_slot, 64);
+  if (tid == 0) {
+    tc::mbar_init(&mbar[0], 1);
+    tc::mbar_init(&mbar[1], 1);
+    tc::fence_mbar_init();
+  }
+  // kN = 8: the K columns 8-15 of A are zero for the whole kernel
+  if (kN == 8) {
+    const float z[16] = {};
+    store_row16(sA, tid, z);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+  const uint32_t aA = tc::smem_u32(sA), aB = tc::smem_u32(sB);
+  bool ok = true;
+  uint32_t phase = 0;
+  // stage-A row: pair i of the tile, grid index j1; stage-B row: target tl, k2
+  const int ri = tid / kN, rj = tid % kN;
+  const int *slot_q = a.slot_q + (size_t)cta * kNearTcSlots;
+
+  for (int ind = 0; ind < nd; ind++) {
+    for (int e = tid; e < qsz; e += kNtThreads) sQ[e] = 0.0f;
+    __syncthreads();
+    for (int t = c.x; t < c.y; t++) {
+      const int4 T = a.tiles[t];
+      const uint16_t *tb = a.tabB + (size_t)T.x * kNtTab;
+      for (int u = tid; u < 3 * kNtB / 16; u += kNtThreads) tc::cp_async16(sB + 16 * u, tb + 8 * u);
+      tc::cp_async_commit();
+      const int2 pr = ri < T.z ? a.pairs[T.y + ri] : make_int2(-1, 0);
+      if (pr.x >= 0) {
+        // F(j1 = rj, j2), j2 = 0..kN-1, of the source (fvals(nd, kN, kN, box), x fastest)
+        const double *src = fv + (size_t)pr.x * nd * npb + ind + (size_t)nd * rj;
+        float v[16];
+#pragma unroll
+        for (int j2 = 0; j2 < 16; j2++) v[j2] = j2 < kN ? __double2float_rn(src[(size_t)nd * kN * j2]) : 0.0f;
+        if (kN == 16) {
+          store_row16(sA, tid, v);
+        } else {
+          // only the first 8 K columns of the row (the rest stay zero)
+          uint32_t p[3][4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const float a0 = v[2 * q], a1 = v[2 * q + 1];
+            const float h0 = tc::bf16_hi(a0), h1 = tc::bf16_hi(a1);
+            const float r0 = a0 - h0, r1 = a1 - h1;
+            const float m0 = tc::bf16_hi(r0), m1 = tc::bf16_hi(r1);
+            const float l0 = r0 - m0, l1 = r1 - m1;
+            p[0][q] = __byte_perm(__float_as_uint(h0), __float_as_uint(h1), 0x7632);
+            p[1][q] = __byte_perm(__float_as_uint(m0), __float_as_uint(m1), 0x7632);
+            p[2][q] = __byte_perm(__float_as_uint(l0), __float_as_uint(l1), 0x7632);
+          }
+          const uint32_t o = tc::kmajor_off(tid, 0, 128);
+#pragma unroll
+          for (int cc = 0; cc < 3; cc++)
+            *reinterpret_cast<uint4 *>(sA + cc * kNtA + o) = make_uint4(p[cc][0], p[cc][1], p[cc][2], p[cc][3]);
+        }
+      }
+      tc::cp_async_wait_all();
+      tc::fence_async_smem();
+      tc::fence_before_sync();
+      __syncthreads();
+      tc::fence_after_sync();
+      if (tid == 0 && ok) {
+        near_mmas(tmem, tmem + 16, aA, aB, 0u);
+        tc::commit(&mbar[0]);
+      }
+      if (ok && !tc::mbar_wait(&mbar[0], phase & 1, a.wait_iters)) {
+        ok = false;
+        atomicExch(a.err, 1);
+      }
+      phase++;
+      tc::fence_after_sync();
+      float d0[16], d1[16];
+      if (kN == 16) {
+        tc::tmem_ld16(tmem + lane_base, d0);
+        tc::tmem_ld16(tmem + lane_base + 16, d1);
+      } else {
+        tc::tmem_ld8(tmem + lane_base, d0);
+        tc::tmem_ld8(tmem + lane_base + 16, d1);
+      }
+      tc::tmem_ld_wait();
+      if (pr.x >= 0 && ok) {
+        const int tl = pr.y & 0xFF, slot = pr.y >> 8;
+        float *q = sQ + ((size_t)(tl * nslot + slot) * kN + rj) * kN;
+#pragma unroll
+        for (int k2 = 0; k2 < kN; k2++) q[k2] += d0[k2] + d1[k2];
+      }
+      tc::fence_before_sync();
+      __syncthreads();
+    }
+    // stage B: one K block per slot, accumulated in TMEM columns 32-63
+    for (int sl = 0; sl < nslot; sl++) {
+      const uint16_t *tb = a.tabB + (size_t)slot_q[sl] * kNtTab;
+      for (int u = tid; u < 3 * kNtB / 16; u += kNtThreads) tc::cp_async16(sB + 16 * u, tb + 8 * u);
+      tc::cp_async_commit();
+      {
+        // A row (tl = ri, k2 = rj): Q(tl, slot, j1, k2) over j1
+        const float *q = sQ + (size_t)(ri * nslot + sl) * npb + rj;
+        float v[16];
+#pragma unroll
+        for (int j1 = 0; j1 < 16; j1++) v[j1] = j1 < kN ? q[(size_t)kN * j1] : 0.0f;
+        store_row16(sA, tid, v);
+      }
+      tc::cp_async_wait_all();
+      tc::fence_async_smem();
+      tc::fence_before_sync();
+      __syncthreads();
+      tc::fence_after_sync();
+      if (tid == 0 && ok) {
+        near_mmas(tmem + 32, tmem + 48, aA, aB, sl > 0 ? 1u : 0u);
+        tc::commit(&mbar[0]);
+      }
+      if (ok && !tc::mbar_wait(&mbar[0], phase & 1, a.wait_iters)) {
+        ok = false;
+        atomicExch(a.err, 1);
+      }
+      phase++;
+      tc::fence_after_sync();
+      __syncthreads();  // every thread has read its Q row and the MMA is done: sA, sB are free
+    }
+    if (nslot > 0) {
+      float d0[16], d1[16];
+      if (kN == 16) {
+        tc::tmem_ld16(tmem + lane_base + 32, d0);
+        tc::tmem_ld16(tmem + lane_base + 48, d1);
+      } else {
+        tc::tmem_ld8(tmem + lane_base + 32, d0);
+        tc::tmem_ld8(tmem + lane_base + 48, d1);
+      }
+      tc::tmem_ld_wait();
+      if (ok && ri < ntarget) {
+        // pot(k1, k2 = rj) of target ri, k1 = 0..kN-1
+        double *pb = pot + (size_t)a.targets[c.z + ri] * nd * npb + ind + (size_t)nd * kN * rj;
+#pragma unroll
+        for (int k1 = 0; k1 < kN; k1++) pb[(size_t)nd * k1] += (double)d0[k1] + (double)d1[k1];
+      }
+      tc::fence_before_sync();
+      __syncthreads();
+    }
+  }
+  // drain: no tensor-core operation of this CTA may be in flight when TMEM is freed
+  if (tid == 0) tc::commit(&mbar[1]);
+  if (!tc::mbar_wait(&mbar[1], 0, kNtWaitIters)) atomicExch(a.err, 2);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 64);
+}
+
+}  // namespace
+
+int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
+  near_tc_destroy(dp);
+  const int n = hp.norder;
+  if (hp.nf_target.empty() || (n != 8 && n != 16)) return BFGT_OK;
+  const int nslots_tab = 13 * (hp.nlevels + 1);
+  if ((int)hp.tab_loc.size() < n * n * nslots_tab || (int)hp.ind_loc.size() < 2 * (n + 1) * nslots_tab) return BFGT_OK;
+  // the table operands: B(out k, in j) = tab_loc(j, k, slot) inside the band
+  // pattern, 0 outside; slots whose band is empty are marked unused
+  std::vector<uint16_t> tab((size_t)nslots_tab * kNtTab, 0);
+  std::vector<char> used(nslots_tab, 0);
+  for (int q = 0; q < nslots_tab; q++) {
+    const int *il = &hp.ind_loc[(size_t)2 * (n + 1) * q];
+    const int k0 = il[2 * n], k1 = il[2 * n + 1];
+    if (k1 - k0 + 1 <= 0) continue;
+    used[q] = 1;
+    const double *t = &hp.tab_loc[(size_t)n * n * q];
+    uint16_t *dst = &tab[(size_t)q * kNtTab];
+    for (int k = k0 - 1; k < k1; k++) {
+      const int lo = il[2 * k], hi = il[2 * k + 1];
+      for (int j = lo - 1; j < hi; j++) {
+        uint16_t s[3];
+        split3_host(t[j + (size_t)n * k], s[0], s[1], s[2]);
+        const uint32_t o = kmajor_off_host(k, j, 16) / 2;
+        for (int cc = 0; cc < 3; cc++) dst[cc * (kNtB / 2) + o] = s[cc];
+      }
+    }
+  }
+  // CTAs of up to kG targets whose entries use at most kNearTcSlots distinct
+  // x tables; entries with an empty table contribute nothing and are dropped
+  const int kG = 128 / n;
+  struct Pair {
+    int src, tl, slot, qy;
+  };
+  std::vector<int4> ctas, tiles;
+  std::vector<int2> pairs;
+  std::vector<int> targets, slot_q;
+  std::vector<Pair> cur;
+  std::vector<int> cur_q, cur_t;
+  int maxslot = 0;
+  auto close_cta = [&]() {
+    if (cur_t.empty()) return;
+    std::stable_sort(cur.begin(), cur.end(), [](const Pair &x, const Pair &y) {
+      if (x.qy != y.qy) return x.qy < y.qy;
+      if (x.tl != y.tl) return x.tl < y.tl;
+      return x.slot < y.slot;
+    });
+    int4 c;
+    c.x = (int)tiles.size();
+    size_t i = 0;
+    while (i < cur.size()) {
+      size_t j = i;
+      while (j < cur.size() && cur[j].qy == cur[i].qy && (int)(j - i) < kG) j++;
+      tiles.push_back(make_int4(cur[i].qy, (int)pairs.size(), (int)(j - i), 0));
+      for (size_t k = i; k < j; k++) pairs.push_back(make_int2(cur[k].src, cur[k].tl | (cur[k].slot << 8)));
+      i = j;
+    }
+    c.y = (int)tiles.size();
+    c.z = (int)targets.size();
+    c.w = (int)cur_t.size() | ((int)cur_q.size() << 8);
+    targets.insert(targets.end(), cur_t.begin(), cur_t.end());
+    for (int s = 0; s < kNearTcSlots; s++) slot_q.push_back(s < (int)cur_q.size() ? cur_q[s] : 0);
+    maxslot = std::max(maxslot, (int)cur_q.size());
+    ctas.push_back(c);
+    cur.clear();
+    cur_q.clear();
+    cur_t.clear();
+  };
+  for (size_t t = 0; t < hp.nf_target.size(); t++) {
+    std::vector<int> ents, qxs;
+    for (int e = hp.nf_begin[t]; e < hp.nf_begin[t + 1]; e++) {
+      const int qx = hp.nf_elev[e] * 13 + hp.nf_ix[e] + 6, qy = hp.nf_elev[e] * 13 + hp.nf_iy[e] + 6;
+      if (qx < 0 || qy < 0 || qx >= nslots_tab || qy >= nslots_tab || !used[qx] || !used[qy]) continue;
+      ents.push_back(e);
+      if (std::find(qxs.begin(), qxs.end(), qx) == qxs.end()) qxs.push_back(qx);
+    }
+    if (ents.empty()) continue;
+    if ((int)qxs.size() > kNearTcSlots) return BFGT_OK;  // the FP64 kernel serves this plan
+    int add = 0;
+    for (int q : qxs)
+      if (std::find(cur_q.begin(), cur_q.end(), q) == cur_q.end()) add++;
+    if ((int)cur_t.size() == kG || (int)cur_q.size() + add > kNearTcSlots) close_cta();
+    const int tl = (int)cur_t.size();
+    cur_t.push_back(hp.nf_target[t]);
+    for (int e : ents) {
+      const int qx = hp.nf_elev[e] * 13 + hp.nf_ix[e] + 6, qy = hp.nf_elev[e] * 13 + hp.nf_iy[e] + 6;
+      auto it = std::find(cur_q.begin(), cur_q.end(), qx);
+      int slot = (int)(it - cur_q.begin());
+      if (it == cur_q.end()) cur_q.push_back(qx);
+      cur.push_back(Pair{hp.nf_src[e], tl, slot, qy});
+    }
+  }
+  close_cta();
+  if (ctas.empty()) return BFGT_OK;
+  NearTcPlan &p = dp.ntc;
+  int rc = BFGT_OK;
+  auto chk = [&](int x) {
+    if (rc == BFGT_OK && x != BFGT_OK) rc = x;
+  };
+  chk(upload_nt(p.ctas, ctas, msg));
+  chk(upload_nt(p.tiles, tiles, msg));
+  chk(upload_nt(p.pairs, pairs, msg));
+  chk(upload_nt(p.targets, targets, msg));
+  chk(upload_nt(p.slot_q, slot_q, msg));
+  chk(upload_nt(p.tabB, tab, msg));
+  if (rc != BFGT_OK) {
+    near_tc_destroy(dp);
+    return rc;
+  }
+  p.nctas = (int)ctas.size();
+  p.maxslot = maxslot;
+  p.smem = std::max(kNtFixed + sizeof(float) * (size_t)kG * maxslot * n * n, kNtMinSmem);
+  const int smax = 227 * 1024 - 1024;
+  if (p.smem > (size_t)smax) {
+    near_tc_destroy(dp);
+    return BFGT_OK;
+  }
+  cudaFuncSetAttribute(k_near_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
+  cudaFuncSetAttribute(k_near_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
+  if (cudaGetLastError() != cudaSuccess) {
+    msg = "CUDA error while preparing the tensor-core near field";
+    near_tc_destroy(dp);
+    return BFGT_ERR_CUDA;
+  }
+  return BFGT_OK;
+}
+
+void near_tc_destroy(DevicePlan &dp) {
+  NearTcPlan &p = dp.ntc;
+  void *ptrs[] = {p.ctas, p.tiles, p.pairs, p.targets, p.slot_q, p.tabB};
+  for (void *x : ptrs)
+    if (x) cudaFree(x);
+  p = NearTcPlan();
+}
+
+NearTcArgs near_tc_args(const DevicePlan &dp, long long elem_off) {
+  const NearTcPlan &p = dp.ntc;
+  return NearTcArgs{p.ctas, p.targets, p.tiles, p.pairs, p.slot_q, p.tabB, dp.split.err, dp.nd, dp.n, p.nctas,
+                    dp.split.wait_iters ? dp.split.wait_iters : kNtWaitIters, elem_off};
+}
+
+void near_tc_launch(int n, int grid, size_t smem, cudaStream_t s, const NearTcLaunch &lp) {
+  if (grid <= 0) return;
+  if (n == 16)
+    k_near_tc<16><<<grid, kNtThreads, smem, s>>>(lp);
+  else
+    k_near_tc<8><<<grid, kNtThreads, smem, s>>>(lp);
+}
+
+}  // namespace bfgt

@@ -39,8 +39,7 @@ struct SplitPlan {
 // Tensor-core near field of a split plan (near_tc.cuh); empty when the FP64
 // near-field kernel serves the plan.
 struct NearTcPlan {
-  int4 *ctas = nullptr, *tiles = nullptr;
-  int2 *pairs = nullptr;
+  int4 *ctas = nullptr, *tiles = nullptr, *blocks = nullptr;
   int *targets = nullptr, *slot_q = nullptr;
   uint16_t *tabB = nullptr;
   int nctas = 0, maxslot = 0;

@@ -17,8 +17,11 @@ constexpr int kNtThreads = 128;                       // one thread per MMA row
 constexpr int kNtA = 128 * 16 * 2;                    // one BF16 slice of a 128 x 16 A operand
 constexpr int kNtB = 16 * 16 * 2;                     // one slice of a 16 x 16 B operand
 constexpr int kNtTab = 3 * kNtB / 2;                  // uint16 per table slot (3 slices)
-constexpr size_t kNtFixed = 3 * kNtA + 3 * kNtB;      // operand buffers
-constexpr size_t kNtMinSmem = 29 * 1024;              // at most 7 CTAs per SM: 7 x 64 TMEM columns fit
+constexpr int kTG = 1;                                // tiles (slots) per MMA round
+constexpr size_t kNtFixed = kTG * 3 * (kNtA + kNtB);  // operand buffers
+constexpr int kColB = 32 * kTG;                       // TMEM column of stage B's accumulators
+constexpr int kTmemCols = kTG == 1 ? 64 : 128;        // 32 columns per stage-A tile of a round and stage B
+constexpr size_t kNtMinSmem = kTG == 1 ? 29 * 1024 : 46 * 1024;  // CTAs per SM x kTmemCols <= 512
 constexpr uint32_t kNtWaitIters = 1u << 26;
 
 // host copy of tc::kmajor_off
@@ -107,15 +110,28 @@ __device__ __forceinline__ void near_mmas(uint32_t d0, uint32_t d1, uint32_t aA,
   tc::mma_bf16(d1, ad[2], bd[0], idesc, 1u);
 }
 
-// One CTA: up to 128/kN targets; per density, stage A over the CTA's pair
-// tiles into Q (shared memory), then stage B over the slots into pot.
-// TMEM: D0, D1 of stage A in columns 0-31, of stage B in 32-63.
+// One CTA: up to 128/kN targets; per density, stage A over the CTA's block
+// tiles into Q (shared memory), then stage B over the slots into pot.  Both
+// stages take kTG tiles (slots) per round: their operands side by side in
+// shared memory, their MMAs issued together under one commit, so that a
+// round's loads are all in flight at once and the round trip (barrier, MMA,
+// wait) is paid once per kTG tiles.  TMEM: tile g of a stage-A round in
+// columns 32 g .. 32 g + 31 (D0, D1), stage B in the 32 after them.  One
+// tile per round measured fastest on the regime-C benchmark tree (0.48 ms):
+// rounds of 3 tiles cut the CTAs per SM from 5 to 3 (0.52 ms), and so did a
+// cp.async staging of the next tile's rows during the MMAs (17 KB of shared
+// memory more: 0.52 ms).  The kernel is bound by the latency of its rounds,
+// and resident CTAs hide it best.  Q is
+// [target][slot][k2][j1], rows of kN + 1 floats: the stage-A adds (fixed k2,
+// consecutive j1 across threads) and the stage-B reads (fixed j1, consecutive
+// k2) are both free of bank conflicts.
 template <int kN>
 __global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ NearTcLaunch lp) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t mbar[2];  // MMA groups; the final drain
+  __shared__ __align__(8) uint64_t mbar[2];  // MMA rounds; the final drain
   __shared__ uint32_t tmem_slot;
-  constexpr int kG = 128 / kN;  // pairs per stage-A tile, targets per CTA
+  constexpr int kG = 128 / kN;  // blocks per stage-A tile, targets per CTA
+  constexpr int kQr = kN + 1;   // Q row stride
   const NearTcArgs &a = lp.descs ? lp.descs[lp.work[blockIdx.x].x] : lp.one;
   const int cta = lp.descs ? lp.work[blockIdx.x].y : (int)blockIdx.x;
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -124,21 +140,21 @@ __global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ 
   const int nd = a.nd, npb = kN * kN;
   const double *fv = lp.fbase + a.elem_off;
   double *pot = lp.pbase + a.elem_off;
-  unsigned char *sA = smem;
-  unsigned char *sB = smem + 3 * kNtA;
-  float *sQ = reinterpret_cast<float *>(smem + kNtFixed);  // [tl][slot][j1][k2]
-  const int qsz = kG * nslot * npb;
+  unsigned char *sA = smem;                                // kTG x 3 slices
+  unsigned char *sB = smem + kTG * 3 * kNtA;               // kTG x 3 slices
+  float *sQ = reinterpret_cast<float *>(smem + kNtFixed);  // [tl][slot][k2][j1]
+  const int qsz = kG * nslot * kN * kQr;
 
-  if (warp == 0) tc::tmem_alloc(&tmem_slot, 64);
+  if (warp == 0) tc::tmem_alloc(&tmem_slot, kTmemCols);
   if (tid == 0) {
     tc::mbar_init(&mbar[0], 1);
     tc::mbar_init(&mbar[1], 1);
     tc::fence_mbar_init();
   }
-  // kN = 8: the K columns 8-15 of A are zero for the whole kernel
+  // kN = 8: the K columns 8-15 of every A buffer are zero for the whole kernel
   if (kN == 8) {
     const float z[16] = {};
-    store_row16(sA, tid, z);
+    for (int g = 0; g < kTG; g++) store_row16(sA + g * 3 * kNtA, tid, z);
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -148,33 +164,64 @@ __global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ 
   const uint32_t aA = tc::smem_u32(sA), aB = tc::smem_u32(sB);
   bool ok = true;
   uint32_t phase = 0;
-  // stage-A row: pair i of the tile, grid index j1; stage-B row: target tl, k2
+  // stage-A row: block i of a tile, grid index j1; stage-B row: target tl, k2
   const int ri = tid / kN, rj = tid % kN;
   const int *slot_q = a.slot_q + (size_t)cta * kNearTcSlots;
+  auto round_trip = [&](int nmma_groups, auto &&issue) {
+    tc::cp_async_wait_all();
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (tid == 0 && ok) {
+      for (int g = 0; g < nmma_groups; g++) issue(g);
+      tc::commit(&mbar[0]);
+    }
+    if (ok && !tc::mbar_wait(&mbar[0], phase & 1, a.wait_iters)) {
+      ok = false;
+      atomicExch(a.err, 1);
+    }
+    phase++;
+    tc::fence_after_sync();
+  };
 
   for (int ind = 0; ind < nd; ind++) {
     for (int e = tid; e < qsz; e += kNtThreads) sQ[e] = 0.0f;
     __syncthreads();
-    for (int t = c.x; t < c.y; t++) {
-      const int4 T = a.tiles[t];
-      const uint16_t *tb = a.tabB + (size_t)T.x * kNtTab;
-      for (int u = tid; u < 3 * kNtB / 16; u += kNtThreads) tc::cp_async16(sB + 16 * u, tb + 8 * u);
-      tc::cp_async_commit();
-      const int2 pr = ri < T.z ? a.pairs[T.y + ri] : make_int2(-1, 0);
-      if (pr.x >= 0) {
-        // F(j1 = rj, j2), j2 = 0..kN-1, of the source (fvals(nd, kN, kN, box), x fastest)
-        const double *src = fv + (size_t)pr.x * nd * npb + ind + (size_t)nd * rj;
-        float v[16];
+    for (int t0 = c.x; t0 < c.y; t0 += kTG) {
+      const int ng = min(kTG, c.y - t0);
+      int4 bk[kTG];
 #pragma unroll
-        for (int j2 = 0; j2 < 16; j2++) v[j2] = j2 < kN ? __double2float_rn(src[(size_t)nd * kN * j2]) : 0.0f;
+      for (int g = 0; g < kTG; g++) {
+        bk[g] = make_int4(-1, 0, 0, 0);
+        if (g < ng) {
+          const int4 T = a.tiles[t0 + g];
+          const uint16_t *tb = a.tabB + (size_t)T.x * kNtTab;
+          for (int u = tid; u < 3 * kNtB / 16; u += kNtThreads) tc::cp_async16(sB + g * 3 * kNtB + 16 * u, tb + 8 * u);
+          if (ri < T.z) bk[g] = a.blocks[T.y + ri];
+        }
+      }
+      tc::cp_async_commit();
+      // F(j1 = rj, j2) of each tile's block, all loads issued before any use
+      float v[kTG][16];
+#pragma unroll
+      for (int g = 0; g < kTG; g++) {
+        const double *src = fv + (size_t)(bk[g].x >= 0 ? bk[g].x : 0) * nd * npb + ind + (size_t)nd * rj;
+#pragma unroll
+        for (int j2 = 0; j2 < 16; j2++)
+          v[g][j2] = (bk[g].x >= 0 && j2 < kN) ? __double2float_rn(src[(size_t)nd * kN * j2]) : 0.0f;
+      }
+#pragma unroll
+      for (int g = 0; g < kTG; g++) {
+        if (bk[g].x < 0) continue;
         if (kN == 16) {
-          store_row16(sA, tid, v);
+          store_row16(sA + g * 3 * kNtA, tid, v[g]);
         } else {
           // only the first 8 K columns of the row (the rest stay zero)
           uint32_t p[3][4];
 #pragma unroll
           for (int q = 0; q < 4; q++) {
-            const float a0 = v[2 * q], a1 = v[2 * q + 1];
+            const float a0 = v[g][2 * q], a1 = v[g][2 * q + 1];
             const float h0 = tc::bf16_hi(a0), h1 = tc::bf16_hi(a1);
             const float r0 = a0 - h0, r1 = a1 - h1;
             const float m0 = tc::bf16_hi(r0), m1 = tc::bf16_hi(r1);
@@ -186,87 +233,74 @@ __global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ 
           const uint32_t o = tc::kmajor_off(tid, 0, 128);
 #pragma unroll
           for (int cc = 0; cc < 3; cc++)
-            *reinterpret_cast<uint4 *>(sA + cc * kNtA + o) = make_uint4(p[cc][0], p[cc][1], p[cc][2], p[cc][3]);
+            *reinterpret_cast<uint4 *>(sA + g * 3 * kNtA + cc * kNtA + o) = make_uint4(p[cc][0], p[cc][1], p[cc][2], p[cc][3]);
         }
       }
-      tc::cp_async_wait_all();
-      tc::fence_async_smem();
-      tc::fence_before_sync();
-      __syncthreads();
-      tc::fence_after_sync();
-      if (tid == 0 && ok) {
-        near_mmas(tmem, tmem + 16, aA, aB, 0u);
-        tc::commit(&mbar[0]);
-      }
-      if (ok && !tc::mbar_wait(&mbar[0], phase & 1, a.wait_iters)) {
-        ok = false;
-        atomicExch(a.err, 1);
-      }
-      phase++;
-      tc::fence_after_sync();
-      float d0[16], d1[16];
-      if (kN == 16) {
-        tc::tmem_ld16(tmem + lane_base, d0);
-        tc::tmem_ld16(tmem + lane_base + 16, d1);
-      } else {
-        tc::tmem_ld8(tmem + lane_base, d0);
-        tc::tmem_ld8(tmem + lane_base + 16, d1);
-      }
-      tc::tmem_ld_wait();
-      if (pr.x >= 0 && ok) {
-        const int tl = pr.y & 0xFF, slot = pr.y >> 8;
-        float *q = sQ + ((size_t)(tl * nslot + slot) * kN + rj) * kN;
+      round_trip(ng, [&](int g) {
+        near_mmas(tmem + 32 * g, tmem + 32 * g + 16, aA + g * 3 * kNtA, aB + g * 3 * kNtB, 0u);
+      });
+      // G rows (block, j1 = rj) -> Q(t, slot, k2, j1) of each pair they serve,
+      // tile after tile (two tiles of a round may serve the same Q rows), 8
+      // columns at a time
+      for (int g = 0; g < ng; g++) {
+        if (g > 0) __syncthreads();
 #pragma unroll
-        for (int k2 = 0; k2 < kN; k2++) q[k2] += d0[k2] + d1[k2];
+        for (int h = 0; h < kN; h += 8) {
+          float d0[8], d1[8];
+          tc::tmem_ld8(tmem + lane_base + 32 * g + h, d0);
+          tc::tmem_ld8(tmem + lane_base + 32 * g + 16 + h, d1);
+          tc::tmem_ld_wait();
+          if (bk[g].x >= 0 && ok) {
+#pragma unroll
+            for (int k2 = 0; k2 < 8; k2++) d0[k2] += d1[k2];
+            for (int u = 0; u < bk[g].w; u++) {
+              const int cs = ((u < 2 ? bk[g].y : bk[g].z) >> (16 * (u & 1))) & 0xFFFF;
+              const int tl = cs & 0xFF, slot = cs >> 8;
+              float *q = sQ + (size_t)(tl * nslot + slot) * kN * kQr + rj;
+#pragma unroll
+              for (int k2 = 0; k2 < 8; k2++) q[(size_t)(h + k2) * kQr] += d0[k2];
+            }
+          }
+        }
       }
       tc::fence_before_sync();
       __syncthreads();
     }
-    // stage B: one K block per slot, accumulated in TMEM columns 32-63
-    for (int sl = 0; sl < nslot; sl++) {
-      const uint16_t *tb = a.tabB + (size_t)slot_q[sl] * kNtTab;
-      for (int u = tid; u < 3 * kNtB / 16; u += kNtThreads) tc::cp_async16(sB + 16 * u, tb + 8 * u);
+    // stage B: one K block per slot, kTG slots per round, accumulated in
+    // TMEM columns kColB ..
+    for (int s0 = 0; s0 < nslot; s0 += kTG) {
+      const int ns = min(kTG, nslot - s0);
+      for (int g = 0; g < ns; g++) {
+        const uint16_t *tb = a.tabB + (size_t)slot_q[s0 + g] * kNtTab;
+        for (int u = tid; u < 3 * kNtB / 16; u += kNtThreads) tc::cp_async16(sB + g * 3 * kNtB + 16 * u, tb + 8 * u);
+      }
       tc::cp_async_commit();
-      {
-        // A row (tl = ri, k2 = rj): Q(tl, slot, j1, k2) over j1
-        const float *q = sQ + (size_t)(ri * nslot + sl) * npb + rj;
+      for (int g = 0; g < ns; g++) {
+        // A row (tl = ri, k2 = rj): Q(tl, slot, k2, j1) over j1
+        const float *q = sQ + ((size_t)(ri * nslot + s0 + g) * kN + rj) * kQr;
         float v[16];
 #pragma unroll
-        for (int j1 = 0; j1 < 16; j1++) v[j1] = j1 < kN ? q[(size_t)kN * j1] : 0.0f;
-        store_row16(sA, tid, v);
+        for (int j1 = 0; j1 < 16; j1++) v[j1] = j1 < kN ? q[j1] : 0.0f;
+        store_row16(sA + g * 3 * kNtA, tid, v);
       }
-      tc::cp_async_wait_all();
-      tc::fence_async_smem();
-      tc::fence_before_sync();
-      __syncthreads();
-      tc::fence_after_sync();
-      if (tid == 0 && ok) {
-        near_mmas(tmem + 32, tmem + 48, aA, aB, sl > 0 ? 1u : 0u);
-        tc::commit(&mbar[0]);
-      }
-      if (ok && !tc::mbar_wait(&mbar[0], phase & 1, a.wait_iters)) {
-        ok = false;
-        atomicExch(a.err, 1);
-      }
-      phase++;
-      tc::fence_after_sync();
-      __syncthreads();  // every thread has read its Q row and the MMA is done: sA, sB are free
+      round_trip(ns, [&](int g) {
+        near_mmas(tmem + kColB, tmem + kColB + 16, aA + g * 3 * kNtA, aB + g * 3 * kNtB, s0 + g > 0 ? 1u : 0u);
+      });
+      __syncthreads();  // every thread has read its Q rows and the MMAs are done: the buffers are free
     }
     if (nslot > 0) {
-      float d0[16], d1[16];
-      if (kN == 16) {
-        tc::tmem_ld16(tmem + lane_base + 32, d0);
-        tc::tmem_ld16(tmem + lane_base + 48, d1);
-      } else {
-        tc::tmem_ld8(tmem + lane_base + 32, d0);
-        tc::tmem_ld8(tmem + lane_base + 48, d1);
-      }
-      tc::tmem_ld_wait();
-      if (ok && ri < ntarget) {
-        // pot(k1, k2 = rj) of target ri, k1 = 0..kN-1
-        double *pb = pot + (size_t)a.targets[c.z + ri] * nd * npb + ind + (size_t)nd * kN * rj;
+      // pot(k1, k2 = rj) of target ri, k1 = 0..kN-1, 8 at a time
+      double *pb = ri < ntarget ? pot + (size_t)a.targets[c.z + ri] * nd * npb + ind + (size_t)nd * kN * rj : nullptr;
 #pragma unroll
-        for (int k1 = 0; k1 < kN; k1++) pb[(size_t)nd * k1] += (double)d0[k1] + (double)d1[k1];
+      for (int h = 0; h < kN; h += 8) {
+        float d0[8], d1[8];
+        tc::tmem_ld8(tmem + lane_base + kColB + h, d0);
+        tc::tmem_ld8(tmem + lane_base + kColB + 16 + h, d1);
+        tc::tmem_ld_wait();
+        if (ok && pb) {
+#pragma unroll
+          for (int k1 = 0; k1 < 8; k1++) pb[(size_t)nd * (h + k1)] += (double)d0[k1] + (double)d1[k1];
+        }
       }
       tc::fence_before_sync();
       __syncthreads();
@@ -277,7 +311,7 @@ __global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ 
   if (!tc::mbar_wait(&mbar[1], 0, kNtWaitIters)) atomicExch(a.err, 2);
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 64);
+  if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
 }
 
 }  // namespace
@@ -310,13 +344,17 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     }
   }
   // CTAs of up to kG targets whose entries use at most kNearTcSlots distinct
-  // x tables; entries with an empty table contribute nothing and are dropped
+  // x tables; entries with an empty table contribute nothing and are dropped.
+  // Within a CTA the pairs that share (source, y table) share one stage-A
+  // block (up to 4 pairs each); blocks are cut into tiles of kG that share the
+  // y table, and a block whose pairs meet one already in the tile (the same
+  // target and x slot) starts a new tile, so that no two rows of a tile add
+  // into the same Q rows.
   const int kG = 128 / n;
   struct Pair {
     int src, tl, slot, qy;
   };
-  std::vector<int4> ctas, tiles;
-  std::vector<int2> pairs;
+  std::vector<int4> ctas, tiles, blocks;
   std::vector<int> targets, slot_q;
   std::vector<Pair> cur;
   std::vector<int> cur_q, cur_t;
@@ -325,24 +363,46 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     if (cur_t.empty()) return;
     std::stable_sort(cur.begin(), cur.end(), [](const Pair &x, const Pair &y) {
       if (x.qy != y.qy) return x.qy < y.qy;
+      if (x.src != y.src) return x.src < y.src;
       if (x.tl != y.tl) return x.tl < y.tl;
       return x.slot < y.slot;
     });
+    // blocks: runs of equal (qy, src), at most 4 consumers each
+    struct Blk {
+      int qy, src, ncons, cons[4];
+    };
+    std::vector<Blk> bl;
+    for (size_t i = 0; i < cur.size(); i++) {
+      const int cs = cur[i].tl | (cur[i].slot << 8);
+      if (!bl.empty() && bl.back().qy == cur[i].qy && bl.back().src == cur[i].src && bl.back().ncons < 4) {
+        bl.back().cons[bl.back().ncons++] = cs;
+      } else {
+        bl.push_back(Blk{cur[i].qy, cur[i].src, 1, {cs, 0, 0, 0}});
+      }
+    }
     int4 c;
     c.x = (int)tiles.size();
     size_t i = 0;
-    while (i < cur.size()) {
+    while (i < bl.size()) {
+      const int begin = (int)blocks.size();
+      std::vector<int> seen;
       size_t j = i;
-      while (j < cur.size() && cur[j].qy == cur[i].qy && (int)(j - i) < kG) j++;
-      tiles.push_back(make_int4(cur[i].qy, (int)pairs.size(), (int)(j - i), 0));
-      for (size_t k = i; k < j; k++) pairs.push_back(make_int2(cur[k].src, cur[k].tl | (cur[k].slot << 8)));
+      for (; j < bl.size() && bl[j].qy == bl[i].qy && (int)(j - i) < kG; j++) {
+        bool clash = false;
+        for (int u = 0; u < bl[j].ncons; u++) clash = clash || std::find(seen.begin(), seen.end(), bl[j].cons[u]) != seen.end();
+        if (clash) break;
+        for (int u = 0; u < bl[j].ncons; u++) seen.push_back(bl[j].cons[u]);
+        const Blk &b = bl[j];
+        blocks.push_back(make_int4(b.src, b.cons[0] | (b.cons[1] << 16), b.cons[2] | (b.cons[3] << 16), b.ncons));
+      }
+      tiles.push_back(make_int4(bl[i].qy, begin, (int)(j - i), 0));
       i = j;
     }
     c.y = (int)tiles.size();
     c.z = (int)targets.size();
     c.w = (int)cur_t.size() | ((int)cur_q.size() << 8);
     targets.insert(targets.end(), cur_t.begin(), cur_t.end());
-    for (int s = 0; s < kNearTcSlots; s++) slot_q.push_back(s < (int)cur_q.size() ? cur_q[s] : 0);
+    for (int q = 0; q < kNearTcSlots; q++) slot_q.push_back(q < (int)cur_q.size() ? cur_q[q] : 0);
     maxslot = std::max(maxslot, (int)cur_q.size());
     ctas.push_back(c);
     cur.clear();
@@ -382,7 +442,7 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   };
   chk(upload_nt(p.ctas, ctas, msg));
   chk(upload_nt(p.tiles, tiles, msg));
-  chk(upload_nt(p.pairs, pairs, msg));
+  chk(upload_nt(p.blocks, blocks, msg));
   chk(upload_nt(p.targets, targets, msg));
   chk(upload_nt(p.slot_q, slot_q, msg));
   chk(upload_nt(p.tabB, tab, msg));
@@ -392,7 +452,7 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   }
   p.nctas = (int)ctas.size();
   p.maxslot = maxslot;
-  p.smem = std::max(kNtFixed + sizeof(float) * (size_t)kG * maxslot * n * n, kNtMinSmem);
+  p.smem = std::max(kNtFixed + sizeof(float) * (size_t)kG * maxslot * n * (n + 1), kNtMinSmem);
   const int smax = 227 * 1024 - 1024;
   if (p.smem > (size_t)smax) {
     near_tc_destroy(dp);
@@ -400,6 +460,10 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   }
   cudaFuncSetAttribute(k_near_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
   cudaFuncSetAttribute(k_near_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
+  // all of the unified L1 as shared memory: as many CTAs per SM as their
+  // shared memory allows
+  cudaFuncSetAttribute(k_near_tc<8>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  cudaFuncSetAttribute(k_near_tc<16>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (cudaGetLastError() != cudaSuccess) {
     msg = "CUDA error while preparing the tensor-core near field";
     near_tc_destroy(dp);
@@ -410,7 +474,7 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
 
 void near_tc_destroy(DevicePlan &dp) {
   NearTcPlan &p = dp.ntc;
-  void *ptrs[] = {p.ctas, p.tiles, p.pairs, p.targets, p.slot_q, p.tabB};
+  void *ptrs[] = {p.ctas, p.tiles, p.blocks, p.targets, p.slot_q, p.tabB};
   for (void *x : ptrs)
     if (x) cudaFree(x);
   p = NearTcPlan();
@@ -418,7 +482,7 @@ void near_tc_destroy(DevicePlan &dp) {
 
 NearTcArgs near_tc_args(const DevicePlan &dp, long long elem_off) {
   const NearTcPlan &p = dp.ntc;
-  return NearTcArgs{p.ctas, p.targets, p.tiles, p.pairs, p.slot_q, p.tabB, dp.split.err, dp.nd, dp.n, p.nctas,
+  return NearTcArgs{p.ctas, p.targets, p.tiles, p.blocks, p.slot_q, p.tabB, dp.split.err, dp.nd, dp.n, p.nctas,
                     dp.split.wait_iters ? dp.split.wait_iters : kNtWaitIters, elem_off};
 }
 

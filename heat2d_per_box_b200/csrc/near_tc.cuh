@@ -8,10 +8,12 @@
 // entries outside the band pattern set to zero (so exactly the reference's
 // banded sums), and the two contractions are tcgen05 MMAs (BF16 x 3 slices,
 // FP32 accumulators in TMEM), M = 128 rows:
-//   stage A (y):  G_p(j1,k2) = sum_j2 F_p(j1,j2) ty_p(j2,k2), rows (pair, j1),
-//                 a tile of 128/n pairs that share iy (one B operand);
-//   the rows are summed per (target, ix) into Q_{t,ix}(j1,k2) (FP32, shared
-//                 memory);
+//   stage A (y):  G_{s,iy}(j1,k2) = sum_j2 F_s(j1,j2) ty_iy(j2,k2), once per
+//                 (source, iy) of the CTA's pairs ("block"), rows (block, j1),
+//                 a tile of 128/n blocks that share iy (one B operand);
+//   each block row is added to Q_{t,ix}(j1,k2) of each pair (t, s) it serves
+//                 (FP32, shared memory): neighbouring targets share sources,
+//                 so a CTA has about a third as many blocks as pairs;
 //   stage B (x):  pot_t(k1,k2) += sum_ix sum_j1 tx_ix(j1,k1) Q_{t,ix}(j1,k2),
 //                 rows (target, k2), one K block of 16 per distinct ix ("slot")
 //                 of the CTA's 128/n targets.
@@ -31,8 +33,9 @@ constexpr int kNearTcSlots = 16;  // distinct x tables (slots) per CTA at most
 struct NearTcArgs {
   const int4 *ctas;      // {tile begin, tile end, target begin, ntarget | nslot << 8}
   const int *targets;    // target leaf boxes (0-based), CTA after CTA
-  const int4 *tiles;     // {table slot of ty, pair begin, pair count, 0}
-  const int2 *pairs;     // {source box, target (CTA-local) | slot << 8}
+  const int4 *tiles;     // {table slot of ty, block begin, block count, 0}
+  const int4 *blocks;    // {source box, consumers 0 | 1 << 16, 2 | 3 << 16, count};
+                         // a consumer is target (CTA-local) | x slot << 8
   const int *slot_q;     // kNearTcSlots per CTA: table slot of each x slot
   const uint16_t *tabB;  // per table slot: 3 BF16 slices of a 16 x 16 K-major B operand
   int *err;

@@ -55,25 +55,28 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// x (|x| <= 1) -> S fixed-point digits: v[c] = d_c 2^-(7+8c), d_c integer in
-// [-128, 128], x - sum v[c] below 2^-(8S) in magnitude.  Every step is exact
-// in FP64 (scaling by powers of two, and the remainder x - v[c] is a multiple
-// of the ulp of x no larger than x), and each v[c] has at most 8 significant
-// bits, so the conversions to FP32 and BF16 are exact.
+// x (|x| < 1) -> S fixed-point digits: v[c] = d_c 2^-(7+8c), d_c integer in
+// [-128, 128], x - sum v[c] at most half the last digit's unit, 2^-(8S), in
+// magnitude.  X = rint(x 2^(7 + 8 (S - 1))) is exact for S <= 6 (at most 47
+// bits; the scaling is by a power of two), the balanced base-256 digits are
+// cut from the least significant one up with integer operations (each
+// X - d is a multiple of 256), and the top digit keeps the rest.  Each v[c]
+// has at most 8 significant bits, so the conversions to FP32 and BF16 are
+// exact.
 __device__ __forceinline__ void fix_digits(double x, int S, float (&v)[kMaxSlices]) {
-  double sc = 128.0, isc = 1.0 / 128.0;
+  const int sh = 7 + 8 * (S - 1);
+  long long X = __double2ll_rn(x * __longlong_as_double((long long)(1023 + sh) << 52));
 #pragma unroll
-  for (int c = 0; c < kMaxSlices; c++) {
+  for (int c = kMaxSlices - 1; c >= 1; c--) {
     if (c < S) {
-      const double s = rint(x * sc) * isc;
-      v[c] = (float)s;
-      x -= s;
-      sc *= 256.0;
-      isc *= 1.0 / 256.0;
+      const int d = (int)((X + 128) & 255) - 128;
+      X = (X - d) >> 8;
+      v[c] = (float)d * __int_as_float((127 - 7 - 8 * c) << 23);
     } else {
       v[c] = 0.0f;
     }
   }
+  v[0] = (float)(int)X * (1.0f / 128.0f);
 }
 
 // power of two 2^e >= |mx| with mx / 2^e < 1, and its inverse.  Rows whose
@@ -303,6 +306,7 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
     double rsc = 1.0, rinv = 1.0;
     if constexpr (kFix) {
       double mx = 0.0;
+#pragma unroll 4
       for (int s2 = 0; s2 < nsteps; s2++) {
         const double *fv = leaf_row(s2);
         if (!fv) continue;

@@ -1104,6 +1104,16 @@ int device_plan_execute_pgh(DevicePlan &dp, int ifpgh, const double *d_fvals, do
       static const int ox[5] = {1, 0, 2, 1, 0}, oy[5] = {0, 1, 0, 1, 2};
       const int nslot = 13 * (dp.nlevels + 1);
       for (int c = 0; c < pt.nc; c++) {
+        if (dp.ntc.nctas > 0) {
+          // split plans: the tensor-core near field on the derivative tables
+          NearTcArgs ta = near_tc_args(dp, 0);
+          ta.out_nd = dp.nd * pt.nc;
+          ta.out_off = c * dp.nd;
+          ta.xoff = ox[pt.c0 + c] * nslot;
+          ta.yoff = oy[pt.c0 + c] * nslot;
+          near_tc_launch(dp.n, dp.ntc.nctas, dp.ntc.smem, s, NearTcLaunch{ta, nullptr, nullptr, d_fvals, pt.out});
+          continue;
+        }
         NearArgs na = near_args(dp, 0);
         na.tab_loc = dp.tab3_loc;
         na.out_nd = dp.nd * pt.nc;

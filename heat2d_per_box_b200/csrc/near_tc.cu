@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ 
         bk[g] = make_int4(-1, 0, 0, 0);
         if (g < ng) {
           const int4 T = a.tiles[t0 + g];
-          const uint16_t *tb = a.tabB + (size_t)T.x * kNtTab;
+          const uint16_t *tb = a.tabB + (size_t)(T.x + a.yoff) * kNtTab;
           for (int u = tid; u < 3 * kNtB / 16; u += kNtThreads) tc::cp_async16(sB + g * 3 * kNtB + 16 * u, tb + 8 * u);
           if (ri < T.z) bk[g] = a.blocks[T.y + ri];
         }
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ 
     for (int s0 = 0; s0 < nslot; s0 += kTG) {
       const int ns = min(kTG, nslot - s0);
       for (int g = 0; g < ns; g++) {
-        const uint16_t *tb = a.tabB + (size_t)slot_q[s0 + g] * kNtTab;
+        const uint16_t *tb = a.tabB + (size_t)(slot_q[s0 + g] + a.xoff) * kNtTab;
         for (int u = tid; u < 3 * kNtB / 16; u += kNtThreads) tc::cp_async16(sB + g * 3 * kNtB + 16 * u, tb + 8 * u);
       }
       tc::cp_async_commit();
@@ -290,7 +290,9 @@ __global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ 
     }
     if (nslot > 0) {
       // pot(k1, k2 = rj) of target ri, k1 = 0..kN-1, 8 at a time
-      double *pb = ri < ntarget ? pot + (size_t)a.targets[c.z + ri] * nd * npb + ind + (size_t)nd * kN * rj : nullptr;
+      double *pb = ri < ntarget ? pot + (size_t)a.targets[c.z + ri] * a.out_nd * npb + a.out_off + ind +
+                                      (size_t)a.out_nd * kN * rj
+                                : nullptr;
 #pragma unroll
       for (int h = 0; h < kN; h += 8) {
         float d0[8], d1[8];
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ 
         tc::tmem_ld_wait();
         if (ok && pb) {
 #pragma unroll
-          for (int k1 = 0; k1 < 8; k1++) pb[(size_t)nd * (h + k1)] += (double)d0[k1] + (double)d1[k1];
+          for (int k1 = 0; k1 < 8; k1++) pb[(size_t)a.out_nd * (h + k1)] += (double)d0[k1] + (double)d1[k1];
         }
       }
       tc::fence_before_sync();
@@ -324,22 +326,29 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   if ((int)hp.tab_loc.size() < n * n * nslots_tab || (int)hp.ind_loc.size() < 2 * (n + 1) * nslots_tab) return BFGT_OK;
   // the table operands: B(out k, in j) = tab_loc(j, k, slot) inside the band
   // pattern, 0 outside; slots whose band is empty are marked unused
-  std::vector<uint16_t> tab((size_t)nslots_tab * kNtTab, 0);
+  // three sets: values, and the first and second derivatives in the target
+  // coordinate (tabx_loc, tabxx_loc) for the gradient and Hessian outputs,
+  // all on the values' band pattern
+  const bool derivs = hp.tabx_loc.size() >= (size_t)n * n * nslots_tab && hp.tabxx_loc.size() >= (size_t)n * n * nslots_tab;
+  const std::vector<double> *sets[3] = {&hp.tab_loc, &hp.tabx_loc, &hp.tabxx_loc};
+  std::vector<uint16_t> tab((size_t)3 * nslots_tab * kNtTab, 0);
   std::vector<char> used(nslots_tab, 0);
   for (int q = 0; q < nslots_tab; q++) {
     const int *il = &hp.ind_loc[(size_t)2 * (n + 1) * q];
     const int k0 = il[2 * n], k1 = il[2 * n + 1];
     if (k1 - k0 + 1 <= 0) continue;
     used[q] = 1;
-    const double *t = &hp.tab_loc[(size_t)n * n * q];
-    uint16_t *dst = &tab[(size_t)q * kNtTab];
-    for (int k = k0 - 1; k < k1; k++) {
-      const int lo = il[2 * k], hi = il[2 * k + 1];
-      for (int j = lo - 1; j < hi; j++) {
-        uint16_t s[3];
-        split3_host(t[j + (size_t)n * k], s[0], s[1], s[2]);
-        const uint32_t o = kmajor_off_host(k, j, 16) / 2;
-        for (int cc = 0; cc < 3; cc++) dst[cc * (kNtB / 2) + o] = s[cc];
+    for (int set = 0; set < (derivs ? 3 : 1); set++) {
+      const double *t = &(*sets[set])[(size_t)n * n * q];
+      uint16_t *dst = &tab[((size_t)set * nslots_tab + q) * kNtTab];
+      for (int k = k0 - 1; k < k1; k++) {
+        const int lo = il[2 * k], hi = il[2 * k + 1];
+        for (int j = lo - 1; j < hi; j++) {
+          uint16_t s[3];
+          split3_host(t[j + (size_t)n * k], s[0], s[1], s[2]);
+          const uint32_t o = kmajor_off_host(k, j, 16) / 2;
+          for (int cc = 0; cc < 3; cc++) dst[cc * (kNtB / 2) + o] = s[cc];
+        }
       }
     }
   }
@@ -483,7 +492,7 @@ void near_tc_destroy(DevicePlan &dp) {
 NearTcArgs near_tc_args(const DevicePlan &dp, long long elem_off) {
   const NearTcPlan &p = dp.ntc;
   return NearTcArgs{p.ctas, p.targets, p.tiles, p.blocks, p.slot_q, p.tabB, dp.split.err, dp.nd, dp.n, p.nctas,
-                    dp.split.wait_iters ? dp.split.wait_iters : kNtWaitIters, elem_off};
+                    dp.split.wait_iters ? dp.split.wait_iters : kNtWaitIters, elem_off, dp.nd, 0, 0, 0};
 }
 
 void near_tc_launch(int n, int grid, size_t smem, cudaStream_t s, const NearTcLaunch &lp) {

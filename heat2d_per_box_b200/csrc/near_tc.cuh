@@ -37,11 +37,17 @@ struct NearTcArgs {
   const int4 *blocks;    // {source box, consumers 0 | 1 << 16, 2 | 3 << 16, count};
                          // a consumer is target (CTA-local) | x slot << 8
   const int *slot_q;     // kNearTcSlots per CTA: table slot of each x slot
-  const uint16_t *tabB;  // per table slot: 3 BF16 slices of a 16 x 16 K-major B operand
+  const uint16_t *tabB;  // per table slot: 3 BF16 slices of a 16 x 16 K-major B operand;
+                         // three sets (values, first, second derivatives in the
+                         // target coordinate), nslot_tab slots each
   int *err;
   int nd, n, nctas;
   uint32_t wait_iters;
   long long elem_off;  // start of this plan's leaf arrays in the (packed) fvals/pot
+  // out(out_nd, npbox, nboxes) += component out_off / nd of the transform
+  // (out_nd = nd ncomp); the x and y tables are read at slot + xoff / yoff
+  // (0: values, nslot_tab: first derivatives, 2 nslot_tab: second)
+  int out_nd, out_off, xoff, yoff;
 };
 
 // a single plan (descs null: CTA b is the plan's CTA b) or a batch (CTA b is
@@ -60,6 +66,8 @@ struct NearTcLaunch {
 int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);
 void near_tc_destroy(DevicePlan &dp);
 NearTcArgs near_tc_args(const DevicePlan &dp, long long elem_off);
+// table slots per derivative set (13 offsets per level)
+inline int near_tc_nslot(const DevicePlan &dp) { return 13 * (dp.nlevels + 1); }
 // one plan's near field, or (lp.descs set) grid CTAs of a batch
 void near_tc_launch(int n, int grid, size_t smem, cudaStream_t s, const NearTcLaunch &lp);
 

@@ -7,8 +7,10 @@ Manufactured solution u = sin(2 pi x) cos(2 pi y) exp(-t) (the reference's
 solver test hpots/test_forcing_adap1.f:86-112 uses the same field) with the
 source S = (8 pi^2 - 1) u + u^3 that makes u_t = Laplacian(u) + S - u^3 hold.
 dt = 1e-3, 200 steps, order-8 Legendre leaves on a uniform level-4 periodic
-tree.  The tree stays fixed: refinement and coarsening between steps are the
-solver's own tree work (vol_tree_adap_fv), which this library does not rebuild.
+tree, and at the configuration's size on an adaptive tree of 6,970 leaves
+(levels 6-8) refined around 10 Gaussians of width 0.02.  The tree stays fixed:
+refinement and coarsening between steps are the solver's own tree work
+(vol_tree_adap_fv), which this library does not rebuild.
 """
 import math
 
@@ -22,11 +24,19 @@ pytestmark = pytest.mark.gpu
 DT, NSTEPS = 1e-3, 200
 
 
-def setup(precision, eps):
+def c5_tree():
+    """Adaptive periodic order-8 tree of the configuration's size: refined to a
+    1e-10 tail around 10 Gaussians of width 0.02 (seed 5), levels 6 to 8."""
+    rng = np.random.default_rng(5)
+    g = hb.gauss_params(rng.uniform(-0.5, 0.5, (10, 2)), np.full(10, 0.02), np.ones(10))
+    return hb.build_adaptive(g, norder=8, ipoly=0, iperiod=1, eps=1e-10, minlev=6, maxlev=9)
+
+
+def setup(precision, eps, tree=None):
     import torch
     from heat_solver import HeatStepper
     g = hb.gauss_params(np.zeros((1, 2)), np.ones(1), np.zeros(1))
-    t = hb.build_uniform(4, g, norder=8, ipoly=0, iperiod=1)
+    t = hb.build_uniform(4, g, norder=8, ipoly=0, iperiod=1) if tree is None else tree
     lv = t.leaves()
     xy = t.grid_points(lv)
     A = np.zeros((t.nboxes, t.npbox))
@@ -53,9 +63,23 @@ def test_heat_stepping_matches_exact_solution(precision, tol):
     assert err < tol, err
 
 
-def test_heat_gradient_checkpointed_adjoint_vs_central_differences():
+@pytest.mark.parametrize("precision,tol", [(hb.BFGT_PREC_FP64, 1e-7), (hb.BFGT_PREC_SPLIT, 2e-5)])
+def test_heat_stepping_at_configuration_size(precision, tol):
+    t = c5_tree()
+    assert 4000 <= len(t.leaves()) <= 16000
+    st, A, hist = setup(precision, 1e-9 if precision == hb.BFGT_PREC_FP64 else 1e-6, tree=t)
+    uN = st.run(A.clone(), hist, NSTEPS)
+    st.batch.check()
+    exact = A * math.exp(-NSTEPS * DT)
+    err = (uN - exact).norm().item() / exact.norm().item()
+    st.close()
+    assert err < tol, err
+
+
+@pytest.mark.parametrize("size", ["level4", "c5"])
+def test_heat_gradient_checkpointed_adjoint_vs_central_differences(size):
     import torch
-    st, A, hist = setup(hb.BFGT_PREC_FP64, 1e-9)
+    st, A, hist = setup(hb.BFGT_PREC_FP64, 1e-9, tree=c5_tree() if size == "c5" else None)
     rng = np.random.default_rng(7)
     leaf = st.leaf.cpu().numpy()
     g = torch.from_numpy(0.5 * rng.standard_normal(leaf.size) * leaf).cuda()

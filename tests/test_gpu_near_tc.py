@@ -77,3 +77,27 @@ def test_fixed_point_plans_keep_the_fp64_near_field(trees):
     ref = oracle.boxfgt(t, t.fvals, 1e-5, 1e-9).reshape(t.nboxes, -1)[lv]
     assert rel_l2(p.reshape(t.nboxes, -1)[lv], ref) < 1e-8
     np.testing.assert_array_equal(p, q)  # regime C: only the near field, and it is the FP64 kernel
+
+
+@pytest.mark.parametrize("name,delta", [("ad_leg_per", 1e-5), ("ad16_leg_per", 1e-5), ("uni3_leg_free", 1e-5)])
+def test_gradient_and_hessian_near_field_on_tensor_cores(trees, name, delta):
+    """ifpgh = 3 in regime C: the derivative tables (tabx_loc, tabxx_loc) through
+    the same tensor-core kernel, within min(2e-6, 20 eps) of the oracle's
+    g2d_tens_prod_to_pghloc restatement."""
+    import torch
+    t = trees[name]
+    lv = t.leaves()
+    eps = 1e-6
+    plan = hb.Plan(t, delta, eps, precision=hb.BFGT_PREC_SPLIT)
+    f = torch.from_numpy(t.fvals.reshape(-1)).cuda()
+    p = torch.zeros_like(f)
+    g = torch.zeros(2 * f.numel(), dtype=torch.float64, device="cuda")
+    h = torch.zeros(3 * f.numel(), dtype=torch.float64, device="cuda")
+    plan.execute_pgh(3, f, p, g, h)
+    plan.check()
+    plan.close()
+    rp, rg, rh = oracle.boxfgt_pgh(t, t.fvals, delta, eps, 3)
+    leaf = lambda v: v.reshape(t.nboxes, -1)[lv]  # noqa: E731
+    assert rel_l2(leaf(p.cpu().numpy()), leaf(rp)) < 1e-6
+    assert rel_l2(leaf(g.cpu().numpy()), leaf(rg)) < 2e-6
+    assert rel_l2(leaf(h.cpu().numpy()), leaf(rh)) < 2e-6

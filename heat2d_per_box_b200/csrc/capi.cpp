@@ -463,7 +463,7 @@ int bfgt_plan_info(bfgt_plan plan, int *out) {
   // split kernels' shapes in use (100 eval step group + 10 x tiles per form
   // thread + 1 if the form kernel stages Y as float2), 0 for FP64 plans
   const bfgt::SplitPlan &sp = plan->dp.split;
-  out[15] = f64 ? 0 : 100 * sp.ebatch + 10 * sp.nt + (sp.yfloat ? 1 : 0);
+  out[15] = f64 ? 0 : 1000 * (sp.ehalf ? 1 : 0) + 100 * sp.ebatch + 10 * sp.nt + (sp.yfloat ? 1 : 0);
   return BFGT_OK;
 }
 

@@ -27,6 +27,14 @@ struct SplitPlan {
   int nitems = 0, items_nd = 0;  // items_nd: the density count the passes were cut for
   int4 *chunks = nullptr;
   int *step_begin = nullptr, *steps = nullptr;
+  // the eval kernel's alternative work: every column group of the chunks cut
+  // into two halves (twice the CTAs, each with half the rows); used when
+  // ehalf is set (the autotuner's choice), else the eval runs the chunks
+  int4 *echunks = nullptr;
+  int *estep_begin = nullptr, *esteps = nullptr;
+  int2 *eitems = nullptr;
+  int nechunks = 0, neitems = 0;
+  bool ehalf = false;
   uint16_t *TyB = nullptr, *EyB = nullptr;
   long long *tyb_off = nullptr, *eyb_off = nullptr;
   long long tyb_tile = 0, eyb_tile = 0;

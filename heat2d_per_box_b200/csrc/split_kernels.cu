@@ -6,6 +6,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -213,41 +214,41 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     }
     groups.swap(g2);
   }
-  // chunks (one per group) and their oy steps
-  std::vector<int4> chunks;
-  std::vector<int> step_begin(1, 0), steps;
-  for (const auto &gr : groups) {
-    const size_t c = gr.first, e = gr.second;
-    chunks.push_back(make_int4((int)c, (int)e, cols[c].icut, cols[c].level));
-    std::vector<size_t> ptr(e - c);
-    for (size_t q = c; q < e; q++) ptr[q - c] = cols[q].begin;
-    for (;;) {
-      int oy = INT32_MAX;
-      for (size_t q = c; q < e; q++)
-        if (ptr[q - c] < (size_t)cols[q].end) oy = std::min(oy, hp.leaves[ptr[q - c]].oy);
-      if (oy == INT32_MAX) break;
-      steps.push_back(oy);
-      for (int slot = 0; slot < sp.cpc; slot++) {
-        size_t q = c + slot;
-        if (q < e && ptr[slot] < (size_t)cols[q].end && hp.leaves[ptr[slot]].oy == oy) {
-          steps.push_back(hp.leaves[ptr[slot]].box);
-          ptr[slot]++;
-        } else {
-          steps.push_back(-1);
-        }
-      }
-    }
-    step_begin.push_back((int)(steps.size() / (1 + sp.cpc)));
-  }
-  // A plan with few, long chunks (a coarse cutoff level: one cutoff box at
-  // delta = 1e-2 on an order-16 tree gives 35 chunks of up to 256 steps)
-  // would leave most SMs idle.  When the chunks fill less than a quarter of
-  // the form kernel's CTA slots, chunks of more than kLongChunkSteps steps
-  // are cut into step ranges of about (total steps) / (slots), at least
-  // kMinPieceSteps: each piece is a chunk of the same columns.  The form kernel's x contraction and the eval
+  // chunks (one per group) and their oy steps.  A plan with few, long
+  // chunks (a coarse cutoff level: one cutoff box at delta = 1e-2 on an
+  // order-16 tree gives 35 chunks of up to 256 steps) would leave most SMs
+  // idle.  When the chunks fill less than a quarter of the form kernel's CTA
+  // slots, chunks of more than kLongChunkSteps steps are cut into step ranges
+  // of about (total steps) / (slots), at least kMinPieceSteps: each piece is a
+  // chunk of the same columns.  The form kernel's x contraction and the eval
   // kernel's H are then done once per piece; the partial expansions of the
   // pieces are summed by the same reduction as those of separate chunks.
-  {
+  auto make_chunks = [&](const std::vector<std::pair<size_t, size_t>> &grs, std::vector<int4> &chunks,
+                         std::vector<int> &step_begin, std::vector<int> &steps) {
+    step_begin.assign(1, 0);
+    for (const auto &gr : grs) {
+      const size_t c = gr.first, e = gr.second;
+      chunks.push_back(make_int4((int)c, (int)e, cols[c].icut, cols[c].level));
+      std::vector<size_t> ptr(e - c);
+      for (size_t q = c; q < e; q++) ptr[q - c] = cols[q].begin;
+      for (;;) {
+        int oy = INT32_MAX;
+        for (size_t q = c; q < e; q++)
+          if (ptr[q - c] < (size_t)cols[q].end) oy = std::min(oy, hp.leaves[ptr[q - c]].oy);
+        if (oy == INT32_MAX) break;
+        steps.push_back(oy);
+        for (int slot = 0; slot < sp.cpc; slot++) {
+          size_t q = c + slot;
+          if (q < e && ptr[slot] < (size_t)cols[q].end && hp.leaves[ptr[slot]].oy == oy) {
+            steps.push_back(hp.leaves[ptr[slot]].box);
+            ptr[slot]++;
+          } else {
+            steps.push_back(-1);
+          }
+        }
+      }
+      step_begin.push_back((int)(steps.size() / (1 + sp.cpc)));
+    }
     const int nch = (int)chunks.size(), total = step_begin.back();
     if (nch > 0 && 4 * nch <= slots) {
       const int smax = std::max(kMinPieceSteps, (total + slots - 1) / slots);
@@ -264,6 +265,26 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
       chunks.swap(pc);
       step_begin.swap(pb);
     }
+  };
+  std::vector<int4> chunks, echunks;
+  std::vector<int> step_begin, steps, estep_begin, esteps;
+  make_chunks(groups, chunks, step_begin, steps);
+  {
+    // the eval kernel's alternative: each group of two or more columns in halves
+    std::vector<std::pair<size_t, size_t>> halves;
+    bool any = false;
+    for (const auto &gr : groups) {
+      const size_t nc = gr.second - gr.first;
+      if (nc >= 2) {
+        const size_t mid = gr.first + (nc + 1) / 2;
+        halves.emplace_back(gr.first, mid);
+        halves.emplace_back(mid, gr.second);
+        any = true;
+      } else {
+        halves.push_back(gr);
+      }
+    }
+    if (any) make_chunks(halves, echunks, estep_begin, esteps);
   }
   // Fixed-point slices: a form CTA accumulates n K-terms per step into the
   // same TMEM rows; chunks with more than kFixMaxTerms / n steps are cut into
@@ -378,6 +399,25 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   chk(upload_vec(sp.chunks, chunks, msg));
   chk(upload_vec(sp.step_begin, step_begin, msg));
   chk(upload_vec(sp.steps, steps, msg));
+  if (!echunks.empty()) {
+    chk(upload_vec(sp.echunks, echunks, msg));
+    chk(upload_vec(sp.estep_begin, estep_begin, msg));
+    chk(upload_vec(sp.esteps, esteps, msg));
+    sp.nechunks = (int)echunks.size();
+    if (dp.nd > 1) {
+      std::vector<int2> items;
+      for (size_t c = 0; c < echunks.size(); c++) {
+        const int rpd = (echunks[c].y - echunks[c].x) * n;
+        const int dpc = std::max(std::min(dp.nd, kRows / rpd), 1);
+        for (int p = 0; p < (dp.nd + dpc - 1) / dpc; p++) items.push_back(make_int2((int)c, p));
+      }
+      chk(upload_vec(sp.eitems, items, msg));
+      sp.neitems = (int)items.size();
+    }
+    // (tests) BFGT_SPLIT_EVAL_HALVES=1: the eval kernel starts on the halves
+    const char *ev = std::getenv("BFGT_SPLIT_EVAL_HALVES");
+    sp.ehalf = ev && std::atoi(ev) == 1;
+  }
   chk(upload_vec(sp.TyB, TyB, msg));
   chk(upload_vec(sp.EyB, EyB, msg));
   chk(upload_vec(sp.tyb_off, tyoff, msg));
@@ -456,7 +496,8 @@ int split_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
 
 void split_plan_destroy(DevicePlan &dp) {
   SplitPlan &sp = dp.split;
-  void *ptrs[] = {sp.chunks, sp.step_begin, sp.steps, sp.TyB, sp.EyB, sp.tyb_off, sp.eyb_off, sp.err, sp.items,
+  void *ptrs[] = {sp.chunks, sp.step_begin, sp.steps, sp.echunks, sp.estep_begin, sp.esteps, sp.eitems,
+                  sp.TyB, sp.EyB, sp.tyb_off, sp.eyb_off, sp.err, sp.items,
                   sp.csc, sp.esc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -472,6 +513,17 @@ const int2 *split_items(const DevicePlan &dp) {
   return dp.split.items && dp.nd == dp.split.items_nd ? dp.split.items : nullptr;
 }
 int split_ctas(const DevicePlan &dp) { return split_items(dp) ? dp.split.nitems : dp.split.nchunks; }
+// the eval kernel's work: the chunks, or their column halves (ehalf); items
+// of the halves exist for the plan's own density count, as the chunks' do
+bool eval_halves(const DevicePlan &dp) { return dp.split.ehalf && dp.split.nechunks > 0; }
+const int2 *eval_items(const DevicePlan &dp) {
+  if (!eval_halves(dp)) return split_items(dp);
+  return dp.split.eitems && dp.nd == dp.split.items_nd ? dp.split.eitems : nullptr;
+}
+int eval_ctas(const DevicePlan &dp) {
+  if (!eval_halves(dp)) return split_ctas(dp);
+  return eval_items(dp) ? dp.split.neitems : dp.split.nechunks;
+}
 
 FormTcArgs form_args(const DevicePlan &dp, long long elem_off) {
   const SplitPlan &sp = dp.split;
@@ -482,9 +534,11 @@ FormTcArgs form_args(const DevicePlan &dp, long long elem_off) {
 
 EvalTcArgs eval_args(const DevicePlan &dp, long long elem_off) {
   const SplitPlan &sp = dp.split;
-  return EvalTcArgs{sp.chunks, sp.step_begin, sp.steps, dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, dp.E, dp.PH,
-                    dp.ph_off, dp.L, sp.err, dp.nd, dp.n, dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH,
-                    sp.lslots, sp.ebatch, sp.wait_iters, elem_off, split_items(dp), sp.esc, sp.S, 0};
+  const bool h = eval_halves(dp);
+  return EvalTcArgs{h ? sp.echunks : sp.chunks, h ? sp.estep_begin : sp.step_begin, h ? sp.esteps : sp.steps,
+                    dp.columns, sp.EyB, sp.eyb_off, sp.eyb_tile, dp.E, dp.PH, dp.ph_off, dp.L, sp.err, dp.nd, dp.n,
+                    dp.npw, dp.hh, dp.nexp, sp.cpc, sp.NB, sp.KE, sp.KH, sp.lslots, sp.ebatch, sp.wait_iters,
+                    elem_off, eval_items(dp), sp.esc, sp.S, 0};
 }
 
 // variant: 0, 1 = unpacked with 1, 2 x-contraction tiles per thread (+2 with
@@ -518,7 +572,7 @@ void split_form(DevicePlan &dp, const double *d_fvals, cudaStream_t s) {
 
 void split_eval(DevicePlan &dp, double *d_pot, cudaStream_t s) {
   EvalTcLaunch lp{eval_args(dp, 0), nullptr, nullptr, d_pot};
-  launch_eval_any(eval_variant(dp), split_ctas(dp), dp.split.smem_eval, s, lp);
+  launch_eval_any(eval_variant(dp), eval_ctas(dp), dp.split.smem_eval, s, lp);
 }
 
 int split_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::string &msg) {
@@ -586,13 +640,20 @@ int split_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::string &
     set_eval_shape(t, dp.n, dp.npw, dp.hh, dp.nd, eb);
     if (t.smem_eval <= (size_t)kMaxDynSmem) ec.push_back(eb);
   }
+  // and, where the chunks have column halves, the halves (twice the CTAs)
   int be = sp.ebatch;
+  bool bh = sp.ehalf;
   double te = 1e30;
-  for (int eb : ec) {
-    set_eval_shape(sp, dp.n, dp.npw, dp.hh, dp.nd, eb);
-    const double ms = time_ms([&] { split_eval(dp, p, s); });
-    if (ms < te) te = ms, be = eb;
-  }
+  int ne = 0;
+  for (int half = 0; half < (sp.nechunks > 0 ? 2 : 1); half++)
+    for (int eb : ec) {
+      sp.ehalf = half != 0;
+      set_eval_shape(sp, dp.n, dp.npw, dp.hh, dp.nd, eb);
+      const double ms = time_ms([&] { split_eval(dp, p, s); });
+      ne++;
+      if (ms < te) te = ms, be = eb, bh = sp.ehalf;
+    }
+  sp.ehalf = bh;
   set_eval_shape(sp, dp.n, dp.npw, dp.hh, dp.nd, be);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -610,7 +671,7 @@ int split_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::string &
   report[0] = tf;
   report[1] = te;
   report[2] = (double)fc.size();
-  report[3] = (double)ec.size();
+  report[3] = (double)ne;
   return BFGT_OK;
 }
 
@@ -630,10 +691,8 @@ int split_batch_create(SplitBatch &b, const std::vector<DevicePlan *> &plans, co
     ed.push_back(eval_args(dp, offs[i]));
     if (dp.precision != BFGT_PREC_SPLIT || dp.direct_only) continue;
     const int fv = form_variant(dp), ev = eval_variant(dp);
-    for (int c = 0; c < split_ctas(dp); c++) {
-      fw[fv].push_back(make_int2((int)i, c));
-      ew[ev].push_back(make_int2((int)i, c));
-    }
+    for (int c = 0; c < split_ctas(dp); c++) fw[fv].push_back(make_int2((int)i, c));
+    for (int c = 0; c < eval_ctas(dp); c++) ew[ev].push_back(make_int2((int)i, c));
     fsm[fv] = std::max(fsm[fv], dp.split.smem_form);
     esm[ev] = std::max(esm[ev], dp.split.smem_eval);
   }

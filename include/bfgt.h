@@ -209,9 +209,10 @@ int bfgt_plan_reserve_events(bfgt_plan plan, int n);
    plane-wave chunks (CTAs of the form and eval kernels), out[12]=kernel
    launches per execute, out[13]/out[14]=FP64 form/eval tile shape in use
    (100 tm + 10 tn + tiles per lane; 0 for split plans), out[15]=split
-   kernel shapes in use (100 eval step group + 10 x-contraction tiles per form
-   thread + 1 when the form kernel stages Y as float2; 0 for FP64 plans).  out
-   must hold 16 ints. */
+   kernel shapes in use (1000 when the eval kernel runs the chunks' column
+   halves + 100 eval step group + 10 x-contraction tiles per form thread + 1
+   when the form kernel stages Y as float2; 0 for FP64 plans).  out must hold
+   16 ints. */
 int bfgt_plan_info(bfgt_plan plan, int *out);
 
 /* Algorithmic work of one execute (every real operation counted once, split
@@ -233,8 +234,8 @@ int bfgt_plan_work(bfgt_plan plan, double *out);
    fastest.  FP64 plans: the tile shapes, remembered for plans of the same
    (norder, npw, nd) created later in the process.  Split-precision plans: Y
    staged as float2 or double2 and 1 or 2 x-contraction tiles per thread in
-   the form kernel, step groups of 8, 4 or 2 in the eval kernel (for this plan
-   only).  FP64 shapes give the same sums to rounding, split shapes the same
+   the form kernel, step groups of 8, 4 or 2 and whole chunks or their column
+   halves in the eval kernel (for this plan only).  FP64 shapes give the same sums to rounding, split shapes the same
    bits.  report (may be NULL) receives
    the best form and eval ms per launch and the numbers of shapes timed.  A
    batch or a captured graph keeps the shapes its plans had when it was made:

@@ -72,3 +72,35 @@ def test_autotune_split_plan_same_bits(trees, name, delta, eps, nd):
     batch.close()
     base.close()
     plan.close()
+
+
+@pytest.mark.parametrize("name,delta,eps,nd", [("ad16_leg_per", 1e-4, 1e-6, 1), ("ad_leg_per", 1e-4, 1e-9, 1),
+                                               ("ad_leg_per", 1e-4, 1e-6, 3)])
+def test_eval_on_column_halves_same_bits(trees, monkeypatch, name, delta, eps, nd):
+    """The eval kernel on the chunks' column halves (an autotuner choice, forced
+    here through BFGT_SPLIT_EVAL_HALVES) gives the same bits, alone and in a
+    batch: each output row's H and MMAs do not depend on the other rows."""
+    import torch
+    t = trees[name]
+    f0 = np.repeat(t.fvals[:, :, None], nd, axis=2) * np.linspace(1.0, 2.0, nd)[None, None, :]
+    f = torch.from_numpy(np.ascontiguousarray(f0).reshape(-1)).cuda()
+    base = hb.Plan(t, delta, eps, nd=nd, precision=hb.BFGT_PREC_SPLIT)
+    p0 = torch.zeros_like(f)
+    base.execute(f, p0)
+    base.check()
+    assert base.info()["split_shape"] < 1000
+    monkeypatch.setenv("BFGT_SPLIT_EVAL_HALVES", "1")
+    plan = hb.Plan(t, delta, eps, nd=nd, precision=hb.BFGT_PREC_SPLIT)
+    assert plan.info()["split_shape"] >= 1000  # the halves are in use
+    p = torch.zeros_like(f)
+    plan.execute(f, p)
+    plan.check()
+    np.testing.assert_array_equal(p.cpu().numpy(), p0.cpu().numpy())
+    batch = hb.Batch([plan])
+    pb = torch.zeros_like(f)
+    batch.execute(f, pb)
+    batch.check()
+    np.testing.assert_array_equal(pb.cpu().numpy(), p0.cpu().numpy())
+    batch.close()
+    plan.close()
+    base.close()

@@ -22,7 +22,8 @@ void split_plan_destroy(DevicePlan &dp);
 // Times the plan's compiled shape choices on its own work lists (scratch
 // arrays; synchronous) and keeps the fastest: form with Y as float2 or
 // double2 and 1 or 2 x-contraction tiles per thread, eval with step groups of
-// 8, 4 or 2.  Every choice gives the same bits.  report: best form and eval
+// 8, 4 or 2 on the chunks or their column halves.  Every choice gives the
+// same bits.  report: best form and eval
 // ms per launch, and the numbers of choices timed.
 int split_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::string &msg);
 

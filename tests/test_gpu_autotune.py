@@ -3,8 +3,8 @@ shapes on the plan's own work lists, keeps the fastest, and later plans of the
 same (norder, npw, nd) start with it.  Results must not change beyond FP64
 rounding (every shape computes the same sums, 1e-11 against the oracle), and
 the caller's arrays are untouched.  Split plans: the form kernel's Y staging
-and x tiles and the eval kernel's step groups are timed; every choice gives
-the same bits as the untuned plan."""
+and x tiles and the eval kernel's step groups and work (chunks or their column
+halves) are timed; every choice gives the same bits as the untuned plan."""
 import numpy as np
 import pytest
 

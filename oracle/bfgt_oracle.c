@@ -40,6 +40,14 @@
  * Arrays use the reference's Fortran (column-major, 1-based) layout through
  * the index macros below, so the restatement can be read against the source.
  * Compile without -ffast-math and with -ffp-contract=off.
+ *
+ * Pin status: pinned to the reference's own known-answer test (the Fourier-
+ * mode eigenfunction of hpots/test_initpot.f:58-80, 239-250) and to a direct
+ * FP64 quadrature of the periodic Gaussian convolution (oracle/quad.py), both
+ * at 10 eps; its lists are also checked against their geometric definition
+ * (tests/test_lists_geometric.py).  Not pinned bit for bit against the
+ * reference's own discrete output: the reference is Fortran, and no Fortran
+ * compiler is available to build it.
  */
 #include <math.h>
 #include <stdint.h>

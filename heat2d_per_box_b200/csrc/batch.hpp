@@ -21,12 +21,12 @@ struct DeviceBatch {
   int2 *tr_work = nullptr, *nf_work = nullptr;    // {plan, block of the plan}
   int tr_blocks = 0, nf_blocks = 0;
   size_t smem_near = 0;
-  // tensor-core near field of split plans: per-plan arguments, {plan, CTA}
-  // work of the order-8 and order-16 plans
+  // block near-field kernels: per-plan arguments, {plan, CTA} work of the
+  // order-8 and order-16 plans on the tensor cores (0, 1) and in FP64 (2, 3)
   void *ntc_descs = nullptr;
-  int2 *ntc_work[2] = {nullptr, nullptr};
-  int ntc_blocks[2] = {0, 0};
-  size_t smem_ntc[2] = {0, 0};
+  int2 *ntc_work[4] = {nullptr, nullptr, nullptr, nullptr};
+  int ntc_blocks[4] = {0, 0, 0, 0};
+  size_t smem_ntc[4] = {0, 0, 0, 0};
   std::vector<std::array<cudaEvent_t, 6>> evsets;
   int nrec = 0;
   bool events = false;

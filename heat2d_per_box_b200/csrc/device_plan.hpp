@@ -49,7 +49,9 @@ struct SplitPlan {
 struct NearTcPlan {
   int4 *ctas = nullptr, *tiles = nullptr, *blocks = nullptr;
   int *targets = nullptr, *slot_q = nullptr;
-  uint16_t *tabB = nullptr;
+  uint16_t *tabB = nullptr;  // split plans: BF16 slices of the tables
+  double *tabD = nullptr;    // FP64 plans (and fixed-point split plans): the tables in FP64
+  bool fp64 = false;         // which of the two kernels runs the lists
   int nctas = 0, maxslot = 0;
   size_t smem = 0;
 };

@@ -877,6 +877,9 @@ int device_plan_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
         chk(upload(dp.split.err, zero, msg));
       }
       chk(near_tc_create(dp, hp, msg));
+    } else if (rc == BFGT_OK) {
+      // FP64 plans and fixed-point split plans: the same work lists on the FP64 pipes
+      chk(near_tc_create(dp, hp, msg, true));
     }
   }
   // the 227 KB per-block limit minus room for the kernels' static shared variables
@@ -1018,7 +1021,8 @@ int device_plan_execute(DevicePlan &dp, const double *d_fvals, double *d_pot, cu
     for (int i = 1; i <= 4; i++) cudaEventRecord(ev[i], s);
   }
   if (dp.ntc.nctas > 0)
-    near_tc_launch(dp.n, dp.ntc.nctas, dp.ntc.smem, s, NearTcLaunch{near_tc_args(dp, 0), nullptr, nullptr, d_fvals, d_pot});
+    (dp.ntc.fp64 ? near_f64_launch : near_tc_launch)(dp.n, dp.ntc.nctas, dp.ntc.smem, s,
+                                                      NearTcLaunch{near_tc_args(dp, 0), nullptr, nullptr, d_fvals, d_pot});
   else if (dp.nnf > 0)
     k_near_fp64<<<(dp.nnf + kWarps - 1) / kWarps, kWarps * 32, dp.smem_near, s>>>(
         NearLaunch{near_args(dp, 0), nullptr, nullptr, d_fvals, d_pot});
@@ -1105,13 +1109,14 @@ int device_plan_execute_pgh(DevicePlan &dp, int ifpgh, const double *d_fvals, do
       const int nslot = 13 * (dp.nlevels + 1);
       for (int c = 0; c < pt.nc; c++) {
         if (dp.ntc.nctas > 0) {
-          // split plans: the tensor-core near field on the derivative tables
+          // the block kernels (tensor cores or FP64) on the derivative tables
           NearTcArgs ta = near_tc_args(dp, 0);
           ta.out_nd = dp.nd * pt.nc;
           ta.out_off = c * dp.nd;
           ta.xoff = ox[pt.c0 + c] * nslot;
           ta.yoff = oy[pt.c0 + c] * nslot;
-          near_tc_launch(dp.n, dp.ntc.nctas, dp.ntc.smem, s, NearTcLaunch{ta, nullptr, nullptr, d_fvals, pt.out});
+          (dp.ntc.fp64 ? near_f64_launch : near_tc_launch)(dp.n, dp.ntc.nctas, dp.ntc.smem, s,
+                                                            NearTcLaunch{ta, nullptr, nullptr, d_fvals, pt.out});
           continue;
         }
         NearArgs na = near_args(dp, 0);
@@ -1324,7 +1329,7 @@ int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, 
   std::vector<TrArgs> tr;
   std::vector<NearArgs> nf;
   std::vector<NearTcArgs> ntc;
-  std::vector<int2> trw, nfw, ntw[2];
+  std::vector<int2> trw, nfw, ntw[4];
   for (size_t i = 0; i < plans.size(); i++) {
     const DevicePlan &dp = *plans[i];
     tr.push_back(tr_args(dp));
@@ -1335,8 +1340,9 @@ int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, 
     }
     ntc.push_back(near_tc_args(dp, b.offs[i]));
     if (dp.ntc.nctas > 0) {
-      // the tensor-core near field: one launch per order (8, 16)
-      const int v = dp.n == 16 ? 1 : 0;
+      // the block near-field kernels: one launch per kind (tensor cores,
+      // FP64) and order (8, 16)
+      const int v = (dp.n == 16 ? 1 : 0) + (dp.ntc.fp64 ? 2 : 0);
       for (int c = 0; c < dp.ntc.nctas; c++) ntw[v].push_back(make_int2((int)i, c));
       b.smem_ntc[v] = std::max(b.smem_ntc[v], dp.ntc.smem);
     } else {
@@ -1346,7 +1352,7 @@ int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, 
   }
   b.tr_blocks = (int)trw.size();
   b.nf_blocks = (int)nfw.size();
-  for (int v = 0; v < 2; v++) b.ntc_blocks[v] = (int)ntw[v].size();
+  for (int v = 0; v < 4; v++) b.ntc_blocks[v] = (int)ntw[v].size();
   TrArgs *dtr = nullptr;
   NearArgs *dnf = nullptr;
   NearTcArgs *dnt = nullptr;
@@ -1357,9 +1363,9 @@ int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, 
   chk(upload(dnf, nf, msg));
   chk(upload(b.tr_work, trw, msg));
   chk(upload(b.nf_work, nfw, msg));
-  if (b.ntc_blocks[0] + b.ntc_blocks[1] > 0) {
+  if (b.ntc_blocks[0] + b.ntc_blocks[1] + b.ntc_blocks[2] + b.ntc_blocks[3] > 0) {
     chk(upload(dnt, ntc, msg));
-    for (int v = 0; v < 2; v++) chk(upload(b.ntc_work[v], ntw[v], msg));
+    for (int v = 0; v < 4; v++) chk(upload(b.ntc_work[v], ntw[v], msg));
   }
   b.tr_descs = dtr;
   b.nf_descs = dnf;
@@ -1372,8 +1378,8 @@ int device_batch_create(DeviceBatch &b, const std::vector<DevicePlan *> &plans, 
 }
 
 int device_batch_launches(const DeviceBatch &b) {
-  int n = split_batch_launches(b.split) + (b.tr_blocks > 0) + (b.nf_blocks > 0) + (b.ntc_blocks[0] > 0) +
-          (b.ntc_blocks[1] > 0);
+  int n = split_batch_launches(b.split) + (b.tr_blocks > 0) + (b.nf_blocks > 0);
+  for (int v = 0; v < 4; v++) n += b.ntc_blocks[v] > 0;
   for (const DevicePlan *dp : b.plans)
     if (dp->precision != BFGT_PREC_SPLIT && has_pw(*dp)) n += 2;
   return n;
@@ -1398,11 +1404,11 @@ int device_batch_execute(DeviceBatch &b, const double *d_fvals, double *d_pot, c
   if (b.nf_blocks > 0)
     k_near_fp64<<<b.nf_blocks, kWarps * 32, b.smem_near, s>>>(
         NearLaunch{NearArgs{}, static_cast<const NearArgs *>(b.nf_descs), b.nf_work, d_fvals, d_pot});
-  for (int v = 0; v < 2; v++)
+  for (int v = 0; v < 4; v++)
     if (b.ntc_blocks[v] > 0)
-      near_tc_launch(v ? 16 : 8, b.ntc_blocks[v], b.smem_ntc[v], s,
-                     NearTcLaunch{NearTcArgs{}, static_cast<const NearTcArgs *>(b.ntc_descs), b.ntc_work[v], d_fvals,
-                                  d_pot});
+      ((v & 2) ? near_f64_launch : near_tc_launch)((v & 1) ? 16 : 8, b.ntc_blocks[v], b.smem_ntc[v], s,
+                                                   NearTcLaunch{NearTcArgs{}, static_cast<const NearTcArgs *>(b.ntc_descs),
+                                                                b.ntc_work[v], d_fvals, d_pot});
   if (ev) cudaEventRecord(ev[5], s);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -1418,7 +1424,8 @@ void device_batch_destroy(DeviceBatch &b) {
   if (b.graph_exec) cudaGraphExecDestroy(b.graph_exec);
   if (b.graph) cudaGraphDestroy(b.graph);
   split_batch_destroy(b.split);
-  void *ptrs[] = {b.tr_descs, b.nf_descs, b.tr_work, b.nf_work, b.ntc_descs, b.ntc_work[0], b.ntc_work[1]};
+  void *ptrs[] = {b.tr_descs,      b.nf_descs,      b.tr_work,       b.nf_work,      b.ntc_descs,
+                  b.ntc_work[0], b.ntc_work[1], b.ntc_work[2], b.ntc_work[3]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &es : b.evsets)

@@ -125,8 +125,10 @@ __device__ __forceinline__ void near_mmas(uint32_t d0, uint32_t d1, uint32_t aA,
 // [target][slot][k2][j1], rows of kN + 1 floats: the stage-A adds (fixed k2,
 // consecutive j1 across threads) and the stage-B reads (fixed j1, consecutive
 // k2) are both free of bank conflicts.
+// (at least 5 CTAs per SM: without the hint ptxas settles at 64 registers
+// with spills, 17% slower on the regime-C benchmark tree)
 template <int kN>
-__global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ NearTcLaunch lp) {
+__global__ void __launch_bounds__(kNtThreads, 5) k_near_tc(const __grid_constant__ NearTcLaunch lp) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar[2];  // MMA rounds; the final drain
   __shared__ uint32_t tmem_slot;
@@ -316,9 +318,120 @@ __global__ void __launch_bounds__(kNtThreads) k_near_tc(const __grid_constant__ 
   if (warp == 0) tc::tmem_dealloc(tmem, kTmemCols);
 }
 
+// The same CTA, tile and block lists on the FP64 pipes (FP64 plans and
+// fixed-point split plans).  Stage A: G_b = F_b ty for the tile's blocks
+// (shared memory, 4 x kN/4 output tiles per thread); stage B: each thread
+// adds tx_slot^T G_b for the pairs of its own target into a 4 x kN/4 tile of
+// that target's pot held in registers, so no Q is needed; pot is updated
+// once per density at the end.  Rows of kN + 1 doubles in shared memory.
+template <int kN>
+__global__ void __launch_bounds__(kNtThreads) k_near_f64(const __grid_constant__ NearTcLaunch lp) {
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ int4 s_blk[128 / kN];
+  constexpr int kG = 128 / kN, kS = kN + 1, kTN = kN / 4;
+  const NearTcArgs &a = lp.descs ? lp.descs[lp.work[blockIdx.x].x] : lp.one;
+  const int cta = lp.descs ? lp.work[blockIdx.x].y : (int)blockIdx.x;
+  const int tid = threadIdx.x;
+  const int4 c = a.ctas[cta];
+  const int ntarget = c.w & 0xFF, nslot = c.w >> 8;
+  const int nd = a.nd, npb = kN * kN;
+  const double *fv = lp.fbase + a.elem_off;
+  double *pot = lp.pbase + a.elem_off;
+  double *sF = dsm;                    // [block][j1][j2]
+  double *sG = sF + kG * kN * kS;      // [block][j1][k2]
+  double *sTY = sG + kG * kN * kS;     // [j2][k2]
+  double *sTX = sTY + kN * kS;         // [slot][j1][k1]
+  const int grp = tid / kN, sub = tid % kN;
+  const int ra = (sub / 4) * 4, ca = (sub % 4) * kTN;  // rows ra..ra+3, columns ca..ca+kTN-1
+  const int *slot_q = a.slot_q + (size_t)cta * kNearTcSlots;
+  for (int e = tid; e < nslot * npb; e += kNtThreads) {
+    const int sl = e / npb, r = e - sl * npb, j = r % kN, k = r / kN;
+    sTX[((size_t)sl * kN + j) * kS + k] = a.tabD[(size_t)(slot_q[sl] + a.xoff) * npb + r];
+  }
+  for (int ind = 0; ind < nd; ind++) {
+    double acc[4][kTN];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int u = 0; u < kTN; u++) acc[i][u] = 0.0;
+    for (int t = c.x; t < c.y; t++) {
+      const int4 T = a.tiles[t];
+      __syncthreads();  // the previous tile's shared data has been read
+      if (tid < T.z) s_blk[tid] = a.blocks[T.y + tid];
+      for (int e = tid; e < npb; e += kNtThreads) {
+        const int j = e % kN, k = e / kN;
+        sTY[j * kS + k] = a.tabD[(size_t)(T.x + a.yoff) * npb + e];
+      }
+      __syncthreads();
+      for (int e = tid; e < T.z * npb; e += kNtThreads) {
+        const int b = e / npb, r = e - b * npb, j1 = r % kN, j2 = r / kN;
+        sF[((size_t)b * kN + j1) * kS + j2] = fv[(size_t)s_blk[b].x * nd * npb + ind + (size_t)nd * r];
+      }
+      __syncthreads();
+      if (grp < T.z) {
+        double g[4][kTN];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+          for (int u = 0; u < kTN; u++) g[i][u] = 0.0;
+        const double *fr = sF + ((size_t)grp * kN + ra) * kS;
+#pragma unroll 4
+        for (int j2 = 0; j2 < kN; j2++) {
+          double f[4], y[kTN];
+#pragma unroll
+          for (int i = 0; i < 4; i++) f[i] = fr[i * kS + j2];
+#pragma unroll
+          for (int u = 0; u < kTN; u++) y[u] = sTY[j2 * kS + ca + u];
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int u = 0; u < kTN; u++) g[i][u] = fma(f[i], y[u], g[i][u]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+          for (int u = 0; u < kTN; u++) sG[((size_t)grp * kN + ra + i) * kS + ca + u] = g[i][u];
+      }
+      __syncthreads();
+      // pairs of this thread's target: (block b, x slot) with target grp
+      if (grp < ntarget) {
+        for (int b = 0; b < T.z; b++) {
+          const int4 bk = s_blk[b];
+          for (int u = 0; u < bk.w; u++) {
+            const int cs = ((u < 2 ? bk.y : bk.z) >> (16 * (u & 1))) & 0xFFFF;
+            if ((cs & 0xFF) != grp) continue;
+            const double *xr = sTX + (size_t)(cs >> 8) * kN * kS;
+            const double *gr = sG + (size_t)b * kN * kS;
+#pragma unroll 4
+            for (int j1 = 0; j1 < kN; j1++) {
+              double x[4], gv[kTN];
+#pragma unroll
+              for (int i = 0; i < 4; i++) x[i] = xr[j1 * kS + ra + i];
+#pragma unroll
+              for (int v = 0; v < kTN; v++) gv[v] = gr[j1 * kS + ca + v];
+#pragma unroll
+              for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int v = 0; v < kTN; v++) acc[i][v] = fma(x[i], gv[v], acc[i][v]);
+            }
+          }
+        }
+      }
+    }
+    if (grp < ntarget) {
+      // pot(k1 = ra + i, k2 = ca + v) of target grp
+      double *pb = pot + (size_t)a.targets[c.z + grp] * a.out_nd * npb + a.out_off + ind;
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int v = 0; v < kTN; v++) pb[(size_t)a.out_nd * ((ra + i) + kN * (ca + v))] += acc[i][v];
+    }
+  }
+}
+
 }  // namespace
 
-int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
+int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg, bool fp64) {
   near_tc_destroy(dp);
   const int n = hp.norder;
   if (hp.nf_target.empty() || (n != 8 && n != 16)) return BFGT_OK;
@@ -331,7 +444,8 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   // all on the values' band pattern
   const bool derivs = hp.tabx_loc.size() >= (size_t)n * n * nslots_tab && hp.tabxx_loc.size() >= (size_t)n * n * nslots_tab;
   const std::vector<double> *sets[3] = {&hp.tab_loc, &hp.tabx_loc, &hp.tabxx_loc};
-  std::vector<uint16_t> tab((size_t)3 * nslots_tab * kNtTab, 0);
+  std::vector<uint16_t> tab(fp64 ? 0 : (size_t)3 * nslots_tab * kNtTab, 0);
+  std::vector<double> tabd(fp64 ? (size_t)3 * nslots_tab * n * n : 0, 0.0);
   std::vector<char> used(nslots_tab, 0);
   for (int q = 0; q < nslots_tab; q++) {
     const int *il = &hp.ind_loc[(size_t)2 * (n + 1) * q];
@@ -340,13 +454,17 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
     used[q] = 1;
     for (int set = 0; set < (derivs ? 3 : 1); set++) {
       const double *t = &(*sets[set])[(size_t)n * n * q];
-      uint16_t *dst = &tab[((size_t)set * nslots_tab + q) * kNtTab];
       for (int k = k0 - 1; k < k1; k++) {
         const int lo = il[2 * k], hi = il[2 * k + 1];
         for (int j = lo - 1; j < hi; j++) {
+          if (fp64) {
+            tabd[((size_t)set * nslots_tab + q) * n * n + j + (size_t)n * k] = t[j + (size_t)n * k];
+            continue;
+          }
           uint16_t s[3];
           split3_host(t[j + (size_t)n * k], s[0], s[1], s[2]);
           const uint32_t o = kmajor_off_host(k, j, 16) / 2;
+          uint16_t *dst = &tab[((size_t)set * nslots_tab + q) * kNtTab];
           for (int cc = 0; cc < 3; cc++) dst[cc * (kNtB / 2) + o] = s[cc];
         }
       }
@@ -455,13 +573,16 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   chk(upload_nt(p.targets, targets, msg));
   chk(upload_nt(p.slot_q, slot_q, msg));
   chk(upload_nt(p.tabB, tab, msg));
+  chk(upload_nt(p.tabD, tabd, msg));
   if (rc != BFGT_OK) {
     near_tc_destroy(dp);
     return rc;
   }
   p.nctas = (int)ctas.size();
   p.maxslot = maxslot;
-  p.smem = std::max(kNtFixed + sizeof(float) * (size_t)kG * maxslot * n * (n + 1), kNtMinSmem);
+  p.fp64 = fp64;
+  p.smem = fp64 ? sizeof(double) * ((size_t)2 * kG * n * (n + 1) + (size_t)n * (n + 1) + (size_t)maxslot * n * (n + 1))
+                : std::max(kNtFixed + sizeof(float) * (size_t)kG * maxslot * n * (n + 1), kNtMinSmem);
   const int smax = 227 * 1024 - 1024;
   if (p.smem > (size_t)smax) {
     near_tc_destroy(dp);
@@ -473,6 +594,10 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
   // shared memory allows
   cudaFuncSetAttribute(k_near_tc<8>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   cudaFuncSetAttribute(k_near_tc<16>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  cudaFuncSetAttribute(k_near_f64<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
+  cudaFuncSetAttribute(k_near_f64<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
+  cudaFuncSetAttribute(k_near_f64<8>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  cudaFuncSetAttribute(k_near_f64<16>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (cudaGetLastError() != cudaSuccess) {
     msg = "CUDA error while preparing the tensor-core near field";
     near_tc_destroy(dp);
@@ -483,7 +608,7 @@ int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg) {
 
 void near_tc_destroy(DevicePlan &dp) {
   NearTcPlan &p = dp.ntc;
-  void *ptrs[] = {p.ctas, p.tiles, p.blocks, p.targets, p.slot_q, p.tabB};
+  void *ptrs[] = {p.ctas, p.tiles, p.blocks, p.targets, p.slot_q, p.tabB, p.tabD};
   for (void *x : ptrs)
     if (x) cudaFree(x);
   p = NearTcPlan();
@@ -491,8 +616,16 @@ void near_tc_destroy(DevicePlan &dp) {
 
 NearTcArgs near_tc_args(const DevicePlan &dp, long long elem_off) {
   const NearTcPlan &p = dp.ntc;
-  return NearTcArgs{p.ctas, p.targets, p.tiles, p.blocks, p.slot_q, p.tabB, dp.split.err, dp.nd, dp.n, p.nctas,
+  return NearTcArgs{p.ctas, p.targets, p.tiles, p.blocks, p.slot_q, p.tabB, p.tabD, dp.split.err, dp.nd, dp.n, p.nctas,
                     dp.split.wait_iters ? dp.split.wait_iters : kNtWaitIters, elem_off, dp.nd, 0, 0, 0};
+}
+
+void near_f64_launch(int n, int grid, size_t smem, cudaStream_t s, const NearTcLaunch &lp) {
+  if (grid <= 0) return;
+  if (n == 16)
+    k_near_f64<16><<<grid, kNtThreads, smem, s>>>(lp);
+  else
+    k_near_f64<8><<<grid, kNtThreads, smem, s>>>(lp);
 }
 
 void near_tc_launch(int n, int grid, size_t smem, cudaStream_t s, const NearTcLaunch &lp) {

@@ -40,6 +40,8 @@ struct NearTcArgs {
   const uint16_t *tabB;  // per table slot: 3 BF16 slices of a 16 x 16 K-major B operand;
                          // three sets (values, first, second derivatives in the
                          // target coordinate), nslot_tab slots each
+  const double *tabD;    // the FP64 kernel's tables: per slot n x n, tab(j, k) at j + n k,
+                         // zero outside the band pattern; the same three sets
   int *err;
   int nd, n, nctas;
   uint32_t wait_iters;
@@ -60,15 +62,19 @@ struct NearTcLaunch {
   double *pbase;
 };
 
-// Builds the CTA, tile and pair lists and the table operands of a split plan
-// with floating slices (norder 8 or 16); leaves dp.ntc empty (the FP64
-// near-field kernel runs) when the plan has no near field or cannot use it.
-int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg);
+// Builds the CTA, tile and block lists and the tables of a plan with norder 8
+// or 16: BF16 table operands for the tensor-core kernel (split plans with
+// floating slices, fp64 false), or FP64 tables for k_near_f64, the same
+// decomposition on the FP64 pipes (FP64 plans and fixed-point split plans,
+// fp64 true).  Leaves dp.ntc empty (the per-target FP64 kernel runs) when the
+// plan has no near field or cannot use it.
+int near_tc_create(DevicePlan &dp, const HostPlan &hp, std::string &msg, bool fp64 = false);
 void near_tc_destroy(DevicePlan &dp);
 NearTcArgs near_tc_args(const DevicePlan &dp, long long elem_off);
 // table slots per derivative set (13 offsets per level)
 inline int near_tc_nslot(const DevicePlan &dp) { return 13 * (dp.nlevels + 1); }
 // one plan's near field, or (lp.descs set) grid CTAs of a batch
 void near_tc_launch(int n, int grid, size_t smem, cudaStream_t s, const NearTcLaunch &lp);
+void near_f64_launch(int n, int grid, size_t smem, cudaStream_t s, const NearTcLaunch &lp);
 
 }  // namespace bfgt

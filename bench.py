@@ -12,8 +12,9 @@ independent tree (seed + rank): weak scaling, no collective on the data path;
 time = max over ranks of the device-timed region.
 
 --impl reference times the reference's CPU algorithm (the oracle: a C
-restatement of bfgt/boxfgt.f with the reference's OpenMP loops; the Fortran
-cannot be compiled in this image) on the box's host cores, same workload.
+restatement of bfgt/boxfgt.f with the reference's OpenMP loops; no Fortran
+compiler is available to build the reference itself) on the host's cores,
+same workload.
 """
 from __future__ import annotations
 

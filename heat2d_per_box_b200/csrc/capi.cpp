@@ -565,9 +565,12 @@ uint64_t g_cache_clock = 0, g_cache_hits = 0, g_cache_misses = 0;
 double g_last_bytes[2] = {0, 0};  // host<->device bytes of the last drop-in call
 int g_default_precision = -1;  // -1: from BFGT_PRECISION at first use
 
+// 16 by default: a solver step calls boxfgt once per delta (an initial-value
+// transform and one per Gauss node, per species: hpots2dadap.f:79, 329-346),
+// and an LRU cache smaller than that cycle would miss on every call
 int cache_capacity() {
   const char *e = std::getenv("BFGT_PLAN_CACHE");
-  if (!e || !*e) return 4;
+  if (!e || !*e) return 16;
   return std::max(0, std::atoi(e));
 }
 

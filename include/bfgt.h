@@ -74,7 +74,7 @@ int bfgt_set_default_precision(int precision);
 
 /* No counterpart in the reference.  boxfgt_ and bfgt_boxfgt keep the plans
    (step-0 precomputation and device tables) of their last few argument sets,
-   4 by default or BFGT_PLAN_CACHE (0 turns the cache off).  A plan is found
+   16 by default or BFGT_PLAN_CACHE (0 turns the cache off).  A plan is found
    again when nd, delta, eps, ipoly, iperiod, norder, precision, nboxes,
    nlevels, ltree, the device, iptr, itree up to its colleague arrays, centers
    and boxsize all equal, bit for bit, those it was built from (the cache keeps

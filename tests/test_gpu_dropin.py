@@ -160,3 +160,20 @@ def test_zero_pot_is_cleared_on_the_device_not_uploaded(trees):
                                atol=1e-14 * (np.abs(base).max() + np.abs(p0).max()))
     nonleaf = t.nchild() > 0
     np.testing.assert_array_equal(pot2.reshape(t.nboxes, -1)[nonleaf], base.reshape(t.nboxes, -1)[nonleaf])
+
+
+def test_a_solver_step_cycle_stays_cached(trees):
+    """One heat-solver step calls boxfgt once per delta (4 dt, and 4 (dt - t_q)
+    for 4 Gauss nodes: hpots2dadap.f:79, 329-346); the next step repeats the
+    cycle, which must then find all 5 plans."""
+    t = trees["uni3_leg_per"]
+    dt = 1e-3
+    xq = (np.polynomial.legendre.leggauss(4)[0] + 1) / 2
+    deltas = [4 * dt] + [4 * (1 - x) * dt for x in xq]
+    first = [call(t, d, 1e-6)[0] for d in deltas]
+    h0 = hb.plan_cache_info()["hits"]
+    again = [call(t, d, 1e-6)[0] for d in deltas]
+    info = hb.plan_cache_info()
+    assert info["hits"] == h0 + len(deltas) and info["entries"] == len(deltas)
+    for a, b in zip(first, again):
+        np.testing.assert_array_equal(a, b)

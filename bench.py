@@ -691,6 +691,28 @@ def main():
            "ms_per_call": el / ne * 1e3, "lookup_ms_per_call": ti[0] * 1e3, "first_call_ms": first_ms,
            "first_call_precompute_ms": first_pre_ms, "cache_hits": cache["hits"],
            "pcie_gbs": (moved["h2d"] + moved["d2h"]) / (el / ne) / 1e9}
+    # the same calls with ordinary (pageable) host arrays, as a Fortran solver
+    # has them: the library stages them through pinned chunks
+    pf = tree.fvals.reshape(-1).copy()
+    pp = np.zeros(nelem)
+
+    def dropin_pageable():
+        hb.boxfgt(1, 2, args.delta, args.eps, tree.ipoly, tree.iperiod, tree.norder, tree.npbox, tree.nboxes,
+                  tree.nlevels, tree.ltree, itree, tree.iptr, tree.centers, tree.boxsize, pf, 1, pp, None, None,
+                  0, 0, None, 0, None, None, None, ti)
+
+    dropin_pageable()
+    evp = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(ne)]
+    for a, b in evp:
+        pp.fill(0.0)
+        a.record(stream)
+        dropin_pageable()
+        b.record(stream)
+    torch.cuda.synchronize()
+    t_pg = sum(a.elapsed_time(b) for a, b in evp) * 1e-3
+    pg_points, pg_el = reduce_over_ranks(dist, npts * ne, t_pg, dev)
+    e2e["pageable"] = {"value": pg_points / pg_el, "ms_per_call": pg_el / ne * 1e3,
+                       "same_result_as_pinned": bool(np.array_equal(pp, hp_np))}
     hb.set_default_precision(hb.BFGT_PREC_FP64)
     hb.plan_cache_clear()
 

@@ -151,6 +151,114 @@ bool all_zero_bits(const double *p, size_t n) {
   return !nonzero.load();
 }
 
+// Copies between a caller's host arrays and the device.  Page-locked arrays
+// are copied directly.  Pageable ones (a Fortran caller's ordinary arrays;
+// cudaMemcpyAsync stages those through the driver's own buffers at a fraction
+// of the link rate) go through two pinned 8 MB chunks of the plan: the host
+// threads fill or drain one chunk while the DMA engine moves the other.
+constexpr size_t kStageChunk = 8u << 20;
+
+bool page_locked(const void *p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+void par_copy(void *dst, const void *src, size_t bytes) {
+  constexpr size_t kPart = 1u << 20;
+  const long np = (long)((bytes + kPart - 1) / kPart);
+#pragma omp parallel for schedule(static) if (np > 1)
+  for (long i = 0; i < np; i++) {
+    const size_t o = (size_t)i * kPart;
+    std::memcpy(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o, std::min(kPart, bytes - o));
+  }
+}
+
+class Stager {
+ public:
+  Stager(bfgt::DevicePlan &dp, cudaStream_t s) : dp_(dp), s_(s) {}
+  ~Stager() {
+    for (cudaEvent_t e : ev_)
+      if (e) cudaEventDestroy(e);
+  }
+  // host -> device (queued on the stream; a pageable source is read before return)
+  bool up(double *d, const double *h, size_t bytes) {
+    if (page_locked(h)) return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s_) == cudaSuccess;
+    for (size_t off = 0; off < bytes; off += kStageChunk) {
+      const size_t len = std::min(kStageChunk, bytes - off);
+      char *b = chunk();
+      if (!b) return false;
+      par_copy(b, reinterpret_cast<const char *>(h) + off, len);
+      if (cudaMemcpyAsync(reinterpret_cast<char *>(d) + off, b, len, cudaMemcpyHostToDevice, s_) != cudaSuccess ||
+          cudaEventRecord(ev_[k_ & 1], s_) != cudaSuccess)
+        return false;
+      used_[k_ & 1] = true;
+      k_++;
+    }
+    return true;
+  }
+  // device -> host (a pageable destination is written by finish() at the latest)
+  bool down(double *h, const double *d, size_t bytes) {
+    if (page_locked(h)) return cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s_) == cudaSuccess;
+    for (size_t off = 0; off < bytes; off += kStageChunk) {
+      const size_t len = std::min(kStageChunk, bytes - off);
+      char *b = chunk();
+      if (!b) return false;
+      if (cudaMemcpyAsync(b, reinterpret_cast<const char *>(d) + off, len, cudaMemcpyDeviceToHost, s_) != cudaSuccess ||
+          cudaEventRecord(ev_[k_ & 1], s_) != cudaSuccess)
+        return false;
+      used_[k_ & 1] = true;
+      // the previous chunk's data, if any, to its host array while this one moves
+      if (!drain()) return false;
+      pend_ = {reinterpret_cast<char *>(h) + off, b, len, k_ & 1};
+      k_++;
+    }
+    return true;
+  }
+  bool finish() { return drain(); }
+
+ private:
+  struct Pending {
+    char *dst = nullptr;
+    const char *src = nullptr;
+    size_t len = 0;
+    int slot = 0;
+  };
+  // the next free chunk: allocated on first use, reused once its last copy is done
+  char *chunk() {
+    if (!dp_.h_stage_f) {
+      if (cudaHostAlloc(reinterpret_cast<void **>(&dp_.h_stage_f), 2 * kStageChunk, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        dp_.h_stage_f = nullptr;
+        return nullptr;
+      }
+    }
+    const int b = k_ & 1;
+    if (!ev_[b] && cudaEventCreateWithFlags(&ev_[b], cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    if (used_[b]) {
+      if (pend_.dst && pend_.slot == b && !drain()) return nullptr;
+      if (cudaEventSynchronize(ev_[b]) != cudaSuccess) return nullptr;
+    }
+    return reinterpret_cast<char *>(dp_.h_stage_f) + (size_t)b * kStageChunk;
+  }
+  bool drain() {
+    if (!pend_.dst) return true;
+    if (cudaEventSynchronize(ev_[pend_.slot]) != cudaSuccess) return false;
+    par_copy(pend_.dst, pend_.src, pend_.len);
+    pend_ = Pending();
+    return true;
+  }
+  bfgt::DevicePlan &dp_;
+  cudaStream_t s_;
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
+  bool used_[2] = {false, false};
+  int k_ = 0;
+  Pending pend_;
+};
+
 // Host-array form of one transform on dp: uploads the leaf runs of the input
 // and of the accumulators, runs, and copies the accumulators' leaf runs back.
 // With ifpgh >= 2 grad(nd,2,..) and, for 3, hess(nd,3,..) are accumulated too.
@@ -195,11 +303,11 @@ int execute_host_on(bfgt_plan plan, bfgt::DevicePlan &dp, const double *in, doub
   std::vector<Acc> accs = {{acc, dp.d_stage_p, 1}};
   if (dg) accs.push_back({grad, dg, 2});
   if (dh) accs.push_back({hess, dh, 3});
+  Stager st(dp, s);
   double up = 0;
   for (const auto &r : plan->leaf_runs) {
     const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
-    if (cudaMemcpyAsync(dp.d_stage_f + o, in + o, c, cudaMemcpyHostToDevice, s) != cudaSuccess)
-      return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
+    if (!st.up(dp.d_stage_f + o, in + o, c)) return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
     up += (double)c;
   }
   for (const auto &r : plan->leaf_runs) {
@@ -209,8 +317,7 @@ int execute_host_on(bfgt_plan plan, bfgt::DevicePlan &dp, const double *in, doub
         if (cudaMemsetAsync(a.d + a.k * o, 0, a.k * c, s) != cudaSuccess)
           return fail(BFGT_ERR_CUDA, "device clear failed");
       } else {
-        if (cudaMemcpyAsync(a.d + a.k * o, a.h + a.k * o, a.k * c, cudaMemcpyHostToDevice, s) != cudaSuccess)
-          return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
+        if (!st.up(a.d + a.k * o, a.h + a.k * o, a.k * c)) return fail(BFGT_ERR_CUDA, "host-to-device copy failed");
         up += (double)(a.k * c);
       }
     }
@@ -224,11 +331,11 @@ int execute_host_on(bfgt_plan plan, bfgt::DevicePlan &dp, const double *in, doub
   for (const auto &r : plan->leaf_runs) {
     const size_t o = per * r.first, c = per * (r.second - r.first) * sizeof(double);
     for (const Acc &a : accs) {
-      if (cudaMemcpyAsync(a.h + a.k * o, a.d + a.k * o, a.k * c, cudaMemcpyDeviceToHost, s) != cudaSuccess)
-        return fail(BFGT_ERR_CUDA, "device-to-host copy failed");
+      if (!st.down(a.h + a.k * o, a.d + a.k * o, a.k * c)) return fail(BFGT_ERR_CUDA, "device-to-host copy failed");
       down += (double)(a.k * c);
     }
   }
+  if (!st.finish()) return fail(BFGT_ERR_CUDA, "device-to-host copy failed");
   plan->last_d2h_bytes = down;
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(BFGT_ERR_CUDA, std::string("transform failed: ") + cudaGetErrorString(cudaGetLastError()));
   return BFGT_OK;

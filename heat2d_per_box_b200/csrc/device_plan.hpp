@@ -108,7 +108,9 @@ struct DevicePlan {
   double *tab_loc = nullptr;
   int *ind_loc = nullptr;
   // staging for host-buffer execution
-  double *h_stage_f = nullptr, *h_stage_p = nullptr;  // pinned
+  // pinned host chunks (2 x 8 MB) through which the host-array entry points
+  // copy pageable caller arrays; allocated on first use
+  double *h_stage_f = nullptr;
   double *d_stage_f = nullptr, *d_stage_p = nullptr;
   size_t stage_elems = 0;
   double *d_stage_gh = nullptr;  // grad (2 x) and hess (3 x) staging, 5 * stage_gh_elems

@@ -912,7 +912,6 @@ void device_plan_destroy(DevicePlan &dp) {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (dp.h_stage_f) cudaFreeHost(dp.h_stage_f);
-  if (dp.h_stage_p) cudaFreeHost(dp.h_stage_p);
   for (auto &es : dp.evsets)
     for (cudaEvent_t e : es) cudaEventDestroy(e);
   dp = DevicePlan();

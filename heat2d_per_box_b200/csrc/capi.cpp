@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <cstdint>
+#include <initializer_list>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -118,10 +119,42 @@ int bfgt_plan_create(bfgt_plan *plan, int nd, double delta, double eps, int ipol
   return BFGT_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Device arrays must live on the plan's device: a kernel reading another
+// device's memory (without peer access) or a host array would fault.  With
+// one process per GPU this catches a plan made before the caller selected
+// its device.  Null pointers are the callers' checks.
+int check_device_array(const void *p, int dev, const char *what) {
+  if (!p) return BFGT_OK;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(BFGT_ERR_ARG, std::string(what) + ": not a CUDA allocation");
+  }
+  if ((at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == dev) return BFGT_OK;
+  return fail(BFGT_ERR_ARG, std::string(what) + ": not device memory of the plan's device " + std::to_string(dev));
+}
+
+int check_device_arrays(int dev, std::initializer_list<std::pair<const void *, const char *>> arrays) {
+  for (const auto &a : arrays) {
+    const int rc = check_device_array(a.first, dev, a.second);
+    if (rc != BFGT_OK) return rc;
+  }
+  return BFGT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int bfgt_plan_execute(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream) {
   g_err.clear();
   if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
   if (!d_fvals || !d_pot) return fail(BFGT_ERR_ARG, "fvals/pot device pointers are NULL");
+  if (check_device_arrays(plan->dp.device, {{d_fvals, "fvals"}, {d_pot, "pot"}}) != BFGT_OK) return BFGT_ERR_ARG;
   std::string msg;
   int rc = bfgt::device_plan_execute(plan->dp, d_fvals, d_pot, (cudaStream_t)stream, msg);
   if (rc != BFGT_OK) return fail(rc, msg);
@@ -456,6 +489,9 @@ int bfgt_plan_execute_pgh(bfgt_plan plan, int ifpgh, const double *d_fvals, doub
   if (ifpgh < 1 || ifpgh > 3) return fail(BFGT_ERR_ARG, "ifpgh must be 1, 2 or 3");
   if (!d_fvals || !d_pot || (ifpgh >= 2 && !d_grad) || (ifpgh == 3 && !d_hess))
     return fail(BFGT_ERR_ARG, "a device array that ifpgh asks for is NULL");
+  if (check_device_arrays(plan->dp.device, {{d_fvals, "fvals"}, {d_pot, "pot"}, {ifpgh >= 2 ? d_grad : nullptr, "grad"},
+                                            {ifpgh == 3 ? d_hess : nullptr, "hess"}}) != BFGT_OK)
+    return BFGT_ERR_ARG;
   if (ifpgh >= 2) {
     int rc = ensure_pgh(plan);
     if (rc != BFGT_OK) return rc;
@@ -487,6 +523,8 @@ int bfgt_plan_eval_targets(bfgt_plan plan, int ncomp, const double *d_vals, int 
   if (ncomp < 1 || ncomp > 3) return fail(BFGT_ERR_ARG, "ncomp must be 1, 2 or 3");
   if (ntarg < 0) return fail(BFGT_ERR_ARG, "ntarg is negative");
   if (ntarg > 0 && (!d_vals || !d_targs || !d_out)) return fail(BFGT_ERR_ARG, "vals/targs/out device pointers are NULL");
+  if (ntarg > 0 && check_device_arrays(plan->dp.device, {{d_vals, "vals"}, {d_targs, "targs"}, {d_out, "out"}}) != BFGT_OK)
+    return BFGT_ERR_ARG;
   std::string msg;
   int rc = bfgt::device_plan_eval_targets(plan->dp, ncomp, d_vals, ntarg, d_targs, d_out, (cudaStream_t)stream, msg);
   if (rc != BFGT_OK) return fail(rc, msg);
@@ -497,6 +535,7 @@ int bfgt_plan_execute_adjoint(bfgt_plan plan, const double *d_potbar, double *d_
   g_err.clear();
   if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
   if (!d_potbar || !d_fbar) return fail(BFGT_ERR_ARG, "potbar/fbar device pointers are NULL");
+  if (check_device_arrays(plan->dp.device, {{d_potbar, "potbar"}, {d_fbar, "fbar"}}) != BFGT_OK) return BFGT_ERR_ARG;
   int rc = ensure_adjoint(plan);
   if (rc != BFGT_OK) return rc;
   std::string msg;
@@ -517,6 +556,8 @@ int bfgt_plan_execute_adjoint_host(bfgt_plan plan, const double *potbar, double 
 int bfgt_plan_graph_capture(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream) {
   g_err.clear();
   if (!plan) return fail(BFGT_ERR_ARG, "plan is NULL");
+  if (!d_fvals || !d_pot) return fail(BFGT_ERR_ARG, "fvals/pot device pointers are NULL");
+  if (check_device_arrays(plan->dp.device, {{d_fvals, "fvals"}, {d_pot, "pot"}}) != BFGT_OK) return BFGT_ERR_ARG;
   bfgt::DevicePlan &dp = plan->dp;
   cudaStream_t s = (cudaStream_t)stream;
   cudaStream_t cs = s;
@@ -1163,6 +1204,8 @@ int bfgt_batch_execute(bfgt_batch batch, const double *d_fvals, double *d_pot, v
   g_err.clear();
   if (!batch) return fail(BFGT_ERR_ARG, "batch is NULL");
   if (!d_fvals || !d_pot) return fail(BFGT_ERR_ARG, "fvals/pot device pointers are NULL");
+  if (check_device_arrays(batch->device, {{d_fvals, "fvals"}, {d_pot, "pot"}}) != BFGT_OK)
+    return BFGT_ERR_ARG;
   std::string msg;
   int rc = bfgt::device_batch_execute(batch->db, d_fvals, d_pot, (cudaStream_t)stream, msg);
   if (rc != BFGT_OK) return fail(rc, msg);
@@ -1173,6 +1216,8 @@ int bfgt_batch_execute_adjoint(bfgt_batch batch, const double *d_potbar, double 
   g_err.clear();
   if (!batch) return fail(BFGT_ERR_ARG, "batch is NULL");
   if (!d_potbar || !d_fbar) return fail(BFGT_ERR_ARG, "potbar/fbar device pointers are NULL");
+  if (check_device_arrays(batch->device, {{d_potbar, "potbar"}, {d_fbar, "fbar"}}) != BFGT_OK)
+    return BFGT_ERR_ARG;
   if (!batch->adj) {
     std::vector<bfgt::DevicePlan *> dps;
     for (bfgt_plan p : batch->plans) {
@@ -1198,6 +1243,9 @@ int bfgt_batch_execute_adjoint(bfgt_batch batch, const double *d_potbar, double 
 int bfgt_batch_graph_capture(bfgt_batch batch, const double *d_fvals, double *d_pot, void *stream) {
   g_err.clear();
   if (!batch) return fail(BFGT_ERR_ARG, "batch is NULL");
+  if (!d_fvals || !d_pot) return fail(BFGT_ERR_ARG, "fvals/pot device pointers are NULL");
+  if (check_device_arrays(batch->device, {{d_fvals, "fvals"}, {d_pot, "pot"}}) != BFGT_OK)
+    return BFGT_ERR_ARG;
   bfgt::DeviceBatch &db = batch->db;
   cudaStream_t cs = (cudaStream_t)stream;
   bool own = false;

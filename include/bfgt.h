@@ -119,6 +119,9 @@ int bfgt_plan_create(bfgt_plan *plan, int nd, double delta, double eps, int ipol
    into on leaf boxes.  stream is a cudaStream_t (NULL = default stream).
    Asynchronous: returns after the launches are queued. */
 int bfgt_plan_execute(bfgt_plan plan, const double *d_fvals, double *d_pot, void *stream);
+/* (Every entry point that takes device arrays returns BFGT_ERR_ARG, before
+   launching anything, for an array that is not device memory of the plan's
+   device.) */
 
 /* Same transform on host arrays: uploads the leaf values, runs, and adds the
    result into the host pot (the reference-facing form of a planned call). */

@@ -183,7 +183,8 @@ def make_uneven_trees(seed, ntrees=64, lo=1000, hi=50000):
     [1e-5, 1e-1] per tree.  A tree is refined uniformly to level L or L+1
     (4^L <= target) and then adaptively by the Legendre-tail criterion with a
     tolerance of 1e-6, 1e-9 or 1e-12 (at most 4 more levels): of these six
-    trees the one whose leaf count is nearest the target (in log) is kept."""
+    trees the one whose leaf count is nearest the target (in log) among those
+    inside [lo, hi] is kept (the nearest overall if none is inside)."""
     import heat2d_per_box_b200 as hb
     rng = np.random.default_rng(seed)
     out = []
@@ -194,12 +195,13 @@ def make_uneven_trees(seed, ntrees=64, lo=1000, hi=50000):
         a = rng.standard_normal(ng)
         target = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
         L = max(1, int(np.floor(np.log(target) / np.log(4))))
-        t, best = None, np.inf
+        t, best = None, (True, np.inf)
         for minlev in (L, L + 1):
             for tail in (1e-6, 1e-9, 1e-12):
                 cand = hb.build_adaptive(hb.gauss_params(c, w, a), norder=8, ipoly=0, iperiod=1, eps=tail,
                                          minlev=minlev, maxlev=minlev + 4)
-                d = abs(np.log(len(cand.leaves()) / target))
+                nl = len(cand.leaves())
+                d = (not lo <= nl <= hi, abs(np.log(nl / target)))
                 if d < best:
                     t, best = cand, d
         delta = float(np.exp(rng.uniform(np.log(1e-5), np.log(1e-1))))

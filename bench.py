@@ -44,25 +44,38 @@ def peaks():
     return 6650.0, 1590.0, 1400.0, "fallback"
 
 
-def make_tree(seed, small=False):
+def make_tree(seed, small=False, minlev=None):
+    """The adaptive order-16 workload tree: uniform to level 8 (6 with small),
+    or to minlev when given (0: the purely adaptive tree of the tail
+    criterion), then refined to a 1e-10 Legendre tail, max level 12."""
     import heat2d_per_box_b200 as hb
     rng = np.random.default_rng(seed)
     c = rng.uniform(-0.5, 0.5, (20, 2))
     w = np.exp(rng.uniform(np.log(1e-3), np.log(1e-2), 20))
     a = rng.standard_normal(20)
     g = hb.gauss_params(c, w, a)
-    minlev = 6 if small else 8
+    if minlev is None:
+        minlev = 6 if small else 8
     return hb.build_adaptive(g, norder=16, ipoly=0, iperiod=1, eps=1e-10, eta=1.0, minlev=minlev, maxlev=12)
 
 
-def workload_config(tree, delta, eps, world):
+def base_level(args):
+    """The uniform base level the arguments give the adaptive workload tree."""
+    m = getattr(args, "minlev", None)
+    return m if m is not None else (6 if getattr(args, "small", False) else 8)
+
+
+def workload_config(tree, delta, eps, world, minlev=8):
     """The config of the adaptive order-16 workload, identical in both arms."""
     npts = len(tree.leaves()) * tree.npbox
+    base = f"uniform to level {minlev} then " if minlev > 0 else ""
     return {"workload": "adaptive order-16 periodic tree, 20 Gaussians (w log-U[1e-3,1e-2], a~N(0,1)), "
-                        "uniform to level 8 then tail<1e-10, max level 12; nd=1",
+                        f"{base}tail<1e-10, max level 12; nd=1",
             "leaves": int(len(tree.leaves())), "points_per_gpu": int(npts), "nd": 1, "delta": delta, "eps": eps,
             "norder": 16,
-            "l2": "inputs larger than L2 (leaf fvals + pot = %.0f MB per step)" % (npts * 24 / 1e6),
+            "l2": ("inputs larger than L2 (leaf fvals + pot = %.0f MB per step)" if npts * 24 > 126e6 else
+                   "inputs fit in L2 (leaf fvals + pot = %.0f MB per step; not flushed between steps)")
+                  % (npts * 24 / 1e6),
             "parallelism": f"replicas x{world} (independent trees)"}
 
 
@@ -148,7 +161,7 @@ def run_reference(args, rank, world):
     from oracle import oracle
     if rank != 0:
         return
-    t = make_tree(2)
+    t = make_tree(2, small=args.small, minlev=args.minlev)
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     delta, eps = args.delta, args.eps
@@ -168,7 +181,7 @@ def run_reference(args, rank, world):
     line = {"metric": METRIC, "value": v, "unit": "leaf points/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": steps, "warmup": args.warmup, "ms_per_step": el / steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(t, delta, eps, world),
+            "config": workload_config(t, delta, eps, world, base_level(args)),
             "cpu_baseline": {"value": v, "unit": "leaf points/s", "cores": threads, "kind": "port",
                              "sample": f"{steps} full transforms of the workload tree (oracle, OpenMP "
                                        f"{threads} threads; bfgt/boxfgt.f restated in C)"},
@@ -507,6 +520,8 @@ def main():
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "split"])
     ap.add_argument("--small", action="store_true", help="level-6 base tree (for profiler captures)")
+    ap.add_argument("--minlev", type=int, default=None,
+                    help="uniform base level of the adaptive tree (default 8; 0: purely adaptive)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="adaptive16", choices=["adaptive16", "uneven64", "uniform5", "heat5", "near16"],
                     help="adaptive16: one adaptive order-16 tree (default); uneven64: 64 uneven order-8 trees, "
@@ -551,7 +566,7 @@ def main():
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
 
-    tree = make_tree(2 + rank, small=args.small)
+    tree = make_tree(2 + rank, small=args.small, minlev=args.minlev)
     leaves = tree.leaves()
     npts = len(leaves) * tree.npbox
     precs = {"fp64": [hb.BFGT_PREC_FP64], "split": [hb.BFGT_PREC_SPLIT]}.get(args.precision)
@@ -750,7 +765,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if main_prec == hb.BFGT_PREC_FP64 else "f16-split/f32acc/f64",
         "data": "synthetic",
-        "config": workload_config(tree, args.delta, args.eps, world),
+        "config": workload_config(tree, args.delta, args.eps, world, base_level(args)),
         "plan": {"npw": R["info"]["npw"], "npwlevel": R["info"]["npwlevel"],
                  "precision": "split" if main_prec == hb.BFGT_PREC_SPLIT else "fp64",
                  "tuned_shape": R["info"]["split_shape"] if main_prec == hb.BFGT_PREC_SPLIT else

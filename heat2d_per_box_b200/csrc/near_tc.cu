@@ -1,9 +1,10 @@
-// Tensor-core near field of split-precision plans (see near_tc.cuh).
+// Near field on block work lists: on the tensor cores for split plans with
+// floating slices (k_near_tc), in FP64 for the others (k_near_f64); see
+// near_tc.cuh.
 #include "near_tc.cuh"
 
 #include <algorithm>
 #include <cstring>
-#include <map>
 #include <vector>
 
 #include "../../include/bfgt.h"

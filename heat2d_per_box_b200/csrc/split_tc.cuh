@@ -324,7 +324,10 @@ __global__ void __launch_bounds__(kThreads) k_form_tc(const __grid_constant__ Fo
       const double *fv = leaf_row(s2);
 #pragma unroll
       for (int k = 0; k < kN; k++)
-        fnext[k] = (fv && (kN == 8 || k < n)) ? fv[(size_t)nd * (kN == 8 ? kN : n) * k] : 0.0;
+        // read once: evict-first loads (the leaf values do not displace the
+        // expansions and pot lines in L2; A/B on the bench tree: the step
+        // 219.8 -> 212.4 us together with the eval kernel's streaming pot)
+        fnext[k] = (fv && (kN == 8 || k < n)) ? __ldcs(fv + (size_t)nd * (kN == 8 ? kN : n) * k) : 0.0;
       if constexpr (!kFix) {
         const int *st2 = a.steps + (size_t)(sb + s2) * stride;
         const uint4 *src = reinterpret_cast<const uint4 *>(tyb + (size_t)st2[0] * a.tyb_tile);
@@ -825,7 +828,8 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
           pb = box >= 0 ? pot + (size_t)box * nd * npb + (d0 + rdl) + (size_t)nd * rk1 : nullptr;
 #pragma unroll
           for (int k2 = 0; k2 < kN; k2++)  // (n = 16: the same code as before kN existed)
-            pv[k2] = (pb && (kN == 8 || k2 < n)) ? pb[(size_t)nd * (kN == 8 ? kN : n) * k2] : 0.0;
+            // pot is read and written once per launch: streaming (evict-first) accesses
+            pv[k2] = (pb && (kN == 8 || k2 < n)) ? __ldcs(pb + (size_t)nd * (kN == 8 ? kN : n) * k2) : 0.0;
         };
         load_pot(warp >> 2);
         for (int st = warp >> 2; st < Sg; st += 2) {
@@ -859,7 +863,7 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
             if (ok && pbc) {
 #pragma unroll
               for (int k2 = 0; k2 < kN; k2++)
-                if (kN == 8 || k2 < n) pbc[(size_t)nd * (kN == 8 ? kN : n) * k2] = pc[k2] + 2.0 * (double)(v0[k2] + v1[k2]);
+                if (kN == 8 || k2 < n) __stcs(pbc + (size_t)nd * (kN == 8 ? kN : n) * k2, pc[k2] + 2.0 * (double)(v0[k2] + v1[k2]));
             }
           }
         }

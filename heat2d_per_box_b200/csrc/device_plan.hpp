@@ -136,8 +136,9 @@ void device_plan_destroy(DevicePlan &dp);
 // Times every compiled FP64 tile shape of the form and eval kernels on this
 // plan's work (scratch inputs; the caller's arrays are not touched), keeps the
 // fastest and remembers it for later plans of the same (norder, npw, nd).
-// report: best form ms, best eval ms, form and eval candidates timed.  No
-// effect on split-precision plans (their shapes are fixed).
+// report: best form ms, best eval ms, form and eval candidates timed.
+// Split-precision plans go to split_autotune (the form kernel's Y staging and
+// x tiles, the eval kernel's step groups and column halves; same bits).
 int device_plan_autotune(DevicePlan &dp, cudaStream_t s, double *report, std::string &msg);
 // Uploads the derivative tables used by device_plan_execute_pgh.
 int device_plan_prepare_pgh(DevicePlan &dp, const HostPlan &hp, std::string &msg);

@@ -78,8 +78,9 @@ def test_autotune_split_plan_same_bits(trees, name, delta, eps, nd):
                                                ("ad_leg_per", 1e-4, 1e-6, 3)])
 def test_eval_on_column_halves_same_bits(trees, monkeypatch, name, delta, eps, nd):
     """The eval kernel on the chunks' column halves (an autotuner choice, forced
-    here through BFGT_SPLIT_EVAL_HALVES) gives the same bits, alone and in a
-    batch: each output row's H and MMAs do not depend on the other rows."""
+    here through BFGT_SPLIT_EVAL_HALVES) gives the same bits, alone, in a batch
+    and in the gradient and Hessian view: each output row's H and MMAs do not
+    depend on the other rows."""
     import torch
     t = trees[name]
     f0 = np.repeat(t.fvals[:, :, None], nd, axis=2) * np.linspace(1.0, 2.0, nd)[None, None, :]
@@ -102,5 +103,16 @@ def test_eval_on_column_halves_same_bits(trees, monkeypatch, name, delta, eps, n
     batch.check()
     np.testing.assert_array_equal(pb.cpu().numpy(), p0.cpu().numpy())
     batch.close()
+    # the gradient and Hessian view (3 nd densities, whole chunks or halves per CTA)
+    outs = []
+    for pl in (base, plan):
+        pp = torch.zeros_like(f)
+        g = torch.zeros(2 * f.numel(), dtype=torch.float64, device="cuda")
+        h = torch.zeros(3 * f.numel(), dtype=torch.float64, device="cuda")
+        pl.execute_pgh(3, f, pp, g, h)
+        pl.check()
+        outs.append([x.cpu().numpy() for x in (pp, g, h)])
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
     plan.close()
     base.close()

@@ -855,9 +855,11 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
             else tc::tmem_ld8(tmem + 2 * kAS + col, v0);
             tc::tmem_ld_wait();
             if (ok && pbc) {
+              // streaming store, as in the floating-slice readout
 #pragma unroll
               for (int k2 = 0; k2 < kN; k2++)
-                if (kN == 8 || k2 < n) pbc[(size_t)nd * (kN == 8 ? kN : n) * k2] = fma(f2 * s_esc[k2], (double)v0[k2], pc[k2]);
+                if (kN == 8 || k2 < n)
+                  __stcs(pbc + (size_t)nd * (kN == 8 ? kN : n) * k2, fma(f2 * s_esc[k2], (double)v0[k2], pc[k2]));
             }
           } else {
             if (ok && pbc) {

@@ -806,21 +806,12 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
         }
         tc::commit(&mbar[0]);
       }
-      if (ok && !tc::mbar_wait(&mbar[0], g & 1, a.wait_iters)) {
-        ok = false;
-        atomicExch(a.err, 1);
-      }
-      tc::fence_after_sync();
-      // the B buffer is free again: fetch the next group's tiles during the readout
-      if (j + 1 < nbatch) load_batch(s0 + eb, min(eb, nsteps - s0 - eb));
-      else if (pass + 1 < pend) load_batch(0, min(eb, nsteps));
       // readout: warp w covers TMEM lanes 32 (w%4)..; warps 0-3 take even steps, 4-7 odd steps
       {
         const int qw = warp & 3, r = 32 * qw + lane, rdl = r % pk.dpc, rsk = r / pk.dpc;
         const int rslot = rsk / n, rk1 = rsk - rslot * n;
         const bool rowok = rdl < dcnt && rsk < pk.rpd;
         const uint32_t lb = (uint32_t)(32 * qw) << 16;
-        const double f2 = kFix && rowok ? 2.0 * s_rsc[r] : 2.0;
         double pv[kN];
         double *pb = nullptr;
         auto load_pot = [&](int st) {
@@ -831,7 +822,17 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
             // pot is read and written once per launch: streaming (evict-first) accesses
             pv[k2] = (pb && (kN == 8 || k2 < n)) ? __ldcs(pb + (size_t)nd * (kN == 8 ? kN : n) * k2) : 0.0;
         };
+        // the group's first pot lines do not depend on the MMAs: in flight while they run
         load_pot(warp >> 2);
+        if (ok && !tc::mbar_wait(&mbar[0], g & 1, a.wait_iters)) {
+          ok = false;
+          atomicExch(a.err, 1);
+        }
+        tc::fence_after_sync();
+        // the B buffer is free again: fetch the next group's tiles during the readout
+        if (j + 1 < nbatch) load_batch(s0 + eb, min(eb, nsteps - s0 - eb));
+        else if (pass + 1 < pend) load_batch(0, min(eb, nsteps));
+        const double f2 = kFix && rowok ? 2.0 * s_rsc[r] : 2.0;
         for (int st = warp >> 2; st < Sg; st += 2) {
           double pc[kN];
 #pragma unroll

@@ -839,6 +839,13 @@ __global__ void __launch_bounds__(kEvalThreads, 2) k_eval_tc(const __grid_consta
           for (int k2 = 0; k2 < kN; k2++) pc[k2] = pv[k2];
           double *pbc = pb;
           if (st + 2 < Sg) load_pot(st + 2);
+          // L2 prefetch of this lane's line (k2 = rk1) of its step st + 4 box
+          if (rowok && st + 4 < Sg) {
+            const int box4 = a.steps[(size_t)(sb + s0 + st + 4) * stride + 1 + rslot];
+            if (box4 >= 0)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(pot + (size_t)box4 * nd * npb + (d0 + rdl) +
+                                                             (size_t)nd * rk1 * (n + 1)));
+          }
           float v0[kN], v1[kN];  // columns 16 st .. 16 st + n - 1 of the step
           const uint32_t col = lb + (uint32_t)(16 * st);
           if constexpr (kN == 16) {
